@@ -1,0 +1,131 @@
+/*
+ * ssblasGemmBatchedEx for NVIDIA B200 (sm_100a): public C ABI.
+ *
+ * The two entry points of the reference library (hirokitokura/ssblasEx, include/ssblasBatch.h:15-57)
+ * keep their exact names, argument order, types and status codes, so a caller of the reference
+ * relinks against libssblas_b200.so unchanged. Differences in meaning:
+ *
+ *  - A[], B[], C[] may be (a) host arrays of host pointers, as the reference takes them: the
+ *    library stages the matrices through device memory and returns after C is written back;
+ *    (b) host arrays of device pointers; or (c) device arrays of device pointers (the cuBLAS
+ *    batched convention). The kind is detected from the first pointer of each array; all
+ *    pointers of one array must be of the same kind.
+ *  - Calls are synchronous by default, as in the reference: the call returns after C is final.
+ *    ssblasSetSyncMode(0) makes device-pointer calls asynchronous on the stream set with
+ *    ssblasSetStream.
+ *  - op C, which the reference rejects on the fp rows and mis-computes on the int8 row, returns
+ *    SSBLAS_STATUS_INVALID_VALUE on every row. A leading dimension smaller than the stored row
+ *    count, or a NULL alpha/beta/array, also returns SSBLAS_STATUS_INVALID_VALUE (the reference
+ *    does not check these). Everything else follows the reference, including:
+ *      m, n or batchCount <= 0 -> SSBLAS_STATUS_INTERNAL_ERROR;  k <= 0 -> success, C unchanged;
+ *      beta == 0 -> C is not read; int8 arithmetic wraps modulo 2^32;
+ *      alpha/beta point to float (fp32 row), double (fp64 row) or int32 (int8 row), in host memory.
+ *  - If SSBLAS_GEMMBATCHEDEX_DEBUG is set in the environment, every call first prints the
+ *    reference's argument dump (reference src/include/Impl/GemmBatchedEx/ssblasGemmBatchedEx.cpp:48-93).
+ */
+#ifndef SSBLASBATCH
+#define SSBLASBATCH
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#include "ssblasBatch_type.h"
+
+/* Replaces reference include/ssblasBatch.h:15-35 (implementation:
+ * src/include/Impl/GemmBatchedEx/ssblasGemmBatchedEx.cpp:173-220). */
+ssblasStatus_t ssblasGemmBatchedEx(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
+                                   SSINT n, SSINT k, const void* alpha, const void* const A[],
+                                   ssblasDataType_t Atype, const SSINT lda, const void* const B[],
+                                   ssblasDataType_t Btype, const SSINT ldb, const void* beta,
+                                   void* const C[], ssblasDataType_t Ctype, const SSINT ldc,
+                                   const SSINT batchCount, ssblasComputeType_t computeType,
+                                   ssblasGemmAlgo_t algo);
+
+/* Replaces reference include/ssblasBatch.h:37-57. The reference's body is a stub that returns an
+ * uninitialised status (ssblasGemmBatchedEx.cpp:222-268); here it is the same computation as
+ * ssblasGemmBatchedEx (all integers are already 64-bit). */
+ssblasStatus_t ssblasGemmBatchedEx_64(ssblasOperation_t transa, ssblasOperation_t transb,
+                                      SSLONG m, SSLONG n, SSLONG k, const void* alpha,
+                                      const void* const A[], ssblasDataType_t Atype,
+                                      const SSLONG lda, const void* const B[],
+                                      ssblasDataType_t Btype, const SSLONG ldb, const void* beta,
+                                      void* const C[], ssblasDataType_t Ctype, const SSLONG ldc,
+                                      const SSLONG batchCount, ssblasComputeType_t computeType,
+                                      ssblasGemmAlgo_t algo);
+
+/* ============================ EXTENSIONS (not in the reference) ============================ */
+
+/* Grouped batched GEMM: group g holds group_size[g] instances sharing transa/transb/m/n/k/
+ * alpha/beta/ld/types of index g; the A/B/C pointer arrays list the instances of all groups in
+ * order. alpha_array[g]/beta_array[g] point to the group's host scalar of its scale type. The
+ * per-group types must form one of the three rows (fp32, fp64, int8->int32); rows may differ
+ * between groups, and all instances run in one persistent launch per phase. Pointer arrays
+ * follow the same three conventions as ssblasGemmBatchedEx. */
+ssblasStatus_t ssblasGemmGroupedBatchedEx(
+    const ssblasOperation_t transa_array[], const ssblasOperation_t transb_array[],
+    const SSINT m_array[], const SSINT n_array[], const SSINT k_array[],
+    const void* const alpha_array[], const void* const A[], const ssblasDataType_t Atype_array[],
+    const SSINT lda_array[], const void* const B[], const ssblasDataType_t Btype_array[],
+    const SSINT ldb_array[], const void* const beta_array[], void* const C[],
+    const ssblasDataType_t Ctype_array[], const SSINT ldc_array[], const SSINT group_count,
+    const SSINT group_size[], ssblasComputeType_t computeType, ssblasGemmAlgo_t algo);
+
+/* The CUDA stream (a cudaStream_t passed as void*) used by all following calls of this host
+ * thread's process; NULL selects the legacy default stream. */
+ssblasStatus_t ssblasSetStream(void* stream);
+ssblasStatus_t ssblasGetStream(void** stream);
+
+/* 1 (default): every call returns after its result is final. 0: calls whose pointer arrays and
+ * matrices are all in device memory return after enqueueing their work on the stream. */
+ssblasStatus_t ssblasSetSyncMode(int synchronous);
+
+/* Bitwise OR of ssblasMathMode_t flags for the fp64 and fp32 rows. */
+ssblasStatus_t ssblasSetMathMode(int mode);
+ssblasStatus_t ssblasGetMathMode(int* mode);
+
+/* Number of int8 slices per operand in SSBLAS_MATH_FP64_OZAKI mode (3..8); 0 selects it from the
+ * error bound (the default). */
+ssblasStatus_t ssblasSetOzakiSlices(int slices);
+
+/* Description of the most recent call on this process. */
+typedef struct {
+  int path;          /* ssblasPath_t of the main GEMM phase */
+  int slices;        /* Ozaki slices per operand (0 when not emulated) */
+  int kernel_launches;
+  int device_error;  /* nonzero if a bounded device-side wait gave up (the call then returned
+                        SSBLAS_STATUS_INTERNAL_ERROR) */
+} ssblasRunInfo_t;
+
+typedef enum {
+  SSBLAS_PATH_NONE = 0,
+  SSBLAS_PATH_SIMT = 1,            /* register-tiled FFMA / DFMA / integer kernel */
+  SSBLAS_PATH_I8_TCGEN05 = 2,      /* int8 -> int32 on tcgen05.mma kind::i8, TMA staging */
+  SSBLAS_PATH_OZAKI_TCGEN05 = 3,   /* fp64 via int8 slices on tcgen05.mma kind::i8 */
+  SSBLAS_PATH_BF16X3_TCGEN05 = 4,  /* fp32 via three BF16 split products, tcgen05 kind::f16 */
+  SSBLAS_PATH_GROUPED = 5          /* grouped persistent launch */
+} ssblasPath_t;
+
+ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);
+
+/* Per-kernel device timing: while enabled, the library records a CUDA event pair around each of
+ * its kernel launches on the launching stream. ssblasGetProfile returns, per kernel name, the
+ * number of launches and their summed event time since profiling was (re)enabled; it waits for
+ * the recorded events. *entries receives the number of kernels (which may exceed max_entries). */
+typedef struct {
+  char name[48];
+  int launches;
+  double total_ms;
+} ssblasKernelProfile_t;
+
+ssblasStatus_t ssblasSetProfiling(int enable);
+ssblasStatus_t ssblasGetProfile(ssblasKernelProfile_t* out, int max_entries, int* entries);
+
+/* Frees the device workspace cached by the library (it is re-created on the next call). */
+ssblasStatus_t ssblasReleaseWorkspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,664 @@
+// Host layer of the C ABI: argument dump, validation, pointer-kind handling, staging of host
+// matrices, dispatch to the device kernels, and the synchronous return.
+//
+// Follows the reference's entry chain: ssblasGemmBatchedEx -> ssblasGemmEx_main (argument dump
+// when SSBLAS_GEMMBATCHEDEX_DEBUG is set, src/include/Impl/GemmBatchedEx/ssblasGemmBatchedEx.cpp:97-172)
+// -> type-row selection (ssblasGemmBatchedExSelector.hpp:35-107) -> per-row trans checks
+// (ssblasGemmBatchedEx_ALLDATASIZESAME.hpp:45-157) -> launch (src/include/Launcher/launcher.hpp:165-246,
+// whose empty-grid check gives INTERNAL_ERROR for m, n or batchCount <= 0).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cstdio>
+#include <iostream>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace ssb {
+
+Settings& settings() {
+  static Settings s = [] {
+    Settings t;
+    if (const char* e = getenv("SSBLAS_MATH_MODE")) {
+      std::string v(e);
+      int mode = 0;
+      if (v.find("OZAKI") != std::string::npos) mode |= SSBLAS_MATH_FP64_OZAKI;
+      if (v.find("BF16X3") != std::string::npos) mode |= SSBLAS_MATH_FP32_BF16X3;
+      t.math_mode = mode;
+    }
+    return t;
+  }();
+  return s;
+}
+
+static std::mutex g_mutex;
+static ssblasRunInfo_t g_info;
+
+// ---------------------------------------------------------------- kernel profiling -----------
+struct ProfPending {
+  const char* name;
+  cudaEvent_t a, b;
+};
+struct ProfTotal {
+  std::string name;
+  int launches = 0;
+  double ms = 0.0;
+};
+static bool g_prof_on = false;
+static std::vector<ProfPending> g_prof_pending;
+static std::vector<ProfTotal> g_prof_total;
+static std::vector<cudaEvent_t> g_prof_free;
+
+static cudaEvent_t prof_event() {
+  cudaEvent_t e = nullptr;
+  if (!g_prof_free.empty()) {
+    e = g_prof_free.back();
+    g_prof_free.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+
+void prof_start(const char* name, cudaStream_t st) {
+  if (!g_prof_on) return;
+  ProfPending p{name, prof_event(), prof_event()};
+  if (p.a) cudaEventRecord(p.a, st);
+  g_prof_pending.push_back(p);
+}
+
+void prof_stop(cudaStream_t st) {
+  if (!g_prof_on || g_prof_pending.empty()) return;
+  ProfPending& p = g_prof_pending.back();
+  if (p.b) cudaEventRecord(p.b, st);
+}
+
+static void prof_resolve() {
+  for (auto& p : g_prof_pending) {
+    float ms = 0.f;
+    if (p.a && p.b && cudaEventSynchronize(p.b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      ProfTotal* t = nullptr;
+      for (auto& q : g_prof_total)
+        if (q.name == p.name) t = &q;
+      if (!t) {
+        g_prof_total.push_back(ProfTotal{p.name});
+        t = &g_prof_total.back();
+      }
+      t->launches += 1;
+      t->ms += ms;
+    }
+    cudaGetLastError();
+    if (p.a) g_prof_free.push_back(p.a);
+    if (p.b) g_prof_free.push_back(p.b);
+  }
+  g_prof_pending.clear();
+}
+
+void note_launch(int count) { g_info.kernel_launches += count; }
+void note_path(int path, int slices) {
+  g_info.path = path;
+  g_info.slices = slices;
+}
+
+int num_sms() {
+  static int sms = [] {
+    int dev = 0, v = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+      return v;
+    cudaGetLastError();
+    return 148;
+  }();
+  return sms;
+}
+
+// ---------------------------------------------------------------- workspace ------------------
+struct DeviceWs {
+  void* ptr[WS_NUM] = {};
+  size_t size[WS_NUM] = {};
+};
+static std::vector<DeviceWs> g_ws;
+
+void* workspace(WsSlot slot, size_t bytes, cudaError_t* err) {
+  int dev = 0;
+  *err = cudaGetDevice(&dev);
+  if (*err != cudaSuccess) return nullptr;
+  if ((int)g_ws.size() <= dev) g_ws.resize(dev + 1);
+  DeviceWs& w = g_ws[dev];
+  if (bytes == 0) bytes = 256;
+  if (w.size[slot] >= bytes) return w.ptr[slot];
+  if (w.ptr[slot]) {
+    // the old buffer may still be read by work in flight
+    cudaStreamSynchronize(settings().stream);
+    cudaFree(w.ptr[slot]);
+    w.ptr[slot] = nullptr;
+    w.size[slot] = 0;
+  }
+  size_t grow = bytes + bytes / 4;
+  grow = (grow + 4095) & ~(size_t)4095;
+  *err = cudaMalloc(&w.ptr[slot], grow);
+  if (*err != cudaSuccess) {
+    cudaGetLastError();
+    w.ptr[slot] = nullptr;
+    return nullptr;
+  }
+  w.size[slot] = grow;
+  return w.ptr[slot];
+}
+
+static void release_workspace() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  if ((int)g_ws.size() <= dev) return;
+  cudaDeviceSynchronize();
+  for (int s = 0; s < WS_NUM; ++s) {
+    if (g_ws[dev].ptr[s]) cudaFree(g_ws[dev].ptr[s]);
+    g_ws[dev].ptr[s] = nullptr;
+    g_ws[dev].size[s] = 0;
+  }
+}
+
+__device__ int g_device_error = 0;
+int* device_error_flag() {
+  int* p = nullptr;
+  if (cudaGetSymbolAddress((void**)&p, g_device_error) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+// ---------------------------------------------------------------- debug dump -----------------
+// Byte-for-byte the reference's dump (ssblasGemmBatchedEx.cpp:8-93), including its spellings.
+static void print_op(ssblasOperation_t t) {
+  if (SSBLAS_OP_N == t) printf("SSBLAS_OP_N");
+  else if (SSBLAS_OP_T == t) printf("SSBLAS_OP_T");
+  else if (SSBLAS_OP_C == t) printf("SSBLAS_OP_C");
+  else printf("UNKNOWN");
+}
+static void print_type(ssblasDataType_t t) {
+  if (SSBLAS_R_8I == t) printf("SSBLAS_R_8I");
+  else if (SSBLAS_R_8U == t) printf("SSBLAS_R_8U");
+  else if (SSBLAS_R_16F == t) printf("SSBLAS_R_16F");
+  else if (SSBLAS_R_32I == t) printf("SSBLAS_R_32I");
+  else if (SSBLAS_R_32F == t) printf("SSBLAS_R_32F");
+  else if (SSBLAS_R_64F == t) printf("SSBLAS_R_64F");
+  else printf("UNKNONW");
+}
+static void print_compute(ssblasComputeType_t c) {
+  if (SSBLAS_COMPUTE_DEFAULT_TYPE == c) printf("SSBLAS_COMPUTE_DEFAULT_TYPE");
+  else if (SSBLAS_COMPUTE_32I == c) printf("SSBLAS_COMPUTE_32I");
+  else if (SSBLAS_COMPUTE_32F == c) printf("SSBLAS_COMPUTE_32F");
+  else printf("UNKNONW");
+}
+static void print_algo(ssblasGemmAlgo_t a) {
+  if (SSBLAS_COMPUTE_DEFAULT == a) printf("SSBLAS_COMPUTE_DEFAULT");
+  else printf("UNKNONW");
+}
+static void debug_dump(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m, SSINT n, SSINT k,
+                       ssblasDataType_t Atype, SSINT lda, ssblasDataType_t Btype, SSINT ldb,
+                       ssblasDataType_t Ctype, SSINT ldc, SSINT batchCount,
+                       ssblasComputeType_t computeType, ssblasGemmAlgo_t algo) {
+  printf("ssblasGemmBatchedExShowdebug: START\n");
+  printf("transa: "); print_op(transa); printf("\n");
+  printf("transb: "); print_op(transb); printf("\n");
+  std::cout << "M: " << m << std::endl;
+  std::cout << "N: " << n << std::endl;
+  std::cout << "K: " << k << std::endl;
+  std::cout << "alpha: " << "" << std::endl;
+  std::cout << "A: " << "" << std::endl;
+  printf("Atype: "); print_type(Atype); printf("\n");
+  std::cout << "lda: " << lda << std::endl;
+  std::cout << "B: " << "" << std::endl;
+  printf("Btype: "); print_type(Btype); printf("\n");
+  std::cout << "ldb: " << ldb << std::endl;
+  std::cout << "beta: " << "" << std::endl;
+  std::cout << "C: " << "" << std::endl;
+  printf("Ctype: "); print_type(Ctype); printf("\n");
+  std::cout << "ldc: " << ldc << std::endl;
+  std::cout << "batchCount: " << batchCount << std::endl;
+  printf("computeType: "); print_compute(computeType); printf("\n");
+  printf("algo: "); print_algo(algo); printf("\n");
+  printf("ssblasGemmBatchedExShowdebug: END\n");
+  fflush(stdout);
+}
+
+// ---------------------------------------------------------------- pointers -------------------
+enum PtrKind { PK_HOST = 0, PK_DEVICE = 1 };
+
+static PtrKind kind_of(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return PK_HOST;
+  }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) ? PK_DEVICE : PK_HOST;
+}
+
+static size_t elem_size(Row r, bool c_operand) {
+  if (r == ROW_F32) return 4;
+  if (r == ROW_F64) return 8;
+  return c_operand ? 4 : 1;
+}
+
+// Uniform byte stride of a host pointer array (0 if not uniform or not increasing).
+static long uniform_stride(const void* const* ptrs, long batch) {
+  if (batch <= 1) return 0;
+  long s = (long)((const char*)ptrs[1] - (const char*)ptrs[0]);
+  if (s <= 0) return 0;
+  for (long b = 2; b < batch; ++b)
+    if ((long)((const char*)ptrs[b] - (const char*)ptrs[b - 1]) != s) return 0;
+  return s;
+}
+
+// Pinned host scratch for pointer arrays; reused after the previous upload has completed.
+struct PinnedRing {
+  void* host = nullptr;
+  size_t size = 0;
+  cudaEvent_t done = nullptr;
+};
+static PinnedRing g_pin;
+
+static void* pinned(size_t bytes, cudaError_t* err) {
+  *err = cudaSuccess;
+  if (g_pin.done) cudaEventSynchronize(g_pin.done);
+  if (g_pin.size < bytes) {
+    if (g_pin.host) cudaFreeHost(g_pin.host);
+    g_pin.host = nullptr;
+    g_pin.size = 0;
+    size_t sz = (bytes + bytes / 4 + 4095) & ~(size_t)4095;
+    *err = cudaMallocHost(&g_pin.host, sz);
+    if (*err != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_pin.size = sz;
+  }
+  if (!g_pin.done) cudaEventCreateWithFlags(&g_pin.done, cudaEventDisableTiming);
+  return g_pin.host;
+}
+
+static ssblasStatus_t map_err(cudaError_t e) {
+  if (e == cudaSuccess) return SSBLAS_STATUS_SUCCESS;
+  if (e == cudaErrorMemoryAllocation) return SSBLAS_STATUS_ALLOC_FAILED;
+  return SSBLAS_STATUS_INTERNAL_ERROR;
+}
+
+// Stages the instances of one host-resident operand into device memory. Returns the device
+// pointers in dptr (host vector). copy_in=false allocates without copying.
+static cudaError_t stage_operand(WsSlot slot, const void* const* hptr, long batch, size_t inst_bytes,
+                                 bool copy_in, cudaStream_t st, std::vector<void*>& dptr,
+                                 long* dev_stride) {
+  long s = uniform_stride(hptr, batch);
+  dptr.resize(batch);
+  cudaError_t e;
+  // one copy of the whole span when the instances are equally spaced and densely packed
+  if (batch == 1 || (s > 0 && (size_t)s >= inst_bytes && (size_t)s <= 2 * inst_bytes + 4096)) {
+    size_t span = (batch == 1) ? inst_bytes : (size_t)s * (batch - 1) + inst_bytes;
+    char* d = (char*)workspace(slot, span, &e);
+    if (!d) return e;
+    if (copy_in) {
+      e = cudaMemcpyAsync(d, hptr[0], span, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return e;
+    }
+    for (long b = 0; b < batch; ++b) dptr[b] = d + (size_t)b * (size_t)s;
+    *dev_stride = (batch == 1) ? (long)((inst_bytes + 255) & ~(size_t)255) : s;
+    return cudaSuccess;
+  }
+  size_t pitch = (inst_bytes + 255) & ~(size_t)255;
+  char* d = (char*)workspace(slot, pitch * batch, &e);
+  if (!d) return e;
+  for (long b = 0; b < batch; ++b) {
+    dptr[b] = d + pitch * b;
+    if (copy_in) {
+      e = cudaMemcpyAsync(dptr[b], hptr[b], inst_bytes, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  *dev_stride = (long)pitch;
+  return cudaSuccess;
+}
+
+struct Rowsel {
+  Row row;
+  bool ok;
+};
+
+static Rowsel select_row(ssblasDataType_t a, ssblasDataType_t b, ssblasDataType_t c) {
+  if (a == SSBLAS_R_8I && b == SSBLAS_R_8I && c == SSBLAS_R_32I) return {ROW_I8, true};
+  if (a == SSBLAS_R_64F && b == SSBLAS_R_64F && c == SSBLAS_R_64F) return {ROW_F64, true};
+  if (a == SSBLAS_R_32F && b == SSBLAS_R_32F && c == SSBLAS_R_32F) return {ROW_F32, true};
+  return {ROW_F32, false};
+}
+
+// Runs the row's kernels on device-resident data.
+static cudaError_t dispatch(const BatchDesc& d, cudaStream_t st) {
+  const int mode = settings().math_mode;
+  if (d.row == ROW_I8) {
+    cudaError_t e = launch_i8_tcgen05(d, st);
+    if (e != cudaErrorNotSupported) {
+      if (e == cudaSuccess) note_path(SSBLAS_PATH_I8_TCGEN05);
+      return e;
+    }
+  } else if (d.row == ROW_F64 && (mode & SSBLAS_MATH_FP64_OZAKI)) {
+    int s = settings().ozaki_slices;
+    cudaError_t e = launch_ozaki_f64(d, s, st);
+    if (e != cudaErrorNotSupported) return e;
+  } else if (d.row == ROW_F32 && (mode & SSBLAS_MATH_FP32_BF16X3)) {
+    cudaError_t e = launch_bf16x3_f32(d, st);
+    if (e != cudaErrorNotSupported) {
+      if (e == cudaSuccess) note_path(SSBLAS_PATH_BF16X3_TCGEN05);
+      return e;
+    }
+  }
+  note_path(SSBLAS_PATH_SIMT);
+  return launch_simt_gemm(d, st);
+}
+
+static ssblasStatus_t check_device_error(cudaStream_t st) {
+  int* flag = device_error_flag();
+  if (!flag) return SSBLAS_STATUS_INTERNAL_ERROR;
+  int h = 0;
+  if (cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SSBLAS_STATUS_INTERNAL_ERROR;
+  if (h != 0) {
+    g_info.device_error = h;
+    int zero = 0;
+    cudaMemcpyAsync(flag, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    return SSBLAS_STATUS_INTERNAL_ERROR;
+  }
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+// Single-launch grouped path (grouped.cu); returns SSBLAS_STATUS_NOT_COMPUTED_ERROR when the
+// call is not eligible and the per-group loop must run instead.
+ssblasStatus_t grouped_persistent(
+    const ssblasOperation_t transa_array[], const ssblasOperation_t transb_array[],
+    const SSINT m_array[], const SSINT n_array[], const SSINT k_array[],
+    const void* const alpha_array[], const void* const A[], const ssblasDataType_t Atype_array[],
+    const SSINT lda_array[], const void* const B[], const ssblasDataType_t Btype_array[],
+    const SSINT ldb_array[], const void* const beta_array[], void* const C[],
+    const ssblasDataType_t Ctype_array[], const SSINT ldc_array[], SSINT group_count,
+    const SSINT group_size[]);
+
+static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
+                                   SSINT n, SSINT k, const void* alpha, const void* const A[],
+                                   ssblasDataType_t Atype, SSINT lda, const void* const B[],
+                                   ssblasDataType_t Btype, SSINT ldb, const void* beta,
+                                   void* const C[], ssblasDataType_t Ctype, SSINT ldc,
+                                   SSINT batchCount, ssblasComputeType_t computeType,
+                                   ssblasGemmAlgo_t algo) {
+  if (getenv("SSBLAS_GEMMBATCHEDEX_DEBUG") != nullptr)
+    debug_dump(transa, transb, m, n, k, Atype, lda, Btype, ldb, Ctype, ldc, batchCount, computeType, algo);
+
+  Rowsel rs = select_row(Atype, Btype, Ctype);
+  if (!rs.ok) return SSBLAS_STATUS_INVALID_VALUE;
+  if ((transa != SSBLAS_OP_N && transa != SSBLAS_OP_T) || (transb != SSBLAS_OP_N && transb != SSBLAS_OP_T))
+    return SSBLAS_STATUS_INVALID_VALUE;
+  if (m <= 0 || n <= 0 || batchCount <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
+  if (k <= 0) return SSBLAS_STATUS_SUCCESS;  // the reference leaves C untouched
+  if (!alpha || !beta || !A || !B || !C) return SSBLAS_STATUS_INVALID_VALUE;
+  const long arows = (transa == SSBLAS_OP_N) ? m : k, acols = (transa == SSBLAS_OP_N) ? k : m;
+  const long brows = (transb == SSBLAS_OP_N) ? k : n, bcols = (transb == SSBLAS_OP_N) ? n : k;
+  if (lda < arows || ldb < brows || ldc < m) return SSBLAS_STATUS_INVALID_VALUE;
+
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_info = ssblasRunInfo_t{};
+  cudaStream_t st = settings().stream;
+  cudaError_t e;
+
+  BatchDesc d{};
+  d.row = rs.row;
+  d.transa = transa; d.transb = transb;
+  d.m = m; d.n = n; d.k = k; d.lda = lda; d.ldb = ldb; d.ldc = ldc; d.batch = batchCount;
+  if (rs.row == ROW_F32) {
+    d.alpha_f = *(const float*)alpha; d.beta_f = *(const float*)beta;
+  } else if (rs.row == ROW_F64) {
+    d.alpha_d = *(const double*)alpha; d.beta_d = *(const double*)beta;
+  } else {
+    d.alpha_i = *(const int32_t*)alpha; d.beta_i = *(const int32_t*)beta;
+  }
+
+  const size_t ea = elem_size(rs.row, false), ec = elem_size(rs.row, true);
+  const size_t a_bytes = (size_t)(lda * (acols - 1) + arows) * ea;
+  const size_t b_bytes = (size_t)(ldb * (bcols - 1) + brows) * ea;
+  const size_t c_bytes = (size_t)(ldc * (n - 1) + m) * ec;
+
+  const PtrKind arr_kind = kind_of((const void*)A);
+  if (arr_kind == PK_HOST && (kind_of((const void*)B) != PK_HOST || kind_of((const void*)C) != PK_HOST))
+    return SSBLAS_STATUS_INVALID_VALUE;
+  const bool sync = settings().synchronous;
+
+  std::vector<const void*> ha, hb;
+  std::vector<void*> hc, staged_c;
+  bool host_matrices = false;
+  if (arr_kind == PK_DEVICE) {
+    if (kind_of((const void*)B) != PK_DEVICE || kind_of((const void*)C) != PK_DEVICE)
+      return SSBLAS_STATUS_INVALID_VALUE;
+    d.A = (const void* const*)A; d.B = (const void* const*)B; d.C = (void* const*)C;
+    if (sync) {  // read the pointers back to find uniform strides for the tensor-map paths
+      void* h = pinned(3 * sizeof(void*) * batchCount, &e);
+      if (!h) return map_err(e);
+      void** hp = (void**)h;
+      if ((e = cudaMemcpyAsync(hp, A, sizeof(void*) * batchCount, cudaMemcpyDeviceToHost, st)) ||
+          (e = cudaMemcpyAsync(hp + batchCount, B, sizeof(void*) * batchCount, cudaMemcpyDeviceToHost, st)) ||
+          (e = cudaMemcpyAsync(hp + 2 * batchCount, C, sizeof(void*) * batchCount, cudaMemcpyDeviceToHost, st)) ||
+          (e = cudaStreamSynchronize(st)))
+        return map_err(e);
+      d.A0 = hp[0]; d.strideA = uniform_stride((const void* const*)hp, batchCount);
+      d.B0 = hp[batchCount]; d.strideB = uniform_stride((const void* const*)(hp + batchCount), batchCount);
+      d.C0 = hp[2 * batchCount]; d.strideC = uniform_stride((const void* const*)(hp + 2 * batchCount), batchCount);
+    }
+  } else {
+    const PtrKind mk = kind_of(A[0]);
+    if (kind_of(B[0]) != mk || kind_of(C[0]) != mk) return SSBLAS_STATUS_INVALID_VALUE;
+    std::vector<void*> da, db, dc;
+    if (mk == PK_DEVICE) {
+      da.assign((void* const*)A, (void* const*)A + batchCount);
+      db.assign((void* const*)B, (void* const*)B + batchCount);
+      dc.assign(C, C + batchCount);
+      d.strideA = uniform_stride(A, batchCount);
+      d.strideB = uniform_stride(B, batchCount);
+      d.strideC = uniform_stride((const void* const*)C, batchCount);
+    } else {
+      // host matrices, as the reference takes them: stage through device memory
+      host_matrices = true;
+      if ((e = stage_operand(WS_STAGE_A, A, batchCount, a_bytes, true, st, da, &d.strideA)) ||
+          (e = stage_operand(WS_STAGE_B, B, batchCount, b_bytes, true, st, db, &d.strideB)) ||
+          (e = stage_operand(WS_STAGE_C, (const void* const*)C, batchCount, c_bytes,
+                             d.beta_d != 0.0 || d.beta_f != 0.0f || d.beta_i != 0, st, dc, &d.strideC)))
+        return map_err(e);
+      if (batchCount == 1) { d.strideA = d.strideB = d.strideC = 0; }
+    }
+    d.A0 = da[0]; d.B0 = db[0]; d.C0 = dc[0];
+    // upload the three pointer arrays
+    void* h = pinned(3 * sizeof(void*) * batchCount, &e);
+    if (!h) return map_err(e);
+    void** hp = (void**)h;
+    memcpy(hp, da.data(), sizeof(void*) * batchCount);
+    memcpy(hp + batchCount, db.data(), sizeof(void*) * batchCount);
+    memcpy(hp + 2 * batchCount, dc.data(), sizeof(void*) * batchCount);
+    void** dp = (void**)workspace(WS_PTRS, 3 * sizeof(void*) * batchCount, &e);
+    if (!dp) return map_err(e);
+    if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * batchCount, cudaMemcpyHostToDevice, st)))
+      return map_err(e);
+    cudaEventRecord(g_pin.done, st);
+    d.A = (const void* const*)dp;
+    d.B = (const void* const*)(dp + batchCount);
+    d.C = (void* const*)(dp + 2 * batchCount);
+    if (host_matrices) {
+      hc.assign(C, C + batchCount);
+      staged_c = dc;
+    }
+  }
+
+  if ((e = dispatch(d, st)) != cudaSuccess) return map_err(e);
+
+  if (host_matrices) {
+    // copy back only the m x n part of each C (the ld padding of the caller stays untouched)
+    long hs = uniform_stride((const void* const*)C, batchCount);
+    if (batchCount > 1 && hs == (long)(ldc * n * ec) && (char*)staged_c[1] - (char*)staged_c[0] == hs) {
+      e = cudaMemcpy2DAsync(hc[0], ldc * ec, staged_c[0], ldc * ec, m * ec, (size_t)n * batchCount,
+                            cudaMemcpyDeviceToHost, st);
+    } else {
+      for (long b = 0; b < batchCount && e == cudaSuccess; ++b)
+        e = cudaMemcpy2DAsync(hc[b], ldc * ec, staged_c[b], ldc * ec, m * ec, n,
+                              cudaMemcpyDeviceToHost, st);
+    }
+    if (e != cudaSuccess) return map_err(e);
+  }
+  if (sync || host_matrices) {
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_err(e);
+    return check_device_error(st);
+  }
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace ssb
+
+using namespace ssb;
+
+extern "C" {
+
+ssblasStatus_t ssblasGemmBatchedEx(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
+                                   SSINT n, SSINT k, const void* alpha, const void* const A[],
+                                   ssblasDataType_t Atype, const SSINT lda, const void* const B[],
+                                   ssblasDataType_t Btype, const SSINT ldb, const void* beta,
+                                   void* const C[], ssblasDataType_t Ctype, const SSINT ldc,
+                                   const SSINT batchCount, ssblasComputeType_t computeType,
+                                   ssblasGemmAlgo_t algo) {
+  return gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta, C, Ctype,
+                      ldc, batchCount, computeType, algo);
+}
+
+ssblasStatus_t ssblasGemmBatchedEx_64(ssblasOperation_t transa, ssblasOperation_t transb,
+                                      SSLONG m, SSLONG n, SSLONG k, const void* alpha,
+                                      const void* const A[], ssblasDataType_t Atype,
+                                      const SSLONG lda, const void* const B[],
+                                      ssblasDataType_t Btype, const SSLONG ldb, const void* beta,
+                                      void* const C[], ssblasDataType_t Ctype, const SSLONG ldc,
+                                      const SSLONG batchCount, ssblasComputeType_t computeType,
+                                      ssblasGemmAlgo_t algo) {
+  return gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta, C, Ctype,
+                      ldc, batchCount, computeType, algo);
+}
+
+// Grouped batched GEMM. Validation follows the batched call for each group; groups run in order
+// on the library stream. (The persistent single-launch scheduler replaces this loop when all
+// groups are device-resident; see grouped.cu.)
+ssblasStatus_t ssblasGemmGroupedBatchedEx(
+    const ssblasOperation_t transa_array[], const ssblasOperation_t transb_array[],
+    const SSINT m_array[], const SSINT n_array[], const SSINT k_array[],
+    const void* const alpha_array[], const void* const A[], const ssblasDataType_t Atype_array[],
+    const SSINT lda_array[], const void* const B[], const ssblasDataType_t Btype_array[],
+    const SSINT ldb_array[], const void* const beta_array[], void* const C[],
+    const ssblasDataType_t Ctype_array[], const SSINT ldc_array[], const SSINT group_count,
+    const SSINT group_size[], ssblasComputeType_t computeType, ssblasGemmAlgo_t algo) {
+  if (group_count <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
+  if (!transa_array || !transb_array || !m_array || !n_array || !k_array || !alpha_array || !A ||
+      !Atype_array || !lda_array || !B || !Btype_array || !ldb_array || !beta_array || !C ||
+      !Ctype_array || !ldc_array || !group_size)
+    return SSBLAS_STATUS_INVALID_VALUE;
+  ssblasStatus_t st = grouped_persistent(transa_array, transb_array, m_array, n_array, k_array,
+                                         alpha_array, A, Atype_array, lda_array, B, Btype_array,
+                                         ldb_array, beta_array, C, Ctype_array, ldc_array,
+                                         group_count, group_size);
+  if (st != SSBLAS_STATUS_NOT_COMPUTED_ERROR) return st;
+  long off = 0;
+  for (SSINT g = 0; g < group_count; ++g) {
+    if (group_size[g] <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
+    st = gemm_batched(transa_array[g], transb_array[g], m_array[g], n_array[g], k_array[g],
+                      alpha_array[g], A + off, Atype_array[g], lda_array[g], B + off,
+                      Btype_array[g], ldb_array[g], beta_array[g], C + off, Ctype_array[g],
+                      ldc_array[g], group_size[g], computeType, algo);
+    if (st != SSBLAS_STATUS_SUCCESS) return st;
+    off += group_size[g];
+  }
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetStream(void* stream) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().stream = (cudaStream_t)stream;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetStream(void** stream) {
+  if (!stream) return SSBLAS_STATUS_INVALID_VALUE;
+  *stream = (void*)settings().stream;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetSyncMode(int synchronous) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().synchronous = synchronous != 0;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetMathMode(int mode) {
+  if (mode & ~(SSBLAS_MATH_FP64_OZAKI | SSBLAS_MATH_FP32_BF16X3)) return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().math_mode = mode;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetMathMode(int* mode) {
+  if (!mode) return SSBLAS_STATUS_INVALID_VALUE;
+  *mode = settings().math_mode;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetOzakiSlices(int slices) {
+  if (slices != 0 && (slices < 3 || slices > 8)) return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().ozaki_slices = slices;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info) {
+  if (!info) return SSBLAS_STATUS_INVALID_VALUE;
+  *info = g_info;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetProfiling(int enable) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  prof_resolve();
+  g_prof_total.clear();
+  g_prof_on = enable != 0;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetProfile(ssblasKernelProfile_t* out, int max_entries, int* entries) {
+  if (!entries || (max_entries > 0 && !out)) return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  prof_resolve();
+  int n = 0;
+  for (auto& t : g_prof_total) {
+    if (n < max_entries) {
+      snprintf(out[n].name, sizeof(out[n].name), "%s", t.name.c_str());
+      out[n].launches = t.launches;
+      out[n].total_ms = t.ms;
+    }
+    ++n;
+  }
+  *entries = n;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasReleaseWorkspace(void) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  release_workspace();
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+}  // extern "C"

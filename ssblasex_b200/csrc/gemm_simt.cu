@@ -1,0 +1,230 @@
+// Register-tiled SIMT batched GEMM: the plain fp32 (FFMA) and fp64 (DFMA) rows, and the int8 row
+// for layouts the tensor-core path does not take.
+//
+// Semantics follow the reference (hirokitokura/ssblasEx): C <- beta*C (not read when beta == 0,
+// src/include/CScale/Xgemm_scale_kernel.hpp:164-176) then C <- C + acc*alpha with one fused
+// multiply-add (src/include/GemmCore/Xgemm_kernel_sve_v4x5_1.hpp:93-127); int8 products
+// accumulate in int32 with wrap-around (sdot, src/include/asm/SVE/def_sve_asm_float.h:46).
+// The reference adds alpha*acc once per 512-wide K block; this kernel adds it once, which
+// differs only by rounding on the fp rows and not at all on the int8 row.
+//
+// Design: one CTA per (BM x BN tile, instance); op(A)/op(B) tiles are staged through shared
+// memory k-major (the transposes are absorbed by the staging loads), double-buffered through
+// registers; each thread owns a TM x TN sub-tile whose rows are spaced by BM/TM so that the
+// column-major C stores of a warp are contiguous.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace ssb {
+namespace {
+
+template <typename T> struct RowTraits;
+template <> struct RowTraits<float> {
+  using AB = float; using Acc = float; using C = float; using S = float;
+  static __device__ __forceinline__ Acc mac(Acc acc, AB a, AB b) { return fmaf(a, b, acc); }
+  static __device__ __forceinline__ C epi(Acc acc, S alpha, S beta, const C* cptr) {
+    C t = (beta == 0.0f) ? 0.0f : beta * (*cptr);
+    return fmaf(acc, alpha, t);
+  }
+};
+template <> struct RowTraits<double> {
+  using AB = double; using Acc = double; using C = double; using S = double;
+  static __device__ __forceinline__ Acc mac(Acc acc, AB a, AB b) { return fma(a, b, acc); }
+  static __device__ __forceinline__ C epi(Acc acc, S alpha, S beta, const C* cptr) {
+    C t = (beta == 0.0) ? 0.0 : beta * (*cptr);
+    return fma(acc, alpha, t);
+  }
+};
+template <> struct RowTraits<int8_t> {
+  using AB = int8_t; using Acc = uint32_t; using C = int32_t; using S = int32_t;
+  static __device__ __forceinline__ Acc mac(Acc acc, AB a, AB b) {
+    return acc + (uint32_t)((int32_t)a * (int32_t)b);
+  }
+  static __device__ __forceinline__ C epi(Acc acc, S alpha, S beta, const C* cptr) {
+    uint32_t t = (beta == 0) ? 0u : (uint32_t)beta * (uint32_t)(*cptr);
+    return (int32_t)(t + acc * (uint32_t)alpha);
+  }
+};
+
+template <typename T>
+struct SimtArgs {
+  int transa, transb;
+  long m, n, k, lda, ldb, ldc, batch;
+  const T* const* A;
+  const T* const* B;
+  typename RowTraits<T>::C* const* C;
+  typename RowTraits<T>::S alpha, beta;
+};
+
+// BM x BN tile, BK deep; NT threads; each thread TM x TN outputs.
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+simt_gemm_kernel(SimtArgs<T> args) {
+  using Tr = RowTraits<T>;
+  using AB = typename Tr::AB;
+  using Acc = typename Tr::Acc;
+  constexpr int TX = BM / TM;            // threads along M (fast index -> coalesced C columns)
+  constexpr int TY = BN / TN;
+  constexpr int NT = TX * TY;
+  constexpr int A_PER = BM * BK / NT;    // staged elements per thread per tile
+  constexpr int B_PER = BK * BN / NT;
+  static_assert(A_PER * NT == BM * BK && B_PER * NT == BK * BN, "tile/thread mismatch");
+
+  __shared__ AB As[2][BK][BM];
+  __shared__ AB Bs[2][BK][BN];
+
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+  const long tiles_m = (args.m + BM - 1) / BM;
+  const long m0 = (blockIdx.x % tiles_m) * BM;
+  const long n0 = (blockIdx.x / tiles_m) * BN;
+
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) {
+    const AB* __restrict__ A = args.A[b];
+    const AB* __restrict__ B = args.B[b];
+
+    AB ra[A_PER], rb[B_PER];
+    // load op(A)[m0.., k0..] and op(B)[k0.., n0..] into registers (zero outside the matrix)
+    auto load_tiles = [&](long k0) {
+#pragma unroll
+      for (int e = 0; e < A_PER; ++e) {
+        int idx = tid + e * NT;
+        int ii, kk;
+        if (args.transa == SSBLAS_OP_N) { ii = idx % BM; kk = idx / BM; }   // rows contiguous
+        else { kk = idx % BK; ii = idx / BK; }                              // k contiguous
+        long gi = m0 + ii, gk = k0 + kk;
+        AB v = AB(0);
+        if (gi < args.m && gk < args.k)
+          v = (args.transa == SSBLAS_OP_N) ? A[gi + gk * args.lda] : A[gi * args.lda + gk];
+        ra[e] = v;
+      }
+#pragma unroll
+      for (int e = 0; e < B_PER; ++e) {
+        int idx = tid + e * NT;
+        int jj, kk;
+        if (args.transb == SSBLAS_OP_N) { kk = idx % BK; jj = idx / BK; }   // k contiguous
+        else { jj = idx % BN; kk = idx / BN; }                              // cols contiguous
+        long gj = n0 + jj, gk = k0 + kk;
+        AB v = AB(0);
+        if (gj < args.n && gk < args.k)
+          v = (args.transb == SSBLAS_OP_N) ? B[gk + gj * args.ldb] : B[gk * args.ldb + gj];
+        rb[e] = v;
+      }
+    };
+    auto store_tiles = [&](int buf) {
+#pragma unroll
+      for (int e = 0; e < A_PER; ++e) {
+        int idx = tid + e * NT;
+        int ii, kk;
+        if (args.transa == SSBLAS_OP_N) { ii = idx % BM; kk = idx / BM; }
+        else { kk = idx % BK; ii = idx / BK; }
+        As[buf][kk][ii] = ra[e];
+      }
+#pragma unroll
+      for (int e = 0; e < B_PER; ++e) {
+        int idx = tid + e * NT;
+        int jj, kk;
+        if (args.transb == SSBLAS_OP_N) { kk = idx % BK; jj = idx / BK; }
+        else { jj = idx % BN; kk = idx / BN; }
+        Bs[buf][kk][jj] = rb[e];
+      }
+    };
+
+    Acc acc[TM][TN];
+#pragma unroll
+    for (int r = 0; r < TM; ++r)
+#pragma unroll
+      for (int c = 0; c < TN; ++c) acc[r][c] = Acc(0);
+
+    const long ktiles = (args.k + BK - 1) / BK;
+    load_tiles(0);
+    store_tiles(0);
+    __syncthreads();
+    for (long kt = 0; kt < ktiles; ++kt) {
+      const int buf = kt & 1;
+      if (kt + 1 < ktiles) load_tiles((kt + 1) * BK);
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        AB av[TM], bv[TN];
+#pragma unroll
+        for (int r = 0; r < TM; ++r) av[r] = As[buf][kk][tx + r * TX];
+#pragma unroll
+        for (int c = 0; c < TN; ++c) bv[c] = Bs[buf][kk][ty + c * TY];
+#pragma unroll
+        for (int r = 0; r < TM; ++r)
+#pragma unroll
+          for (int c = 0; c < TN; ++c) acc[r][c] = Tr::mac(acc[r][c], av[r], bv[c]);
+      }
+      if (kt + 1 < ktiles) store_tiles(buf ^ 1);
+      __syncthreads();
+    }
+
+    typename Tr::C* __restrict__ Cm = args.C[b];
+#pragma unroll
+    for (int c = 0; c < TN; ++c) {
+      long gj = n0 + ty + c * TY;
+      if (gj >= args.n) continue;
+#pragma unroll
+      for (int r = 0; r < TM; ++r) {
+        long gi = m0 + tx + r * TX;
+        if (gi < args.m) {
+          typename Tr::C* p = Cm + gi + gj * args.ldc;
+          *p = Tr::epi(acc[r][c], args.alpha, args.beta, p);
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+cudaError_t launch_tile(const SimtArgs<T>& a, cudaStream_t stream) {
+  long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
+  if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)tiles, (unsigned)(a.batch < 65535 ? a.batch : 65535));
+  ProfScope prof("simt_gemm", stream);
+  simt_gemm_kernel<T, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, stream>>>(a);
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <typename T>
+SimtArgs<T> make_args(const BatchDesc& d) {
+  SimtArgs<T> a;
+  a.transa = d.transa; a.transb = d.transb;
+  a.m = d.m; a.n = d.n; a.k = d.k; a.lda = d.lda; a.ldb = d.ldb; a.ldc = d.ldc; a.batch = d.batch;
+  a.A = (const T* const*)d.A; a.B = (const T* const*)d.B;
+  a.C = (typename RowTraits<T>::C* const*)d.C;
+  return a;
+}
+
+}  // namespace
+
+cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
+  // Large tiles when there is enough work to fill the GPU with them, small tiles otherwise.
+  const long big_tiles = ((d.m + 127) / 128) * ((d.n + 127) / 128) * d.batch;
+  const bool big = big_tiles >= 2L * num_sms();
+  switch (d.row) {
+    case ROW_F32: {
+      auto a = make_args<float>(d);
+      a.alpha = d.alpha_f; a.beta = d.beta_f;
+      return big ? launch_tile<float, 128, 128, 16, 8, 8>(a, stream)
+                 : launch_tile<float, 64, 64, 16, 4, 4>(a, stream);
+    }
+    case ROW_F64: {
+      auto a = make_args<double>(d);
+      a.alpha = d.alpha_d; a.beta = d.beta_d;
+      return big ? launch_tile<double, 128, 128, 8, 8, 8>(a, stream)
+                 : launch_tile<double, 64, 64, 16, 4, 4>(a, stream);
+    }
+    case ROW_I8: {
+      auto a = make_args<int8_t>(d);
+      a.alpha = d.alpha_i; a.beta = d.beta_i;
+      return launch_tile<int8_t, 64, 64, 32, 4, 4>(a, stream);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace ssb

@@ -139,3 +139,36 @@ def normalized_error(p, C: np.ndarray, instances=None, rows=None) -> float:
 
 def unit_roundoff(row: str) -> float:
     return {"f32": 2.0 ** -24, "f64": 2.0 ** -53}[row]
+
+
+def ozaki_f64(p, slices: int, C: np.ndarray | None = None):
+    """The library's Ozaki FP64 emulation restated on the CPU (bit-exact target), all instances.
+    Returns (status, C) -- status -1 if an int32 accumulator would have overflowed."""
+    lib = _load_oracle()
+    f = lib.oracle_ozaki_f64
+    f.argtypes = [c_int, c_int, c_long, c_long, c_long, c_double, c_vp, c_long, c_vp, c_long,
+                  c_double, c_vp, c_long, c_int]
+    f.restype = c_int
+    C = p.C.copy() if C is None else C
+    st = 0
+    for b in range(p.batch):
+        A = np.ascontiguousarray(p.A[b]); B = np.ascontiguousarray(p.B[b])
+        Cb = np.ascontiguousarray(C[b])
+        st |= f(p.transa, p.transb, p.m, p.n, p.k, float(p.alpha), A.ctypes.data, p.lda, B.ctypes.data,
+                p.ldb, float(p.beta), Cb.ctypes.data, p.ldc, slices)
+        C[b] = Cb
+    return st, C
+
+
+def bf16x3_f32(p, b: int):
+    """FP64-exact value of the three-BF16-product emulation for instance b (m x n array)."""
+    lib = _load_oracle()
+    f = lib.oracle_bf16x3_f32
+    f.argtypes = [c_int, c_int, c_long, c_long, c_long, c_float, c_vp, c_long, c_vp, c_long,
+                  c_float, c_vp, c_long, c_vp]
+    f.restype = None
+    out = np.empty(p.m * p.n, dtype=np.float64)
+    A = np.ascontiguousarray(p.A[b]); B = np.ascontiguousarray(p.B[b]); Cb = np.ascontiguousarray(p.C[b])
+    f(p.transa, p.transb, p.m, p.n, p.k, float(p.alpha), A.ctypes.data, p.lda, B.ctypes.data, p.ldb,
+      float(p.beta), Cb.ctypes.data, p.ldc, out.ctypes.data)
+    return out.reshape(p.n, p.m).T

@@ -186,3 +186,112 @@ void oracle_exact_f64(int transa, int transb, long m, long n, long k, double alp
     }
   }
 }
+
+/* --------------------------------------------------------------- Ozaki int8-slice FP64 ---- */
+/* CPU restatement of the library's FP64 emulation (SSBLAS_MATH_FP64_OZAKI), operation for
+ * operation, so the device result must match it bit for bit:
+ *   per row i of op(A): e_i with max_k |a_ik| < 2^e_i (0 for a zero row),
+ *     X = rint(a * 2^(8S-2-e_i)), balanced base-256 digits d_0..d_{S-1} (low digits in
+ *     [-128,127], d_0 = the rest); the same per column j of op(B) with f_j;
+ *   acc_l = sum_{p+q=l, l<S} sum_k dA_p[i,k] dB_q[j,k]  (exact integers);
+ *   v = Horner over l = S-1..0 of v*2^-8 + acc_l (FP64); w = v * 2^(e_i+f_j-12);
+ *   C = fma(w, alpha, beta==0 ? 0 : beta*C).
+ * Returns 0, or -1 if an accumulator left the int32 range the device uses. */
+static void oz_digits(long long X, int S, int8_t* d) {
+  for (int p = S - 1; p >= 1; --p) {
+    long long lo = ((X + 128) & 255) - 128;
+    d[p] = (int8_t)lo;
+    X = (X - lo) >> 8;
+  }
+  d[0] = (int8_t)X;
+}
+
+static void oz_slice(int trans, long rows, long k, const double* X, long ld, int rows_are_cols, int S,
+                     int8_t* dig /* [S][rows][k] */, int* ex) {
+  for (long r = 0; r < rows; ++r) {
+    double mx = 0.0;
+    for (long kk = 0; kk < k; ++kk) {
+      double v = rows_are_cols ? X[at(trans, kk, r, ld)] : X[at(trans, r, kk, ld)];
+      mx = fmax(mx, fabs(v));
+    }
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);
+    ex[r] = e;
+    for (long kk = 0; kk < k; ++kk) {
+      double v = rows_are_cols ? X[at(trans, kk, r, ld)] : X[at(trans, r, kk, ld)];
+      long long Xi = llrint(scalbn(v, 8 * S - 2 - e));
+      int8_t d[8];
+      oz_digits(Xi, S, d);
+      for (int p = 0; p < S; ++p) dig[((long)p * rows + r) * k + kk] = d[p];
+    }
+  }
+}
+
+int oracle_ozaki_f64(int transa, int transb, long m, long n, long k, double alpha, const double* A,
+                     long lda, const double* B, long ldb, double beta, double* C, long ldc, int S) {
+  int8_t* da = (int8_t*)malloc((size_t)S * m * k);
+  int8_t* db = (int8_t*)malloc((size_t)S * n * k);
+  int* ea = (int*)malloc(sizeof(int) * m);
+  int* eb = (int*)malloc(sizeof(int) * n);
+  int status = 0;
+  oz_slice(transa, m, k, A, lda, 0, S, da, ea);
+  oz_slice(transb, n, k, B, ldb, 1, S, db, eb);
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : status)
+  for (long j = 0; j < n; ++j) {
+    long long acc[8];
+    for (long i = 0; i < m; ++i) {
+      for (int l = 0; l < S; ++l) acc[l] = 0;
+      for (int p = 0; p < S; ++p)
+        for (int q = 0; p + q < S; ++q) {
+          const int8_t* x = da + ((long)p * m + i) * k;
+          const int8_t* y = db + ((long)q * n + j) * k;
+          long long s = 0;
+          for (long kk = 0; kk < k; ++kk) s += (long long)x[kk] * (long long)y[kk];
+          acc[p + q] += s;
+        }
+      double v = 0.0;
+      for (int l = S - 1; l >= 0; --l) {
+        if (acc[l] > 2147483647LL || acc[l] < -2147483648LL) status = -1;
+        v = v * 0x1p-8 + (double)acc[l];
+      }
+      double w = scalbn(v, ea[i] + eb[j] - 12);
+      double t = (beta == 0.0) ? 0.0 : beta * C[i + j * ldc];
+      C[i + j * ldc] = fma(w, alpha, t);
+    }
+  }
+  free(da); free(db); free(ea); free(eb);
+  return status;
+}
+
+/* ---------------------------------------------------------------- 3 x BF16 FP32 ---------- */
+static float bf16_rn(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x; /* inf / nan unchanged */
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+/* The value the library's SSBLAS_MATH_FP32_BF16X3 mode approximates, computed exactly in FP64:
+ * hi = bf16(x), lo = bf16(x - hi) for each entry; out = alpha * sum_k (ha hb + ha lb + la hb)
+ * + beta * C (the device accumulates the same products in FP32). */
+void oracle_bf16x3_f32(int transa, int transb, long m, long n, long k, float alpha, const float* A,
+                       long lda, const float* B, long ldb, float beta, const float* C, long ldc,
+                       double* out /* m x n, ld m */) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long j = 0; j < n; ++j)
+    for (long i = 0; i < m; ++i) {
+      double s = 0.0;
+      for (long kk = 0; kk < k; ++kk) {
+        float a = A[at(transa, i, kk, lda)], b = B[at(transb, kk, j, ldb)];
+        float ha = bf16_rn(a), la = bf16_rn(a - ha), hb = bf16_rn(b), lb = bf16_rn(b - hb);
+        s += (double)ha * hb + (double)ha * lb + (double)la * hb;
+      }
+      double r = (double)alpha * s;
+      if (beta != 0.0f) r += (double)beta * C[i + j * ldc];
+      out[i + j * m] = r;
+    }
+}

@@ -1,0 +1,26 @@
+// Operand pre-pass interfaces (prepass.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ssb {
+
+struct PlaneArgs {
+  const void* const* X;   // device array of per-instance operand pointers
+  long rows;              // rows of the K-major result (m for op(A), n for op(B))
+  long K;
+  long ld;                // caller's leading dimension
+  bool kcontig;           // element (r, k) at X[r*ld + k] (true) or X[r + k*ld] (false)
+  long batch;
+  void* out;              // planes [batch][P][rows][Kp]
+  long Kp;                // padded K (elements) = row pitch of a plane
+  long plane_stride;      // bytes between planes = rows * Kp * elem
+  long batch_stride;      // bytes between instances = P * plane_stride
+};
+
+cudaError_t launch_pack_i8(const PlaneArgs& a, cudaStream_t st);
+cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st);
+cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st);
+
+}  // namespace ssb

@@ -1,0 +1,309 @@
+// Persistent, warp-specialised tcgen05 GEMM over a batch of (instance, 128 x BN tile) pairs.
+//
+// Replaces the reference's blocked CPU launcher + packing + SVE microkernel chain
+// (launch_kernels/ssblasGemmBatchedEx_Batchgemm_tune_kernel_BMKN.hpp:157-336 for the tile loop,
+// src/include/ACopy and BCopy for packing, src/include/GemmCore/Xgemm_kernel_sve_v4x5_1.hpp for
+// the register-tile FMA loop, src/include/CScale for the beta pass):
+//   - operand tiles are staged by TMA (cp.async.bulk.tensor) straight into the 128B/64B/32B
+//     swizzled K-major layout the tensor cores read -- there is no packing pass;
+//   - one elected thread issues tcgen05.mma (kind::i8 or kind::f16) accumulating in tensor memory;
+//   - four epilogue warps drain tensor memory (tcgen05.ld) and apply alpha/beta in one pass
+//     (C is read only when beta != 0, as in src/include/CScale/Xgemm_scale_kernel.hpp:164-176).
+//
+// An operand may consist of several "planes" (int8 slices of an FP64 value, or the hi/lo BF16
+// parts of an FP32 value) stored as [batch][plane][rows][K]. Each stage loads all planes of a
+// K block for A and for B with one 4-D TMA each, then multiplies the plane pairs the
+// configuration selects; each pair accumulates into the tensor-memory "level" the configuration
+// assigns to it.
+//
+// Warp roles (192 threads): warp 0 = TMA producer, warp 1 = MMA issuer and TMEM owner,
+// warps 2-5 = epilogue (warp w reads TMEM lanes 32*(w%4) .. +31).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ptx.cuh"
+
+namespace ssb {
+namespace tc {
+
+enum Kind { KIND_I8 = 0, KIND_BF16 = 1 };
+enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2 };
+
+struct Params {
+  long m, n, k;             // GEMM shape (k in elements)
+  long batch;
+  int tiles_m, tiles_n;
+  long total_tiles;
+  long ldc;
+  void* const* C;           // device array of C pointers
+  int c_batch_offset;       // instance b of this launch is C[b + c_batch_offset]
+  double alpha_d, beta_d;
+  float alpha_f, beta_f;
+  int32_t alpha_i, beta_i;
+  const int32_t* exp_a;     // Ozaki: per-row exponents of op(A), [batch][m]
+  const int32_t* exp_b;     // Ozaki: per-column exponents of op(B), [batch][n]
+  int exp_shift;            // Ozaki: result = alpha * 2^(ea+eb+exp_shift) * sum_l acc_l 2^(-8 l)
+  int* err;                 // device error flag
+};
+
+template <int KIND_, int PA_, int PB_, int BN_, int KB_, int STAGES_, int NLEV_, int ACCB_, int EPI_, int PAIRS_>
+struct Config {
+  static constexpr int KIND = KIND_;
+  static constexpr int PA = PA_;       // planes of A
+  static constexpr int PB = PB_;       // planes of B
+  static constexpr int BM = 128;
+  static constexpr int BN = BN_;
+  static constexpr int KB = KB_;       // bytes of K per stage (= swizzle span)
+  static constexpr int STAGES = STAGES_;
+  static constexpr int NLEV = NLEV_;   // accumulator levels
+  static constexpr int ACCB = ACCB_;   // accumulator buffers (2 = epilogue overlaps next tile)
+  static constexpr int EPI = EPI_;
+  static constexpr int PAIRS = PAIRS_; // 0: (0,0) only; 1: p+q <= 1 (bf16x3); 2: p+q < NLEV (Ozaki)
+  static constexpr int ELEM = (KIND == KIND_I8) ? 1 : 2;
+  static constexpr int A_STAGE = PA * BM * KB;
+  static constexpr int B_STAGE = PB * BN * KB;
+  static constexpr int STAGE = A_STAGE + B_STAGE;
+  static constexpr int TMEM_COLS_USED = ACCB * NLEV * BN;
+  static constexpr int TMEM_COLS = TMEM_COLS_USED <= 32 ? 32 : TMEM_COLS_USED <= 64 ? 64 : TMEM_COLS_USED <= 128 ? 128
+                                   : TMEM_COLS_USED <= 256 ? 256 : 512;
+  static constexpr int SMEM = 1024 + STAGES * STAGE + 256;
+  static_assert(TMEM_COLS_USED <= 512, "tensor memory overflow");
+  static_assert(A_STAGE % 1024 == 0 && B_STAGE % 1024 == 0, "stage alignment");
+  static_assert(SMEM <= 232448, "shared memory overflow");
+
+  __host__ __device__ static constexpr bool use_pair(int p, int q) {
+    return PAIRS == 0 ? (p == 0 && q == 0) : PAIRS == 1 ? (p + q <= 1) : (p + q < NLEV);
+  }
+  __host__ __device__ static constexpr int level(int p, int q) { return PAIRS == 2 ? p + q : 0; }
+  // the first pair (in issue order p-major) that writes a level starts it from zero
+  __host__ __device__ static constexpr bool first_of_level(int p, int q) {
+    return PAIRS == 2 ? (p == 0) : (p == 0 && q == 0);
+  }
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(192, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* stages = smem;
+  uint64_t* bars = (uint64_t*)(smem + Cfg::STAGES * Cfg::STAGE);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + Cfg::STAGES;
+  uint64_t* tfull = bars + 2 * Cfg::STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  int* err = prm.err;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::STAGES; ++s) {
+      ptx::mbar_init(ptx::smem_u32(&full[s]), 1);
+      ptx::mbar_init(ptx::smem_u32(&empty[s]), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      ptx::mbar_init(ptx::smem_u32(&tfull[a]), 1);
+      ptx::mbar_init(ptx::smem_u32(&tempty[a]), 4);
+    }
+    ptx::mbar_init(ptx::smem_u32(drain), 1);
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    ptx::prefetch_tmap(&tmA);
+    ptx::prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    ptx::tmem_alloc(ptx::smem_u32(tmem_slot), Cfg::TMEM_COLS);
+    ptx::tmem_relinquish();
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const long tiles_mn = (long)prm.tiles_m * prm.tiles_n;
+  const int KE = Cfg::KB / Cfg::ELEM;                       // K elements per stage
+  const int nk = (int)((prm.k + KE - 1) / KE);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------------ TMA producer ------
+    if (lane == 0) {
+      long it = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x) {
+        const int b = (int)(t / tiles_mn);
+        const long r = t % tiles_mn;
+        const int mt = (int)(r / prm.tiles_n), nt = (int)(r % prm.tiles_n);
+        for (int kb = 0; kb < nk; ++kb, ++it) {
+          const int s = (int)(it % Cfg::STAGES);
+          const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
+          if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11)) { ok = false; break; }
+          const uint32_t fb = ptx::smem_u32(&full[s]);
+          ptx::mbar_arrive_expect_tx(fb, Cfg::STAGE);
+          uint8_t* sa = stages + (size_t)s * Cfg::STAGE;
+          ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, mt * Cfg::BM, 0, b);
+          ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, nt * Cfg::BN, 0, b);
+        }
+      }
+      // no copy may still be in flight when the CTA exits
+      for (long j = (it > Cfg::STAGES ? it - Cfg::STAGES : 0); j < it; ++j)
+        ptx::mbar_wait(ptx::smem_u32(&full[j % Cfg::STAGES]), (uint32_t)((j / Cfg::STAGES) & 1), err, 12);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------------ MMA issuer --------
+    if (lane == 0) {
+      constexpr uint32_t IDESC = (Cfg::KIND == KIND_I8) ? ptx::idesc_i8(128, Cfg::BN, true, true)
+                                                        : ptx::idesc_bf16(128, Cfg::BN);
+      long it = 0;
+      int tcount = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x, ++tcount) {
+        const int acc = tcount % Cfg::ACCB;
+        const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
+        if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21)) { ok = false; break; }
+        ptx::tc_fence_after();
+        const uint32_t d_base = tmem_base + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
+        for (int kb = 0; kb < nk; ++kb, ++it) {
+          const int s = (int)(it % Cfg::STAGES);
+          const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
+          if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), ph, err, 22)) { ok = false; break; }
+          ptx::tc_fence_after();
+          const uint32_t sa = ptx::smem_u32(stages + (size_t)s * Cfg::STAGE);
+          const uint32_t sb = sa + Cfg::A_STAGE;
+#pragma unroll
+          for (int p = 0; p < Cfg::PA; ++p) {
+#pragma unroll
+            for (int q = 0; q < Cfg::PB; ++q) {
+              if (!Cfg::use_pair(p, q)) continue;
+              const uint32_t d = d_base + (uint32_t)(Cfg::level(p, q) * Cfg::BN);
+#pragma unroll
+              for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
+                const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
+                const uint64_t bd = ptx::smem_desc_kmajor(sb + q * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
+                const uint32_t accum = (kb > 0 || kk > 0 || !Cfg::first_of_level(p, q)) ? 1u : 0u;
+                if (Cfg::KIND == KIND_I8) ptx::mma_i8(d, ad, bd, IDESC, accum);
+                else ptx::mma_f16(d, ad, bd, IDESC, accum);
+              }
+            }
+          }
+          ptx::mma_commit(ptx::smem_u32(&empty[s]));   // frees the stage when these MMAs finish
+        }
+        if (!ok) break;
+        ptx::mma_commit(ptx::smem_u32(&tfull[acc]));     // accumulator ready for the epilogue
+      }
+      ptx::mma_commit(ptx::smem_u32(drain));
+      ptx::mbar_wait(ptx::smem_u32(drain), 0, err, 23);
+    }
+  } else {
+    // ------------------------------------------------------------------ epilogue ----------
+    const int quarter = warp % 4;
+    const int row_in_tile = quarter * 32 + lane;
+    int tcount = 0;
+    for (long t = blockIdx.x; t < prm.total_tiles; t += gridDim.x, ++tcount) {
+      const int b = (int)(t / tiles_mn);
+      const long r = t % tiles_mn;
+      const int mt = (int)(r / prm.tiles_n), nt = (int)(r % prm.tiles_n);
+      const int acc = tcount % Cfg::ACCB;
+      const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
+      if (!ptx::mbar_wait(ptx::smem_u32(&tfull[acc]), acc_ph, err, 31)) break;
+      ptx::tc_fence_after();
+      const long gi = (long)mt * Cfg::BM + row_in_tile;
+      const long n0 = (long)nt * Cfg::BN;
+      const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
+      const bool row_ok = gi < prm.m;
+      uint8_t* Cb = (uint8_t*)prm.C[b + prm.c_batch_offset];
+      int32_t ea = 0;
+      if (Cfg::EPI == EPI_OZAKI && row_ok) ea = prm.exp_a[(long)b * prm.m + gi];
+#pragma unroll 1
+      for (int c0 = 0; c0 < Cfg::BN; c0 += 16) {
+        if (Cfg::EPI == EPI_OZAKI) {
+          double v[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = 0.0;
+#pragma unroll 1
+          for (int l = Cfg::NLEV - 1; l >= 0; --l) {
+            uint32_t raw[16];
+            ptx::tmem_ld16(t_row + (uint32_t)(l * Cfg::BN + c0), raw);
+            ptx::tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = v[j] * 0x1p-8 + (double)(int32_t)raw[j];
+          }
+          if (row_ok) {
+            double* Cd = (double*)Cb;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const long gj = n0 + c0 + j;
+              if (gj < prm.n) {
+                const int32_t eb = prm.exp_b[(long)b * prm.n + gj];
+                const double w = scalbn(v[j], ea + eb + prm.exp_shift);
+                double* cp = Cd + gi + gj * prm.ldc;
+                const double tb = (prm.beta_d == 0.0) ? 0.0 : prm.beta_d * (*cp);
+                *cp = fma(w, prm.alpha_d, tb);
+              }
+            }
+          }
+        } else {
+          uint32_t raw[16];
+          ptx::tmem_ld16(t_row + (uint32_t)c0, raw);
+          ptx::tmem_wait_ld();
+          if (row_ok) {
+            if (Cfg::EPI == EPI_I32) {
+              int32_t* Ci = (int32_t*)Cb;
+              if (prm.beta_i == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  const long gj = n0 + c0 + j;
+                  if (gj < prm.n) Ci[gi + gj * prm.ldc] = (int32_t)(raw[j] * (uint32_t)prm.alpha_i);
+                }
+              } else {
+                uint32_t cv[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  const long gj = n0 + c0 + j;
+                  cv[j] = (gj < prm.n) ? (uint32_t)__ldcs(Ci + gi + gj * prm.ldc) : 0u;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  const long gj = n0 + c0 + j;
+                  if (gj < prm.n)
+                    __stcs(Ci + gi + gj * prm.ldc,
+                           (int32_t)((uint32_t)prm.beta_i * cv[j] + raw[j] * (uint32_t)prm.alpha_i));
+                }
+              }
+            } else {
+              float* Cf = (float*)Cb;
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                const long gj = n0 + c0 + j;
+                if (gj < prm.n) {
+                  float* cp = Cf + gi + gj * prm.ldc;
+                  const float tb = (prm.beta_f == 0.0f) ? 0.0f : prm.beta_f * (*cp);
+                  *cp = fmaf(__uint_as_float(raw[j]), prm.alpha_f, tb);
+                }
+              }
+            }
+          }
+        }
+      }
+      ptx::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[acc]));
+    }
+  }
+
+  ptx::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    ptx::tc_fence_after();
+    ptx::tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
+  }
+}
+
+}  // namespace tc
+}  // namespace ssb

@@ -1,14 +1,228 @@
-// placeholder until the tensor-core kernels land
+// Host launchers of the tcgen05 paths: int8 -> int32 (direct TMA from the caller's matrices, or
+// through the int8 pack pre-pass), FP64 via Ozaki int8 slices, FP32 via three BF16 products.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
 #include "internal.h"
+#include "prepass.h"
+#include "tc_gemm.cuh"
+
 namespace ssb {
-cudaError_t launch_i8_tcgen05(const BatchDesc&, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t launch_ozaki_f64(const BatchDesc&, int, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t launch_bf16x3_f32(const BatchDesc&, cudaStream_t) { return cudaErrorNotSupported; }
+namespace {
+
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encoder() {
+  static EncodeFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (EncodeFn) nullptr;
+    }
+    return (EncodeFn)p;
+  }();
+  return fn;
 }
-namespace ssb {
-ssblasStatus_t grouped_persistent(const ssblasOperation_t*, const ssblasOperation_t*, const SSINT*, const SSINT*, const SSINT*,
-    const void* const*, const void* const*, const ssblasDataType_t*, const SSINT*, const void* const*, const ssblasDataType_t*,
-    const SSINT*, const void* const*, void* const*, const ssblasDataType_t*, const SSINT*, SSINT, const SSINT*) {
+
+bool is_sm100() {
+  static int ok = [] {
+    int dev = 0, major = 0, minor = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    cudaGetLastError();
+    return (major == 10 && minor == 0) ? 1 : 0;
+  }();
+  return ok != 0;
+}
+
+// 4-D tiled tensor map: dims {K, rows, planes, batch} (K innermost), strides in bytes.
+bool make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, long K, long rows, long planes,
+              long batch, long row_stride, long plane_stride, long batch_stride, int box_k, int box_rows,
+              int box_planes, int swz_bytes) {
+  EncodeFn enc = encoder();
+  if (!enc) return false;
+  cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)planes, (cuuint64_t)batch};
+  cuuint64_t strides[3] = {(cuuint64_t)row_stride, (cuuint64_t)plane_stride, (cuuint64_t)batch_stride};
+  cuuint32_t box[4] = {(cuuint32_t)box_k, (cuuint32_t)box_rows, (cuuint32_t)box_planes, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUtensorMapSwizzle sw = swz_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                          : swz_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                            : CU_TENSOR_MAP_SWIZZLE_32B;
+  CUresult r = enc(map, dt, 4, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <class Cfg>
+cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params prm, cudaStream_t st,
+                     const char* name) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  prm.tiles_m = (int)((prm.m + Cfg::BM - 1) / Cfg::BM);
+  prm.tiles_n = (int)((prm.n + Cfg::BN - 1) / Cfg::BN);
+  prm.total_tiles = (long)prm.tiles_m * prm.tiles_n * prm.batch;
+  long grid = prm.total_tiles < num_sms() ? prm.total_tiles : num_sms();
+  ProfScope prof(name, st);
+  tc::tc_gemm_kernel<Cfg><<<(unsigned)grid, 192, Cfg::SMEM, st>>>(ta, tb, prm);
+  note_launch();
+  return cudaGetLastError();
+}
+
+tc::Params base_params(const BatchDesc& d) {
+  tc::Params p{};
+  p.m = d.m; p.n = d.n; p.k = d.k; p.batch = d.batch; p.ldc = d.ldc;
+  p.C = d.C;
+  p.c_batch_offset = 0;
+  p.alpha_d = d.alpha_d; p.beta_d = d.beta_d;
+  p.alpha_f = d.alpha_f; p.beta_f = d.beta_f;
+  p.alpha_i = d.alpha_i; p.beta_i = d.beta_i;
+  p.err = device_error_flag();
+  return p;
+}
+
+inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
+
+// int8 planes of op(A) and op(B), K-major, through the pack pre-pass.
+cudaError_t pack_operands_i8(const BatchDesc& d, cudaStream_t st, int8_t** pa, int8_t** pb, long* Kp) {
+  cudaError_t e;
+  *Kp = round_up(d.k, 16);
+  const long sa = d.m * *Kp, sb = d.n * *Kp;
+  *pa = (int8_t*)workspace(WS_PACK_A, (size_t)sa * d.batch, &e);
+  if (!*pa) return e;
+  *pb = (int8_t*)workspace(WS_PACK_B, (size_t)sb * d.batch, &e);
+  if (!*pb) return e;
+  PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, *pa, *Kp, sa, sa};
+  if ((e = launch_pack_i8(a, st)) != cudaSuccess) return e;
+  PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, *pb, *Kp, sb, sb};
+  return launch_pack_i8(b, st);
+}
+
+using CfgI8N256 = tc::Config<tc::KIND_I8, 1, 1, 256, 128, 4, 1, 2, tc::EPI_I32, 0>;
+using CfgI8N128 = tc::Config<tc::KIND_I8, 1, 1, 128, 128, 6, 1, 2, tc::EPI_I32, 0>;
+using CfgBf64 = tc::Config<tc::KIND_BF16, 2, 2, 64, 128, 4, 1, 2, tc::EPI_F32, 1>;
+using CfgBf128 = tc::Config<tc::KIND_BF16, 2, 2, 128, 128, 3, 1, 2, tc::EPI_F32, 1>;
+template <int S> struct OzCfg;
+template <> struct OzCfg<3> { using T = tc::Config<tc::KIND_I8, 3, 3, 64, 32, 8, 3, 1, tc::EPI_OZAKI, 2>; };
+template <> struct OzCfg<4> { using T = tc::Config<tc::KIND_I8, 4, 4, 64, 32, 8, 4, 1, tc::EPI_OZAKI, 2>; };
+template <> struct OzCfg<5> { using T = tc::Config<tc::KIND_I8, 5, 5, 64, 32, 7, 5, 1, tc::EPI_OZAKI, 2>; };
+template <> struct OzCfg<6> { using T = tc::Config<tc::KIND_I8, 6, 6, 64, 32, 6, 6, 1, tc::EPI_OZAKI, 2>; };
+template <> struct OzCfg<7> { using T = tc::Config<tc::KIND_I8, 7, 7, 64, 32, 5, 7, 1, tc::EPI_OZAKI, 2>; };
+template <> struct OzCfg<8> { using T = tc::Config<tc::KIND_I8, 8, 8, 64, 32, 4, 8, 1, tc::EPI_OZAKI, 2>; };
+
+template <int S>
+cudaError_t run_ozaki(const CUtensorMap& ta, const CUtensorMap& tb, const tc::Params& prm, cudaStream_t st) {
+  return run_gemm<typename OzCfg<S>::T>(ta, tb, prm, st, "ozaki_gemm");
+}
+
+}  // namespace
+
+cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t st) {
+  if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
+  if (d.k > (1L << 31) || d.m > (1L << 31) || d.n > (1L << 31)) return cudaErrorNotSupported;
+  CUtensorMap ta, tb;
+  const bool uniform = d.batch == 1 || (d.strideA > 0 && d.strideB > 0);
+  const bool direct = d.transa == SSBLAS_OP_T && d.transb == SSBLAS_OP_N && uniform && d.lda % 16 == 0 &&
+                      d.ldb % 16 == 0 && ((uintptr_t)d.A0 % 16) == 0 && ((uintptr_t)d.B0 % 16) == 0 &&
+                      d.strideA % 16 == 0 && d.strideB % 16 == 0;
+  const int BN = d.n <= 128 ? 128 : 256;
+  bool ok;
+  if (direct) {
+    const long psa = d.batch > 1 ? d.strideA : round_up(d.lda * d.m, 16);
+    const long psb = d.batch > 1 ? d.strideB : round_up(d.ldb * d.n, 16);
+    ok = make_map(&ta, d.A0, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, 1, d.batch, d.lda, psa, psa, 128, 128, 1, 128) &&
+         make_map(&tb, d.B0, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, 1, d.batch, d.ldb, psb, psb, 128, BN, 1, 128);
+  } else {
+    int8_t *pa, *pb;
+    long Kp;
+    cudaError_t e = pack_operands_i8(d, st, &pa, &pb, &Kp);
+    if (e != cudaSuccess) return e;
+    ok = make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, 1, d.batch, Kp, d.m * Kp, d.m * Kp, 128, 128, 1, 128) &&
+         make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, 1, d.batch, Kp, d.n * Kp, d.n * Kp, 128, BN, 1, 128);
+  }
+  if (!ok) return cudaErrorNotSupported;
+  tc::Params prm = base_params(d);
+  note_path(SSBLAS_PATH_I8_TCGEN05);
+  return BN == 128 ? run_gemm<CfgI8N128>(ta, tb, prm, st, "i8_gemm") : run_gemm<CfgI8N256>(ta, tb, prm, st, "i8_gemm");
+}
+
+cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
+  if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
+  // int32 accumulation stays exact while (pairs per level) * k * 2^14 < 2^31
+  if (d.k > 16384 || d.m > (1L << 31) || d.n > (1L << 31)) return cudaErrorNotSupported;
+  const int S = slices == 0 ? 7 : slices;
+  if (S < 3 || S > 8) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const long Kp = round_up(d.k, 16);
+  const long sa = d.m * Kp, sb = d.n * Kp;
+  int8_t* pa = (int8_t*)workspace(WS_PACK_A, (size_t)sa * S * d.batch, &e);
+  if (!pa) return e;
+  int8_t* pb = (int8_t*)workspace(WS_PACK_B, (size_t)sb * S * d.batch, &e);
+  if (!pb) return e;
+  int32_t* ex = (int32_t*)workspace(WS_EXP, sizeof(int32_t) * (size_t)(d.m + d.n) * d.batch, &e);
+  if (!ex) return e;
+  PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * S};
+  PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * S};
+  if ((e = launch_ozaki_slice(a, S, ex, st)) != cudaSuccess) return e;
+  if ((e = launch_ozaki_slice(b, S, ex + d.m * d.batch, st)) != cudaSuccess) return e;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, 32, 128, S, 32) ||
+      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, 32, 64, S, 32))
+    return cudaErrorNotSupported;
+  tc::Params prm = base_params(d);
+  prm.exp_a = ex;
+  prm.exp_b = ex + d.m * d.batch;
+  prm.exp_shift = -12;
+  note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
+  switch (S) {
+    case 3: return run_ozaki<3>(ta, tb, prm, st);
+    case 4: return run_ozaki<4>(ta, tb, prm, st);
+    case 5: return run_ozaki<5>(ta, tb, prm, st);
+    case 6: return run_ozaki<6>(ta, tb, prm, st);
+    case 7: return run_ozaki<7>(ta, tb, prm, st);
+    default: return run_ozaki<8>(ta, tb, prm, st);
+  }
+}
+
+cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
+  if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
+  if (d.m > (1L << 31) || d.n > (1L << 31) || d.k > (1L << 31)) return cudaErrorNotSupported;
+  cudaError_t e;
+  const long Kp = round_up(d.k, 8);
+  const long sa = d.m * Kp * 2, sb = d.n * Kp * 2;   // bytes per plane
+  void* pa = workspace(WS_PACK_A, (size_t)sa * 2 * d.batch, &e);
+  if (!pa) return e;
+  void* pb = workspace(WS_PACK_B, (size_t)sb * 2 * d.batch, &e);
+  if (!pb) return e;
+  PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * 2};
+  PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * 2};
+  if ((e = launch_split_bf16(a, st)) != cudaSuccess) return e;
+  if ((e = launch_split_bf16(b, st)) != cudaSuccess) return e;
+  const int BN = d.n <= 64 ? 64 : 128;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.m, 2, d.batch, Kp * 2, sa, sa * 2, 64, 128, 2, 128) ||
+      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.n, 2, d.batch, Kp * 2, sb, sb * 2, 64, BN, 2, 128))
+    return cudaErrorNotSupported;
+  tc::Params prm = base_params(d);
+  note_path(SSBLAS_PATH_BF16X3_TCGEN05);
+  return BN == 64 ? run_gemm<CfgBf64>(ta, tb, prm, st, "bf16x3_gemm") : run_gemm<CfgBf128>(ta, tb, prm, st, "bf16x3_gemm");
+}
+
+ssblasStatus_t grouped_persistent(const ssblasOperation_t*, const ssblasOperation_t*, const SSINT*, const SSINT*,
+                                  const SSINT*, const void* const*, const void* const*, const ssblasDataType_t*,
+                                  const SSINT*, const void* const*, const ssblasDataType_t*, const SSINT*,
+                                  const void* const*, void* const*, const ssblasDataType_t*, const SSINT*, SSINT,
+                                  const SSINT*) {
   return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
 }
-}
+
+}  // namespace ssb

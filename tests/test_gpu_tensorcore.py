@@ -1,0 +1,132 @@
+"""The tcgen05 paths against their CPU restatements, through the C ABI, on a B200.
+
+  * int8 -> int32 (kind::i8): bit-exact against the reference semantics, on the direct TMA path
+    (op(A)=T, op(B)=N, equally spaced instances) and through the pack pre-pass (every other
+    layout, unequal spacing, odd leading dimensions);
+  * FP64 Ozaki emulation: bit-exact against oracle.ozaki_f64 (the same algorithm on the CPU) for
+    every slice count, and its error against the FP64-exact oracle;
+  * FP32 three-BF16 emulation: within FP32 accumulation error of the FP64-exact value of the
+    same three products, and its stated error against the FP64-exact oracle.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def S():
+    import torch
+    assert torch.cuda.is_available()
+    import ssblasex_b200 as S
+    S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+    S.set_ozaki_slices(0)
+    yield S
+    S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+    S.set_ozaki_slices(0)
+
+
+def run(p, mode="device_array", **kw):
+    from ssblasex_b200 import runner
+    st, C = runner.call(p, mode=mode, **kw)
+    assert st == 0, st
+    return C
+
+
+# ------------------------------------------------------------------------- int8 ------------
+@pytest.mark.parametrize("shape", [(128, 256, 128), (200, 300, 520), (512, 512, 512), (37, 29, 45), (1, 1, 1),
+                                   (130, 40, 2048)])
+def test_i8_direct_tn(S, shape):
+    from ssblasex_b200 import workloads as W
+    m, n, k = shape
+    lda = -(-k // 16) * 16
+    p = W.make_problem("i8", 1, 0, m, n, k, 3, 1, 1, lda=lda, ldb=lda, seed=m + n)
+    C = run(p)
+    assert S.last_run_info()["path"] == "i8_tcgen05"
+    np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 1), (1, 0)])
+def test_i8_packed_layouts(S, ta, tb):
+    from ssblasex_b200 import workloads as W
+    p = W.make_problem("i8", ta, tb, 150, 270, 333, 2, -3, 2, seed=7 + ta + 2 * tb)   # odd ld -> pack path
+    C = run(p)
+    assert S.last_run_info()["path"] == "i8_tcgen05"
+    np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+
+
+def test_i8_unequally_spaced_instances(S):
+    """Host array of device pointers in shuffled order: no uniform stride, so the pack path."""
+    import torch
+    from ssblasex_b200 import runner, workloads as W
+    p = W.make_problem("i8", 1, 0, 64, 96, 256, 4, 1, 0, lda=256, ldb=256, seed=3)
+    dp = runner.DeviceProblem(p)
+    order = [2, 0, 3, 1]
+    A, B, C = (dp.ptrs(t) for t in (dp.A, dp.B, dp.C))
+    arr = [(ct.c_void_p * 4)(*[x[o] for o in order]) for x in (A, B, C)]
+    al, be = np.array([1], np.int32), np.array([0], np.int32)
+    st = S.lib().ssblasGemmBatchedEx(1, 0, 64, 96, 256, al.ctypes.data, arr[0], 0, 256, arr[1], 0, 256,
+                                     be.ctypes.data, arr[2], 3, 64, 4, 0, 0)
+    assert st == 0
+    np.testing.assert_array_equal(dp.C.cpu().numpy(), O.restated_gemm(p)[1])
+
+
+# ------------------------------------------------------------------------- Ozaki -----------
+@pytest.mark.parametrize("slices", [3, 4, 5, 6, 7, 8])
+def test_ozaki_bit_exact_per_slice_count(S, slices):
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_ozaki_slices(slices)
+    p = W.make_problem("f64", 0, 1, 140, 90, 200, 2, 0.75, -1.25, seed=slices, dist="expspread")
+    C = run(p)
+    info = S.last_run_info()
+    assert info["path"] == "ozaki_tcgen05" and info["slices"] == slices
+    st, C_o = O.ozaki_f64(p, slices)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_ozaki_layouts_and_error(S, ta, tb):
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", ta, tb, 257, 70, 1030, 2, 1.0, 0.5, seed=20 + ta + 2 * tb, dist="expspread")
+    C = run(p)
+    st, C_o = O.ozaki_f64(p, 7)
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+    # the default slice count keeps the FP64 bound of the plain path: 4 k u
+    assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
+
+
+def test_ozaki_zero_rows_and_tiny_shapes(S):
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    for (m, n, k) in [(1, 1, 1), (3, 5, 7), (129, 65, 33)]:
+        p = W.make_problem("f64", 1, 1, m, n, k, 2, 2.0, 0.0, seed=m, dist="expspread")
+        p.A[0][: p.lda] = 0.0      # first stored column of A[0] is zero
+        C = run(p)
+        np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
+
+
+# ------------------------------------------------------------------------- 3 x BF16 --------
+@pytest.mark.parametrize("ta,tb,shape", [(1, 1, (64, 64, 64)), (0, 0, (200, 150, 300)), (0, 1, (129, 257, 96)),
+                                         (1, 0, (33, 17, 513))])
+def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP32_BF16X3)
+    m, n, k = shape
+    p = W.make_problem("f32", ta, tb, m, n, k, 2, 0.75, 0.25, seed=k, dist="outliers")
+    C = run(p)
+    assert S.last_run_info()["path"] == "bf16x3_tcgen05"
+    for b in range(p.batch):
+        emu = O.bf16x3_f32(p, b)
+        ex, nrm = O.exact_f64(p, b)
+        got = p.c_view(C, b).astype(np.float64)
+        # same products, FP32 accumulation on the tensor cores
+        assert np.max(np.abs(got - emu) / nrm) <= 4 * k * 2.0 ** -24
+        # stated error of the mode against the FP64-exact result
+        assert np.max(np.abs(got - ex) / nrm) <= 2.0 ** -14

@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--mode", default="auto", choices=["auto", "ozaki", "plain", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch", type=int, default=None,
+                    help="fewer instances than the named workload (profiling runs only)")
     return ap.parse_args()
 
 
@@ -214,7 +216,7 @@ def main():
     from ssblasex_b200 import runner
     from oracle import oracle as O
 
-    p = W.workload(args.workload)
+    p = W.workload(args.workload, batch=args.batch)
     mode = args.mode
     if mode == "auto":
         mode = {"f64": "ozaki", "f32": "plain", "i8": "plain"}[p.row]

@@ -98,76 +98,114 @@ __global__ void __launch_bounds__(NTH) split_bf16_kernel(PlaneArgs a) {
   }
 }
 
-// Balanced base-256 digits of X (|X| < 2^(8S-2)), most significant first.
-template <int S>
-__device__ __forceinline__ void digits(long long X, int8_t (&d)[S]) {
-#pragma unroll
-  for (int p = S - 1; p >= 1; --p) {
-    const long long lo = ((X + 128) & 255) - 128;
-    d[p] = (int8_t)lo;
-    X = (X - lo) >> 8;
-  }
-  d[0] = (int8_t)X;
-}
+// Ozaki slicing. With Y = X + 0x80..80 (128 added to each of the S-1 low bytes), the balanced
+// base-256 digits of X are: d_p = byte_{S-1-p}(Y) - 128 for p >= 1 (that is, the byte with its
+// top bit flipped, read as int8), and d_0 = byte_{S-1}(Y) read as int8 -- the carries of the
+// digit-by-digit recurrence d = ((X + 128) mod 256) - 128, X <- (X - d) / 256 are exactly the
+// carries of the single addition.
+constexpr int ORT = 32;    // rows per work item
+constexpr int OKT = 128;   // k per smem tile
 
 template <int S>
-__global__ void __launch_bounds__(NTH) ozaki_slice_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
-  __shared__ double tile[RT][KT + 1];
-  __shared__ double rmax[RT];
-  __shared__ int rexp[RT];
-  const long b = blockIdx.y;
-  const long row0 = (long)blockIdx.x * RT;
-  const double* X = (const double*)a.X[b];
-  int8_t* out = (int8_t*)a.out + b * a.batch_stride;
-  if (threadIdx.x < RT) rmax[threadIdx.x] = 0.0;
-  __syncthreads();
-  // pass 1: row maxima of |x|
-  for (long k0 = 0; k0 < a.K; k0 += KT) {
-    load_tile<double>(tile, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+__global__ void __launch_bounds__(NTH, 2) ozaki_slice_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
+  __shared__ double tile[ORT][OKT + 1];
+  __shared__ double rmax[ORT];
+  __shared__ double rscale[ORT][2];
+  const long blocks_per_inst = (a.rows + ORT - 1) / ORT;
+  const long total = blocks_per_inst * a.batch;
+  unsigned long long bias = 0;
+#pragma unroll
+  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+
+  // persistent loop: ~2 work items per SM in flight keeps both passes of an item inside L2
+  for (long w = blockIdx.x; w < total; w += gridDim.x) {
+    const long b = w / blocks_per_inst;
+    const long row0 = (w % blocks_per_inst) * ORT;
+    const double* X = (const double*)a.X[b];
+    int8_t* out = (int8_t*)a.out + b * a.batch_stride;
+    if (threadIdx.x < ORT) rmax[threadIdx.x] = 0.0;
     __syncthreads();
-    {
-      const int r = threadIdx.x / 8, part = threadIdx.x % 8;   // 8 threads per row
-      double mx = 0.0;
+    // pass 1: row maxima of |x|
+    for (long k0 = 0; k0 < a.K; k0 += OKT) {
 #pragma unroll
-      for (int j = 0; j < KT / 8; ++j) mx = fmax(mx, fabs(tile[r][part * (KT / 8) + j]));
+      for (int e = 0; e < ORT * OKT / NTH; ++e) {
+        const int idx = threadIdx.x + e * NTH;
+        int r, kk;
+        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
+        else { kk = idx / ORT; r = idx % ORT; }
+        const long gr = row0 + r, gk = k0 + kk;
+        double v = 0.0;
+        if (gr < a.rows && gk < a.K) v = a.kcontig ? X[gr * a.ld + gk] : X[gr + gk * a.ld];
+        tile[r][kk] = fabs(v);
+      }
+      __syncthreads();
+      {
+        const int r = threadIdx.x / 8, part = threadIdx.x % 8;   // 8 threads per row
+        double mx = 0.0;
 #pragma unroll
-      for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (part == 0) rmax[r] = fmax(rmax[r], mx);
+        for (int j = 0; j < OKT / 8; ++j) mx = fmax(mx, tile[r][part * (OKT / 8) + j]);
+#pragma unroll
+        for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (part == 0) rmax[r] = fmax(rmax[r], mx);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x < ORT) {
+      int e = 0;
+      if (rmax[threadIdx.x] > 0.0) frexp(rmax[threadIdx.x], &e);
+      const long gr = row0 + threadIdx.x;
+      if (gr < a.rows) exps[b * a.rows + gr] = e;
+      // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
+      const int sh = 8 * S - 2 - e;
+      const int h1 = sh / 2;
+      rscale[threadIdx.x][0] = ldexp(1.0, h1);
+      rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
     }
     __syncthreads();
-  }
-  if (threadIdx.x < RT) {
-    int e = 0;
-    if (rmax[threadIdx.x] > 0.0) frexp(rmax[threadIdx.x], &e);
-    rexp[threadIdx.x] = e;
-    const long gr = row0 + threadIdx.x;
-    if (gr < a.rows) exps[b * a.rows + gr] = e;
-  }
-  __syncthreads();
-  // pass 2: digits (the rows were just read, so this pass is served from L2)
-  for (long k0 = 0; k0 < a.K; k0 += KT) {
-    load_tile<double>(tile, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
-    __syncthreads();
-    for (int it = threadIdx.x; it < RT * (KT / 4); it += NTH) {
-      const int r = it / (KT / 4), g = it % (KT / 4);
-      const long gr = row0 + r, gk = k0 + 4 * g;
-      if (gr < a.rows && gk < a.Kp) {
-        const int sh = 8 * S - 2 - rexp[r];
-        int8_t dg[4][S];
+    // pass 2: digits (this item's rows were just read, so this pass is served from L2)
+    for (long k0 = 0; k0 < a.K; k0 += OKT) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const long long Xi = __double2ll_rn(scalbn(tile[r][4 * g + j], sh));
-          digits<S>(Xi, dg[j]);
-        }
+      for (int e = 0; e < ORT * OKT / NTH; ++e) {
+        const int idx = threadIdx.x + e * NTH;
+        int r, kk;
+        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
+        else { kk = idx / ORT; r = idx % ORT; }
+        const long gr = row0 + r, gk = k0 + kk;
+        double v = 0.0;
+        if (gr < a.rows && gk < a.K) v = a.kcontig ? X[gr * a.ld + gk] : X[gr + gk * a.ld];
+        tile[r][kk] = v;
+      }
+      __syncthreads();
 #pragma unroll
-        for (int p = 0; p < S; ++p) {
-          const uint32_t w = (uint32_t)(uint8_t)dg[0][p] | ((uint32_t)(uint8_t)dg[1][p] << 8) |
-                             ((uint32_t)(uint8_t)dg[2][p] << 16) | ((uint32_t)(uint8_t)dg[3][p] << 24);
-          *(uint32_t*)(out + p * a.plane_stride + gr * a.Kp + gk) = w;
+      for (int it0 = 0; it0 < ORT * (OKT / 4) / NTH; ++it0) {
+        const int it = threadIdx.x + it0 * NTH;
+        const int r = it / (OKT / 4), g = it % (OKT / 4);
+        const long gr = row0 + r, gk = k0 + 4 * g;
+        if (gr < a.rows && gk < a.Kp) {
+          const double s0 = rscale[r][0], s1 = rscale[r][1];
+          uint32_t lo[4], hi[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const unsigned long long Y = (unsigned long long)__double2ll_rn(tile[r][4 * g + j] * s0 * s1) + bias;
+            lo[j] = (uint32_t)Y;
+            hi[j] = (uint32_t)(Y >> 32);
+          }
+#pragma unroll
+          for (int p = 0; p < S; ++p) {
+            const int byte = S - 1 - p;
+            const uint32_t flip = (p == 0) ? 0u : 0x80808080u;
+            uint32_t wv = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const uint32_t src = byte < 4 ? (lo[j] >> (8 * byte)) : (hi[j] >> (8 * (byte - 4)));
+              wv |= (src & 255u) << (8 * j);
+            }
+            *(uint32_t*)(out + p * a.plane_stride + gr * a.Kp + gk) = wv ^ flip;
+          }
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -193,13 +231,15 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
   ProfScope prof("ozaki_slice", st);
+  const long items = (a.rows + ORT - 1) / ORT * a.batch;
+  const unsigned grid = (unsigned)(items < 2L * num_sms() ? items : 2L * num_sms());
   switch (slices) {
-    case 3: ozaki_slice_kernel<3><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
-    case 4: ozaki_slice_kernel<4><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
-    case 5: ozaki_slice_kernel<5><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
-    case 6: ozaki_slice_kernel<6><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
-    case 7: ozaki_slice_kernel<7><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
-    case 8: ozaki_slice_kernel<8><<<grid_of(a), NTH, 0, st>>>(a, exps); break;
+    case 3: ozaki_slice_kernel<3><<<grid, NTH, 0, st>>>(a, exps); break;
+    case 4: ozaki_slice_kernel<4><<<grid, NTH, 0, st>>>(a, exps); break;
+    case 5: ozaki_slice_kernel<5><<<grid, NTH, 0, st>>>(a, exps); break;
+    case 6: ozaki_slice_kernel<6><<<grid, NTH, 0, st>>>(a, exps); break;
+    case 7: ozaki_slice_kernel<7><<<grid, NTH, 0, st>>>(a, exps); break;
+    case 8: ozaki_slice_kernel<8><<<grid, NTH, 0, st>>>(a, exps); break;
     default: return cudaErrorInvalidValue;
   }
   note_launch();

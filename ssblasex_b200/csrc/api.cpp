@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "grouped.h"
 #include "internal.h"
 
 namespace ssb {
@@ -379,16 +380,82 @@ static ssblasStatus_t check_device_error(cudaStream_t st) {
   return SSBLAS_STATUS_SUCCESS;
 }
 
-// Single-launch grouped path (grouped.cu); returns SSBLAS_STATUS_NOT_COMPUTED_ERROR when the
-// call is not eligible and the per-group loop must run instead.
-ssblasStatus_t grouped_persistent(
+static ssblasStatus_t check_device_error(cudaStream_t st);
+static ssblasStatus_t map_err(cudaError_t e);
+static void* pinned(size_t bytes, cudaError_t* err);
+
+// Grouped call with device-resident matrices: validation of every group (the batched call's
+// rules), pointer arrays made device-resident, then grouped_run (grouped.cu). Returns
+// SSBLAS_STATUS_NOT_COMPUTED_ERROR when the matrices are in host memory, which the caller then
+// stages group by group.
+static ssblasStatus_t grouped_device(
     const ssblasOperation_t transa_array[], const ssblasOperation_t transb_array[],
     const SSINT m_array[], const SSINT n_array[], const SSINT k_array[],
     const void* const alpha_array[], const void* const A[], const ssblasDataType_t Atype_array[],
     const SSINT lda_array[], const void* const B[], const ssblasDataType_t Btype_array[],
     const SSINT ldb_array[], const void* const beta_array[], void* const C[],
     const ssblasDataType_t Ctype_array[], const SSINT ldc_array[], SSINT group_count,
-    const SSINT group_size[]);
+    const SSINT group_size[]) {
+  GroupedDesc g;
+  long total = 0;
+  for (SSINT gi = 0; gi < group_count; ++gi) {
+    Rowsel rs = select_row(Atype_array[gi], Btype_array[gi], Ctype_array[gi]);
+    if (!rs.ok) return SSBLAS_STATUS_INVALID_VALUE;
+    const int ta = transa_array[gi], tb = transb_array[gi];
+    if ((ta != SSBLAS_OP_N && ta != SSBLAS_OP_T) || (tb != SSBLAS_OP_N && tb != SSBLAS_OP_T))
+      return SSBLAS_STATUS_INVALID_VALUE;
+    const long m = m_array[gi], n = n_array[gi], k = k_array[gi];
+    if (m <= 0 || n <= 0 || group_size[gi] <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
+    if (!alpha_array[gi] || !beta_array[gi]) return SSBLAS_STATUS_INVALID_VALUE;
+    const long arows = (ta == SSBLAS_OP_N) ? m : k, brows = (tb == SSBLAS_OP_N) ? k : n;
+    if (k > 0 && (lda_array[gi] < arows || ldb_array[gi] < brows)) return SSBLAS_STATUS_INVALID_VALUE;
+    if (ldc_array[gi] < m) return SSBLAS_STATUS_INVALID_VALUE;
+    GroupedInst in{};
+    in.row = rs.row; in.transa = ta; in.transb = tb;
+    in.m = m; in.n = n; in.k = k; in.lda = lda_array[gi]; in.ldb = ldb_array[gi]; in.ldc = ldc_array[gi];
+    if (rs.row == ROW_F32) { in.alpha_f = *(const float*)alpha_array[gi]; in.beta_f = *(const float*)beta_array[gi]; }
+    else if (rs.row == ROW_F64) { in.alpha_d = *(const double*)alpha_array[gi]; in.beta_d = *(const double*)beta_array[gi]; }
+    else { in.alpha_i = *(const int32_t*)alpha_array[gi]; in.beta_i = *(const int32_t*)beta_array[gi]; }
+    for (SSINT j = 0; j < group_size[gi]; ++j) {
+      in.idx = total++;
+      g.inst.push_back(in);
+    }
+  }
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_info = ssblasRunInfo_t{};
+  cudaStream_t st = settings().stream;
+  cudaError_t e;
+  const bool dev_arrays = kind_of((const void*)A) == PK_DEVICE;
+  if (dev_arrays) {
+    if (kind_of((const void*)B) != PK_DEVICE || kind_of((const void*)C) != PK_DEVICE)
+      return SSBLAS_STATUS_INVALID_VALUE;
+    g.A = A; g.B = B; g.C = C;
+  } else {
+    if (kind_of((const void*)B) == PK_DEVICE || kind_of((const void*)C) == PK_DEVICE)
+      return SSBLAS_STATUS_INVALID_VALUE;
+    if (kind_of(A[0]) != PK_DEVICE) return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
+    if (kind_of(B[0]) != PK_DEVICE || kind_of(C[0]) != PK_DEVICE) return SSBLAS_STATUS_INVALID_VALUE;
+    void* h = pinned(3 * sizeof(void*) * total, &e);
+    if (!h) return map_err(e);
+    void** hp = (void**)h;
+    memcpy(hp, A, sizeof(void*) * total);
+    memcpy(hp + total, B, sizeof(void*) * total);
+    memcpy(hp + 2 * total, C, sizeof(void*) * total);
+    void** dp = (void**)workspace(WS_PTRS, 3 * sizeof(void*) * total, &e);
+    if (!dp) return map_err(e);
+    if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * total, cudaMemcpyHostToDevice, st))) return map_err(e);
+    cudaEventRecord(g_pin.done, st);
+    g.A = (const void* const*)dp;
+    g.B = (const void* const*)(dp + total);
+    g.C = (void* const*)(dp + 2 * total);
+  }
+  if ((e = grouped_run(g, st)) != cudaSuccess) return map_err(e);
+  if (settings().synchronous) {
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return map_err(e);
+    return check_device_error(st);
+  }
+  return SSBLAS_STATUS_SUCCESS;
+}
 
 static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
                                    SSINT n, SSINT k, const void* alpha, const void* const A[],
@@ -568,11 +635,12 @@ ssblasStatus_t ssblasGemmGroupedBatchedEx(
       !Atype_array || !lda_array || !B || !Btype_array || !ldb_array || !beta_array || !C ||
       !Ctype_array || !ldc_array || !group_size)
     return SSBLAS_STATUS_INVALID_VALUE;
-  ssblasStatus_t st = grouped_persistent(transa_array, transb_array, m_array, n_array, k_array,
-                                         alpha_array, A, Atype_array, lda_array, B, Btype_array,
-                                         ldb_array, beta_array, C, Ctype_array, ldc_array,
-                                         group_count, group_size);
+  ssblasStatus_t st = grouped_device(transa_array, transb_array, m_array, n_array, k_array,
+                                     alpha_array, A, Atype_array, lda_array, B, Btype_array,
+                                     ldb_array, beta_array, C, Ctype_array, ldc_array, group_count,
+                                     group_size);
   if (st != SSBLAS_STATUS_NOT_COMPUTED_ERROR) return st;
+  // host matrices (the reference's convention): each group through the batched path
   long off = 0;
   for (SSINT g = 0; g < group_count; ++g) {
     if (group_size[g] <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
@@ -658,6 +726,7 @@ ssblasStatus_t ssblasGetProfile(ssblasKernelProfile_t* out, int max_entries, int
 ssblasStatus_t ssblasReleaseWorkspace(void) {
   std::lock_guard<std::mutex> lock(g_mutex);
   release_workspace();
+  grouped_release();
   return SSBLAS_STATUS_SUCCESS;
 }
 

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "grouped.h"
 #include "internal.h"
 
 namespace ssb {
@@ -59,9 +60,9 @@ struct SimtArgs {
 };
 
 // BM x BN tile, BK deep; NT threads; each thread TM x TN outputs.
+// One BM x BN tile of instance b at (m0, n0).
 template <typename T, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
-simt_gemm_kernel(SimtArgs<T> args) {
+__device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long m0, long n0) {
   using Tr = RowTraits<T>;
   using AB = typename Tr::AB;
   using Acc = typename Tr::Acc;
@@ -77,11 +78,7 @@ simt_gemm_kernel(SimtArgs<T> args) {
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const long tiles_m = (args.m + BM - 1) / BM;
-  const long m0 = (blockIdx.x % tiles_m) * BM;
-  const long n0 = (blockIdx.x / tiles_m) * BN;
-
-  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) {
+  {
     const AB* __restrict__ A = args.A[b];
     const AB* __restrict__ B = args.B[b];
 
@@ -179,6 +176,30 @@ simt_gemm_kernel(SimtArgs<T> args) {
 }
 
 template <typename T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) simt_gemm_kernel(SimtArgs<T> args) {
+  const long tiles_m = (args.m + BM - 1) / BM;
+  const long m0 = (blockIdx.x % tiles_m) * BM;
+  const long n0 = (blockIdx.x / tiles_m) * BN;
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) simt_tile<T, BM, BN, BK, TM, TN>(args, b, m0, n0);
+}
+
+// Grouped form: one CTA per (instance, tile) entry of the tile table.
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+simt_grouped_kernel(const SimtGInst* __restrict__ inst, const int* __restrict__ tiles, const T* const* A,
+                    const T* const* B, typename RowTraits<T>::C* const* C) {
+  const int* t = tiles + 3 * (long)blockIdx.x;
+  const SimtGInst g = inst[t[0]];
+  SimtArgs<T> a;
+  a.transa = g.transa; a.transb = g.transb;
+  a.m = g.m; a.n = g.n; a.k = g.k; a.lda = g.lda; a.ldb = g.ldb; a.ldc = g.ldc; a.batch = 1;
+  a.A = A; a.B = B; a.C = C;
+  if constexpr (sizeof(T) == 8) { a.alpha = g.alpha_d; a.beta = g.beta_d; }
+  else { a.alpha = g.alpha_f; a.beta = g.beta_f; }
+  simt_tile<T, BM, BN, BK, TM, TN>(a, g.idx, (long)t[1] * BM, (long)t[2] * BN);
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN>
 cudaError_t launch_tile(const SimtArgs<T>& a, cudaStream_t stream) {
   long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
   if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
@@ -225,6 +246,65 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
     }
   }
   return cudaErrorInvalidValue;
+}
+
+GroupedSimt::~GroupedSimt() {
+  for (void* p : {inst32, tiles32, inst64, tiles64})
+    if (p) cudaFree(p);
+}
+
+cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& members, GroupedSimt& out,
+                              cudaStream_t st) {
+  std::vector<SimtGInst> in32, in64;
+  std::vector<int> t32, t64;
+  for (int id : members) {
+    const GroupedInst& x = g.inst[id];
+    SimtGInst s{x.transa, x.transb, x.m, x.n, x.k, x.lda, x.ldb, x.ldc, x.idx, x.alpha_d, x.beta_d, x.alpha_f, x.beta_f};
+    auto& iv = (x.row == ROW_F64) ? in64 : in32;
+    auto& tv = (x.row == ROW_F64) ? t64 : t32;
+    const int li = (int)iv.size();
+    iv.push_back(s);
+    for (long a = 0; a < (x.m + 63) / 64; ++a)
+      for (long b = 0; b < (x.n + 63) / 64; ++b) {
+        tv.push_back(li);
+        tv.push_back((int)a);
+        tv.push_back((int)b);
+      }
+  }
+  cudaError_t e;
+  auto up = [&](void** dst, const void* src, size_t n) -> cudaError_t {
+    if (n == 0) return cudaSuccess;
+    cudaError_t r = cudaMalloc(dst, n);
+    if (r) return r;
+    return cudaMemcpyAsync(*dst, src, n, cudaMemcpyHostToDevice, st);
+  };
+  if ((e = up(&out.inst32, in32.data(), in32.size() * sizeof(SimtGInst))) ||
+      (e = up(&out.tiles32, t32.data(), t32.size() * sizeof(int))) ||
+      (e = up(&out.inst64, in64.data(), in64.size() * sizeof(SimtGInst))) ||
+      (e = up(&out.tiles64, t64.data(), t64.size() * sizeof(int))))
+    return e;
+  out.ntiles32 = (long)t32.size() / 3;
+  out.ntiles64 = (long)t64.size() / 3;
+  out.A = g.A; out.B = g.B; out.C = g.C;
+  out.launches = (out.ntiles32 ? 1 : 0) + (out.ntiles64 ? 1 : 0);
+  return cudaStreamSynchronize(st);
+}
+
+cudaError_t launch_simt_grouped(const GroupedSimt& s, cudaStream_t st) {
+  ProfScope prof("simt_grouped", st);
+  if (s.ntiles32) {
+    simt_grouped_kernel<float, 64, 64, 16, 4, 4><<<(unsigned)s.ntiles32, 256, 0, st>>>(
+        (const SimtGInst*)s.inst32, (const int*)s.tiles32, (const float* const*)s.A, (const float* const*)s.B,
+        (float* const*)s.C);
+    note_launch();
+  }
+  if (s.ntiles64) {
+    simt_grouped_kernel<double, 64, 64, 16, 4, 4><<<(unsigned)s.ntiles64, 256, 0, st>>>(
+        (const SimtGInst*)s.inst64, (const int*)s.tiles64, (const double* const*)s.A, (const double* const*)s.B,
+        (double* const*)s.C);
+    note_launch();
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace ssb

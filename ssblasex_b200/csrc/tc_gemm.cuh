@@ -32,6 +32,25 @@ namespace tc {
 enum Kind { KIND_I8 = 0, KIND_BF16 = 1 };
 enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2 };
 
+// Grouped launches: one entry per instance ...
+struct GInst {
+  long m, n, k;
+  long ldc;
+  long idx;                 // position of the instance in the caller's A/B/C pointer arrays
+  long offA, offB;          // byte offsets of its packed operand tiles
+  long offEA, offEB;        // element offsets of its Ozaki exponents
+  int nk;                   // K blocks (stages) per tile
+  int tiles_n;
+  double alpha_d, beta_d;
+  float alpha_f, beta_f;
+  int32_t alpha_i, beta_i;
+};
+// ... and one per output tile, longest K first.
+struct GTile {
+  int inst;
+  int mt, nt;
+};
+
 struct Params {
   long m, n, k;             // GEMM shape (k in elements)
   long batch;
@@ -47,7 +66,36 @@ struct Params {
   const int32_t* exp_b;     // Ozaki: per-column exponents of op(B), [batch][n]
   int exp_shift;            // Ozaki: result = alpha * 2^(ea+eb+exp_shift) * sum_l acc_l 2^(-8 l)
   int* err;                 // device error flag
+  // grouped launches only: operands come pre-tiled (already swizzled) from packA/packB and are
+  // staged with plain bulk copies; shapes and scalars come from the instance table
+  const GInst* ginst;
+  const GTile* gtiles;
+  const uint8_t* packA;
+  const uint8_t* packB;
 };
+
+struct TileInfo {
+  int b, mt, nt, nk;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ TileInfo tile_info(const Params& p, long t, long tiles_mn, int nk) {
+  TileInfo ti;
+  if constexpr (GROUPED) {
+    const GTile g = p.gtiles[t];
+    ti.b = g.inst;
+    ti.mt = g.mt;
+    ti.nt = g.nt;
+    ti.nk = p.ginst[g.inst].nk;
+  } else {
+    ti.b = (int)(t / tiles_mn);
+    const long r = t % tiles_mn;
+    ti.mt = (int)(r / p.tiles_n);
+    ti.nt = (int)(r % p.tiles_n);
+    ti.nk = nk;
+  }
+  return ti;
+}
 
 template <int KIND_, int PA_, int PB_, int BN_, int KB_, int STAGES_, int NLEV_, int ACCB_, int EPI_, int PAIRS_>
 struct Config {
@@ -84,7 +132,7 @@ struct Config {
   }
 };
 
-template <class Cfg>
+template <class Cfg, bool GROUPED>
 __global__ void __launch_bounds__(192, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
   extern __shared__ uint8_t smem_raw[];
@@ -114,7 +162,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     ptx::mbar_init(ptx::smem_u32(drain), 1);
     ptx::fence_mbar_init();
   }
-  if (warp == 0 && lane == 0) {
+  if (!GROUPED && warp == 0 && lane == 0) {
     ptx::prefetch_tmap(&tmA);
     ptx::prefetch_tmap(&tmB);
   }
@@ -129,26 +177,36 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
   const long tiles_mn = (long)prm.tiles_m * prm.tiles_n;
   const int KE = Cfg::KB / Cfg::ELEM;                       // K elements per stage
-  const int nk = (int)((prm.k + KE - 1) / KE);
+  const int nk_uniform = GROUPED ? 0 : (int)((prm.k + KE - 1) / KE);
 
   if (warp == 0) {
-    // ------------------------------------------------------------------ TMA producer ------
+    // ------------------------------------------------------------------ producer ----------
     if (lane == 0) {
       long it = 0;
       bool ok = true;
       for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x) {
-        const int b = (int)(t / tiles_mn);
-        const long r = t % tiles_mn;
-        const int mt = (int)(r / prm.tiles_n), nt = (int)(r % prm.tiles_n);
-        for (int kb = 0; kb < nk; ++kb, ++it) {
+        const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
+        const uint8_t* srcA = nullptr;
+        const uint8_t* srcB = nullptr;
+        if constexpr (GROUPED) {
+          const GInst& gi = prm.ginst[ti.b];
+          srcA = prm.packA + gi.offA + (size_t)ti.mt * ti.nk * Cfg::A_STAGE;
+          srcB = prm.packB + gi.offB + (size_t)ti.nt * ti.nk * Cfg::B_STAGE;
+        }
+        for (int kb = 0; kb < ti.nk; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
           if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11)) { ok = false; break; }
           const uint32_t fb = ptx::smem_u32(&full[s]);
           ptx::mbar_arrive_expect_tx(fb, Cfg::STAGE);
           uint8_t* sa = stages + (size_t)s * Cfg::STAGE;
-          ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, mt * Cfg::BM, 0, b);
-          ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, nt * Cfg::BN, 0, b);
+          if constexpr (GROUPED) {
+            ptx::bulk_load(ptx::smem_u32(sa), srcA + (size_t)kb * Cfg::A_STAGE, Cfg::A_STAGE, fb);
+            ptx::bulk_load(ptx::smem_u32(sa + Cfg::A_STAGE), srcB + (size_t)kb * Cfg::B_STAGE, Cfg::B_STAGE, fb);
+          } else {
+            ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, ti.mt * Cfg::BM, 0, ti.b);
+            ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, ti.nt * Cfg::BN, 0, ti.b);
+          }
         }
       }
       // no copy may still be in flight when the CTA exits
@@ -164,12 +222,13 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       int tcount = 0;
       bool ok = true;
       for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x, ++tcount) {
+        const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
         const int acc = tcount % Cfg::ACCB;
         const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
         if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21)) { ok = false; break; }
         ptx::tc_fence_after();
         const uint32_t d_base = tmem_base + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
-        for (int kb = 0; kb < nk; ++kb, ++it) {
+        for (int kb = 0; kb < ti.nk; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
           if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), ph, err, 22)) { ok = false; break; }
@@ -206,22 +265,38 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int row_in_tile = quarter * 32 + lane;
     int tcount = 0;
     for (long t = blockIdx.x; t < prm.total_tiles; t += gridDim.x, ++tcount) {
-      const int b = (int)(t / tiles_mn);
-      const long r = t % tiles_mn;
-      const int mt = (int)(r / prm.tiles_n), nt = (int)(r % prm.tiles_n);
+      const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
+      long m = prm.m, n = prm.n, ldc = prm.ldc;
+      double alpha_d = prm.alpha_d, beta_d = prm.beta_d;
+      float alpha_f = prm.alpha_f, beta_f = prm.beta_f;
+      int32_t alpha_i = prm.alpha_i, beta_i = prm.beta_i;
+      const int32_t* exa = prm.exp_a + (long)ti.b * prm.m;
+      const int32_t* exb = prm.exp_b + (long)ti.b * prm.n;
+      uint8_t* Cb;
+      if constexpr (GROUPED) {
+        const GInst& g = prm.ginst[ti.b];
+        m = g.m; n = g.n; ldc = g.ldc;
+        alpha_d = g.alpha_d; beta_d = g.beta_d; alpha_f = g.alpha_f; beta_f = g.beta_f;
+        alpha_i = g.alpha_i; beta_i = g.beta_i;
+        exa = prm.exp_a + g.offEA;
+        exb = prm.exp_a + g.offEB;
+        Cb = (uint8_t*)prm.C[g.idx];
+      } else {
+        Cb = (uint8_t*)prm.C[ti.b + prm.c_batch_offset];
+      }
       const int acc = tcount % Cfg::ACCB;
       const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
       if (!ptx::mbar_wait(ptx::smem_u32(&tfull[acc]), acc_ph, err, 31)) break;
       ptx::tc_fence_after();
-      const long gi = (long)mt * Cfg::BM + row_in_tile;
-      const long n0 = (long)nt * Cfg::BN;
+      const long gi = (long)ti.mt * Cfg::BM + row_in_tile;
+      const long n0 = (long)ti.nt * Cfg::BN;
       const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
-      const bool row_ok = gi < prm.m;
-      uint8_t* Cb = (uint8_t*)prm.C[b + prm.c_batch_offset];
+      const bool row_ok = gi < m;
       int32_t ea = 0;
-      if (Cfg::EPI == EPI_OZAKI && row_ok) ea = prm.exp_a[(long)b * prm.m + gi];
+      if (Cfg::EPI == EPI_OZAKI && row_ok) ea = exa[gi];
 #pragma unroll 1
       for (int c0 = 0; c0 < Cfg::BN; c0 += 16) {
+        if (n0 + c0 >= n) break;   // whole chunk outside C: nothing to read or write
         if (Cfg::EPI == EPI_OZAKI) {
           double v[16];
 #pragma unroll
@@ -239,12 +314,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const long gj = n0 + c0 + j;
-              if (gj < prm.n) {
-                const int32_t eb = prm.exp_b[(long)b * prm.n + gj];
-                const double w = scalbn(v[j], ea + eb + prm.exp_shift);
-                double* cp = Cd + gi + gj * prm.ldc;
-                const double tb = (prm.beta_d == 0.0) ? 0.0 : prm.beta_d * (*cp);
-                *cp = fma(w, prm.alpha_d, tb);
+              if (gj < n) {
+                const double w = scalbn(v[j], ea + exb[gj] + prm.exp_shift);
+                double* cp = Cd + gi + gj * ldc;
+                const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+                *cp = fma(w, alpha_d, tb);
               }
             }
           }
@@ -255,25 +329,24 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           if (row_ok) {
             if (Cfg::EPI == EPI_I32) {
               int32_t* Ci = (int32_t*)Cb;
-              if (prm.beta_i == 0) {
+              if (beta_i == 0) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                   const long gj = n0 + c0 + j;
-                  if (gj < prm.n) Ci[gi + gj * prm.ldc] = (int32_t)(raw[j] * (uint32_t)prm.alpha_i);
+                  if (gj < n) __stcs(Ci + gi + gj * ldc, (int32_t)(raw[j] * (uint32_t)alpha_i));
                 }
               } else {
                 uint32_t cv[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                   const long gj = n0 + c0 + j;
-                  cv[j] = (gj < prm.n) ? (uint32_t)__ldcs(Ci + gi + gj * prm.ldc) : 0u;
+                  cv[j] = (gj < n) ? (uint32_t)__ldcs(Ci + gi + gj * ldc) : 0u;
                 }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                   const long gj = n0 + c0 + j;
-                  if (gj < prm.n)
-                    __stcs(Ci + gi + gj * prm.ldc,
-                           (int32_t)((uint32_t)prm.beta_i * cv[j] + raw[j] * (uint32_t)prm.alpha_i));
+                  if (gj < n)
+                    __stcs(Ci + gi + gj * ldc, (int32_t)((uint32_t)beta_i * cv[j] + raw[j] * (uint32_t)alpha_i));
                 }
               }
             } else {
@@ -281,10 +354,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
                 const long gj = n0 + c0 + j;
-                if (gj < prm.n) {
-                  float* cp = Cf + gi + gj * prm.ldc;
-                  const float tb = (prm.beta_f == 0.0f) ? 0.0f : prm.beta_f * (*cp);
-                  *cp = fmaf(__uint_as_float(raw[j]), prm.alpha_f, tb);
+                if (gj < n) {
+                  float* cp = Cf + gi + gj * ldc;
+                  const float tb = (beta_f == 0.0f) ? 0.0f : beta_f * (*cp);
+                  *cp = fmaf(__uint_as_float(raw[j]), alpha_f, tb);
                 }
               }
             }

@@ -64,7 +64,7 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
                      const char* name) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
@@ -73,7 +73,7 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   prm.total_tiles = (long)prm.tiles_m * prm.tiles_n * prm.batch;
   long grid = prm.total_tiles < num_sms() ? prm.total_tiles : num_sms();
   ProfScope prof(name, st);
-  tc::tc_gemm_kernel<Cfg><<<(unsigned)grid, 192, Cfg::SMEM, st>>>(ta, tb, prm);
+  tc::tc_gemm_kernel<Cfg, false><<<(unsigned)grid, 192, Cfg::SMEM, st>>>(ta, tb, prm);
   note_launch();
   return cudaGetLastError();
 }
@@ -215,14 +215,6 @@ cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   tc::Params prm = base_params(d);
   note_path(SSBLAS_PATH_BF16X3_TCGEN05);
   return BN == 64 ? run_gemm<CfgBf64>(ta, tb, prm, st, "bf16x3_gemm") : run_gemm<CfgBf128>(ta, tb, prm, st, "bf16x3_gemm");
-}
-
-ssblasStatus_t grouped_persistent(const ssblasOperation_t*, const ssblasOperation_t*, const SSINT*, const SSINT*,
-                                  const SSINT*, const void* const*, const void* const*, const ssblasDataType_t*,
-                                  const SSINT*, const void* const*, const ssblasDataType_t*, const SSINT*,
-                                  const void* const*, void* const*, const ssblasDataType_t*, const SSINT*, SSINT,
-                                  const SSINT*) {
-  return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
 }
 
 }  // namespace ssb

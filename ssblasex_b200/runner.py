@@ -104,3 +104,50 @@ def call(p: Problem, mode: str = "device_array", dp: DeviceProblem | None = None
     else:
         raise ValueError(mode)
     return st, dp.C.cpu().numpy()
+
+
+class GroupedDevice:
+    """Device copies of a list of single-instance Problems, packed into one buffer per dtype,
+    plus the per-group argument arrays of ssblasGemmGroupedBatchedEx (one group per problem)."""
+
+    def __init__(self, probs, device="cuda"):
+        torch = _torch()
+        self.probs = probs
+        self.device = device
+        self.tensors = []
+        ptrs = {"A": [], "B": [], "C": []}
+        for p in probs:
+            a = torch.from_numpy(p.A[0]).to(device)
+            b = torch.from_numpy(p.B[0]).to(device)
+            c = torch.from_numpy(p.C[0]).to(device)
+            self.tensors.append((a, b, c))
+            ptrs["A"].append(a.data_ptr()); ptrs["B"].append(b.data_ptr()); ptrs["C"].append(c.data_ptr())
+        G = len(probs)
+        L = lambda xs: np.array(xs, dtype=np.int64)
+        I = lambda xs: np.array(xs, dtype=np.int32)
+        self.ta = I([p.transa for p in probs]); self.tb = I([p.transb for p in probs])
+        self.m = L([p.m for p in probs]); self.n = L([p.n for p in probs]); self.k = L([p.k for p in probs])
+        self.lda = L([p.lda for p in probs]); self.ldb = L([p.ldb for p in probs]); self.ldc = L([p.ldc for p in probs])
+        self.at = I([p.types[0] for p in probs]); self.bt = I([p.types[1] for p in probs]); self.ct = I([p.types[2] for p in probs])
+        self.gs = L([1] * G)
+        self.scal = [(np.array([p.alpha], dtype=p.scale_dtype), np.array([p.beta], dtype=p.scale_dtype)) for p in probs]
+        self.alpha = (ct.c_void_p * G)(*[s[0].ctypes.data for s in self.scal])
+        self.beta = (ct.c_void_p * G)(*[s[1].ctypes.data for s in self.scal])
+        self.host_ptrs = {k: (ct.c_void_p * G)(*v) for k, v in ptrs.items()}
+        self.dev_ptrs = {k: torch.tensor(v, dtype=torch.int64, device=device) for k, v in ptrs.items()}
+
+    def reset_c(self):
+        torch = _torch()
+        for p, (_, _, c) in zip(self.probs, self.tensors):
+            c.copy_(torch.from_numpy(p.C[0]))
+
+    def call(self, device_arrays: bool = True) -> int:
+        d = (lambda k: self.dev_ptrs[k].data_ptr()) if device_arrays else (lambda k: ct.addressof(self.host_ptrs[k]))
+        a = lambda arr: arr.ctypes.data
+        return lib().ssblasGemmGroupedBatchedEx(
+            a(self.ta), a(self.tb), a(self.m), a(self.n), a(self.k), ct.addressof(self.alpha), d("A"), a(self.at),
+            a(self.lda), d("B"), a(self.bt), a(self.ldb), ct.addressof(self.beta), d("C"), a(self.ct), a(self.ldc),
+            len(self.probs), a(self.gs), 0, 0)
+
+    def results(self):
+        return [c.cpu().numpy()[None, :] for (_, _, c) in self.tensors]

@@ -189,3 +189,23 @@ def grouped_sizes(count: int = 10000, seed: int = 5, lo: int = 8, hi: int = 512)
     dims = np.clip(dims, lo, hi)
     trans = rng.integers(0, 2, size=(count, 2))
     return dims, trans
+
+
+def grouped_problems(count: int = 10000, seed: int = 5, lo: int = 8, hi: int = 512,
+                     fp64_fraction: float = 0.5) -> list[Problem]:
+    """The uneven grouped workload: `count` single-instance problems with m, n, k log-uniform
+    integers in [lo, hi], op N/T uniform, ld = stored rows rounded up to a multiple of 8, entries
+    U[-1,1), alpha 1, beta 0; the first fp64_fraction of them fp64, the rest fp32."""
+    dims, trans = grouped_sizes(count, seed, lo, hi)
+    out = []
+    n64 = int(round(count * fp64_fraction))
+    for i in range(count):
+        m, n, k = (int(x) for x in dims[i])
+        ta, tb = (int(x) for x in trans[i])
+        ar, _ = stored_shape(ta, m, k)
+        br, _ = stored_shape(tb, k, n)
+        r8 = lambda x: (x + 7) // 8 * 8
+        out.append(make_problem("f64" if i < n64 else "f32", ta, tb, m, n, k, 1, 1.0, 0.0,
+                                lda=r8(ar), ldb=r8(br), ldc=r8(m), seed=seed * 100003 + i,
+                                name=f"g{i}"))
+    return out

@@ -1,0 +1,75 @@
+"""ssblasGemmGroupedBatchedEx on a B200: uneven instances of every kind in one call, each checked
+against its CPU restatement (Ozaki bit-exact, int8 bit-exact, BF16x3 and plain fp within their
+bounds), first as a fresh plan and then as a replayed CUDA graph."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed(count=60, seed=9):
+    from ssblasex_b200 import workloads as W
+    probs = W.grouped_problems(count=count, seed=seed, lo=1, hi=300)
+    rng = np.random.default_rng(seed)
+    # a few int8 instances and non-zero beta to cover every epilogue
+    for i in range(0, count, 7):
+        p = probs[i]
+        probs[i] = W.make_problem("i8", p.transa, p.transb, p.m, p.n, p.k, 1, 2, -1, seed=seed + i)
+    for i in range(3, count, 11):
+        p = probs[i]
+        probs[i] = W.make_problem(p.row, p.transa, p.transb, p.m, p.n, p.k, 1, 0.5, 1.5, seed=seed + 1000 + i)
+    return probs
+
+
+def _check(p, C, mode):
+    if p.row == "i8":
+        np.testing.assert_array_equal(C, O.restated_gemm(p)[1], err_msg=p.name)
+    elif p.row == "f64" and mode & 1:
+        np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64), err_msg=p.name)
+    elif p.row == "f32" and mode & 2:
+        emu = O.bf16x3_f32(p, 0)
+        ex, nrm = O.exact_f64(p, 0)
+        got = p.c_view(C, 0).astype(np.float64)
+        assert np.max(np.abs(got - emu) / nrm) <= 4 * p.k * 2.0 ** -24, p.name
+    else:
+        u = 2.0 ** -24 if p.row == "f32" else 2.0 ** -53
+        assert O.normalized_error(p, C) <= 4 * p.k * u, p.name
+
+
+@pytest.mark.parametrize("mode", [0, 3])
+@pytest.mark.parametrize("device_arrays", [True, False])
+def test_grouped_mixed_kinds(mode, device_arrays):
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner
+    S.set_math_mode(mode)
+    try:
+        probs = _mixed()
+        gd = runner.GroupedDevice(probs)
+        for rep in range(3):            # plan, capture, replay
+            gd.reset_c()
+            assert gd.call(device_arrays=device_arrays) == 0
+            res = gd.results()
+            for p, C in zip(probs, res):
+                _check(p, C, mode)
+        assert S.last_run_info()["path"] == "grouped"
+    finally:
+        S.set_math_mode(0)
+
+
+def test_grouped_status_conventions():
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    probs = [W.make_problem("f32", 0, 0, 5, 4, 3, 1, 1.0, 0.0, seed=1) for _ in range(3)]
+    gd = runner.GroupedDevice(probs)
+    gd.m[1] = 0
+    assert gd.call() == S.SSBLAS_STATUS_INTERNAL_ERROR
+    gd.m[1] = 5
+    gd.ta[2] = 2
+    assert gd.call() == S.SSBLAS_STATUS_INVALID_VALUE
+    gd.ta[2] = 0
+    gd.k[0] = 0                        # k = 0: that instance's C stays untouched
+    gd.reset_c()
+    assert gd.call() == 0
+    np.testing.assert_array_equal(gd.results()[0], probs[0].C)

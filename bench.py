@@ -21,6 +21,7 @@ over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes as ct
 import json
 import os
 import pathlib
@@ -46,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="f64_batch32_1024", choices=list(W.WORKLOADS))
+    ap.add_argument("--workload", default="f64_batch32_1024", choices=list(W.WORKLOADS) + ["grouped_10000"])
     ap.add_argument("--mode", default="auto", choices=["auto", "ozaki", "plain", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -195,10 +196,70 @@ def run_reference_arm(args):
     return 0
 
 
+def run_grouped(args):
+    """10,000 uneven GEMMs (m, n, k log-uniform in [8, 512]; half fp64 in the Ozaki mode, half
+    fp32 in the 3xBF16 mode) through one ssblasGemmGroupedBatchedEx call per step (pre-pass and
+    persistent GEMM launches replayed from a CUDA graph), against the same instances as one plain
+    ssblasGemmBatchedEx launch each (asynchronous, back to back)."""
+    import torch
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner
+    count = args.batch or 10000
+    probs = W.grouped_problems(count=count)
+    flops = sum(2.0 * p.m * p.n * p.k for p in probs)
+    gd = runner.GroupedDevice(probs)
+    stream = torch.cuda.Stream()
+    S.set_stream(stream.cuda_stream)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, (time.perf_counter() - t0) * 1e3 / steps
+
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI | S.SSBLAS_MATH_FP32_BF16X3)
+    S.set_sync_mode(False)
+    ms_g, wall_g = timed(lambda: gd.call(device_arrays=True), args.steps, args.warmup)
+    launches = S.last_run_info()["kernel_launches"]
+    # one plain launch per instance
+    S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+    calls = []
+    for p, (a, b, c) in zip(probs, gd.tensors):
+        arrs = [(ct.c_void_p * 1)(t.data_ptr()) for t in (a, b, c)]
+        al, be = np.array([p.alpha], p.scale_dtype), np.array([p.beta], p.scale_dtype)
+        calls.append((p, arrs, al, be))
+
+    def loop():
+        for p, arrs, al, be in calls:
+            S.lib().ssblasGemmBatchedEx(p.transa, p.transb, p.m, p.n, p.k, al.ctypes.data, arrs[0], p.types[0],
+                                        p.lda, arrs[1], p.types[1], p.ldb, be.ctypes.data, arrs[2], p.types[2],
+                                        p.ldc, 1, 0, 0)
+    ms_l, wall_l = timed(loop, max(1, args.steps // 5), 1)
+    S.set_sync_mode(True)
+    line = {"metric": METRIC, "value": flops / (ms_g * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_g, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "i8+bf16", "data": "synthetic (seeded)",
+            "config": {"workload": f"grouped_{count}", "instances": count, "flops": flops,
+                       "grouped": {"ms_device": ms_g, "ms_wall": wall_g, "launches": launches},
+                       "plain_loop": {"ms_device": ms_l, "ms_wall": wall_l, "launches": count},
+                       "speedup_vs_plain_loop_wall": wall_l / wall_g}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "grouped_10000":
+        return run_grouped(args)
 
     import torch
     import torch.distributed as dist

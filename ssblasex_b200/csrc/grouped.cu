@@ -284,7 +284,7 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
   memset(&dummy, 0, sizeof(dummy));
   const long grid = kd.ntiles < num_sms() ? kd.ntiles : num_sms();
   ProfScope prof(gemm_name, st);
-  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, 192, Cfg::SMEM, st>>>(dummy, dummy, prm);
+  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(dummy, dummy, prm);
   note_launch();
   return cudaGetLastError();
 }

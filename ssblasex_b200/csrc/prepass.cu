@@ -34,16 +34,24 @@ constexpr int NTH = 256;
 template <typename T>
 __device__ __forceinline__ void load_tile(T (&tile)[RT][KT + 1], const T* __restrict__ X, long rows, long K,
                                           long ld, bool kcontig, long row0, long k0) {
+  constexpr int PER = RT * KT / NTH;
+  T v[PER];   // all loads first, then the smem stores, so the loads overlap
 #pragma unroll
-  for (int e = 0; e < RT * KT / NTH; ++e) {
+  for (int e = 0; e < PER; ++e) {
     const int idx = threadIdx.x + e * NTH;
     int r, kk;
     if (kcontig) { r = idx / KT; kk = idx % KT; }
     else { kk = idx / RT; r = idx % RT; }
     const long gr = row0 + r, gk = k0 + kk;
-    T v = T(0);
-    if (gr < rows && gk < K) v = kcontig ? X[gr * ld + gk] : X[gr + gk * ld];
-    tile[r][kk] = v;
+    v[e] = (gr < rows && gk < K) ? __ldg(kcontig ? X + gr * ld + gk : X + gr + gk * ld) : T(0);
+  }
+#pragma unroll
+  for (int e = 0; e < PER; ++e) {
+    const int idx = threadIdx.x + e * NTH;
+    int r, kk;
+    if (kcontig) { r = idx / KT; kk = idx % KT; }
+    else { kk = idx / RT; r = idx % RT; }
+    tile[r][kk] = v[e];
   }
 }
 
@@ -125,19 +133,32 @@ __global__ void __launch_bounds__(NTH, 2) ozaki_slice_kernel(PlaneArgs a, int32_
     int8_t* out = (int8_t*)a.out + b * a.batch_stride;
     if (threadIdx.x < ORT) rmax[threadIdx.x] = 0.0;
     __syncthreads();
-    // pass 1: row maxima of |x|
-    for (long k0 = 0; k0 < a.K; k0 += OKT) {
+    // Loads the ORT x OKT tile at k0 into smem: all loads are issued before any smem store so
+    // that they are in flight together (a store to smem between them would serialise them).
+    auto load_tile = [&](long k0, bool absval) {
+      constexpr int PER = ORT * OKT / NTH;
+      double v[PER];
 #pragma unroll
-      for (int e = 0; e < ORT * OKT / NTH; ++e) {
+      for (int e = 0; e < PER; ++e) {
         const int idx = threadIdx.x + e * NTH;
         int r, kk;
         if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
         else { kk = idx / ORT; r = idx % ORT; }
         const long gr = row0 + r, gk = k0 + kk;
-        double v = 0.0;
-        if (gr < a.rows && gk < a.K) v = a.kcontig ? X[gr * a.ld + gk] : X[gr + gk * a.ld];
-        tile[r][kk] = fabs(v);
+        v[e] = (gr < a.rows && gk < a.K) ? __ldg(a.kcontig ? X + gr * a.ld + gk : X + gr + gk * a.ld) : 0.0;
       }
+#pragma unroll
+      for (int e = 0; e < PER; ++e) {
+        const int idx = threadIdx.x + e * NTH;
+        int r, kk;
+        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
+        else { kk = idx / ORT; r = idx % ORT; }
+        tile[r][kk] = absval ? fabs(v[e]) : v[e];
+      }
+    };
+    // pass 1: row maxima of |x|
+    for (long k0 = 0; k0 < a.K; k0 += OKT) {
+      load_tile(k0, true);
       __syncthreads();
       {
         const int r = threadIdx.x / 8, part = threadIdx.x % 8;   // 8 threads per row
@@ -164,17 +185,7 @@ __global__ void __launch_bounds__(NTH, 2) ozaki_slice_kernel(PlaneArgs a, int32_
     __syncthreads();
     // pass 2: digits (this item's rows were just read, so this pass is served from L2)
     for (long k0 = 0; k0 < a.K; k0 += OKT) {
-#pragma unroll
-      for (int e = 0; e < ORT * OKT / NTH; ++e) {
-        const int idx = threadIdx.x + e * NTH;
-        int r, kk;
-        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
-        else { kk = idx / ORT; r = idx % ORT; }
-        const long gr = row0 + r, gk = k0 + kk;
-        double v = 0.0;
-        if (gr < a.rows && gk < a.K) v = a.kcontig ? X[gr * a.ld + gk] : X[gr + gk * a.ld];
-        tile[r][kk] = v;
-      }
+      load_tile(k0, false);
       __syncthreads();
 #pragma unroll
       for (int it0 = 0; it0 < ORT * (OKT / 4) / NTH; ++it0) {

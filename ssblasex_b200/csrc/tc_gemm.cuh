@@ -16,8 +16,8 @@
 // configuration selects; each pair accumulates into the tensor-memory "level" the configuration
 // assigns to it.
 //
-// Warp roles (192 threads): warp 0 = TMA producer, warp 1 = MMA issuer and TMEM owner,
-// warps 2-5 = epilogue (warp w reads TMEM lanes 32*(w%4) .. +31).
+// Warp roles (320 threads): warp 0 = TMA producer, warp 1 = MMA issuer and TMEM owner,
+// warps 2-9 = epilogue (warp w reads TMEM lanes 32*(w%4) .. +31, half (w-2)/4 of the columns).
 #pragma once
 
 #include <cuda.h>
@@ -28,6 +28,8 @@
 
 namespace ssb {
 namespace tc {
+
+constexpr int kThreads = 320;
 
 enum Kind { KIND_I8 = 0, KIND_BF16 = 1 };
 enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2 };
@@ -133,7 +135,7 @@ struct Config {
 };
 
 template <class Cfg, bool GROUPED>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kThreads, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -157,7 +159,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
     for (int a = 0; a < 2; ++a) {
       ptx::mbar_init(ptx::smem_u32(&tfull[a]), 1);
-      ptx::mbar_init(ptx::smem_u32(&tempty[a]), 4);
+      ptx::mbar_init(ptx::smem_u32(&tempty[a]), 8);
     }
     ptx::mbar_init(ptx::smem_u32(drain), 1);
     ptx::fence_mbar_init();
@@ -261,7 +263,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
   } else {
     // ------------------------------------------------------------------ epilogue ----------
+    // 8 warps: warp w reads TMEM lanes 32*(w%4) .. +31 (its rows) and half (w-2)/4 of the columns
+    constexpr int HALF = Cfg::BN / 2;
     const int quarter = warp % 4;
+    const int half = (warp - 2) / 4;
     const int row_in_tile = quarter * 32 + lane;
     int tcount = 0;
     for (long t = blockIdx.x; t < prm.total_tiles; t += gridDim.x, ++tcount) {
@@ -289,40 +294,60 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       if (!ptx::mbar_wait(ptx::smem_u32(&tfull[acc]), acc_ph, err, 31)) break;
       ptx::tc_fence_after();
       const long gi = (long)ti.mt * Cfg::BM + row_in_tile;
-      const long n0 = (long)ti.nt * Cfg::BN;
-      const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
+      const long n0 = (long)ti.nt * Cfg::BN + half * HALF;
+      const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                             (uint32_t)(acc * Cfg::NLEV * Cfg::BN + half * HALF);
       const bool row_ok = gi < m;
-      int32_t ea = 0;
-      if (Cfg::EPI == EPI_OZAKI && row_ok) ea = exa[gi];
-#pragma unroll 1
-      for (int c0 = 0; c0 < Cfg::BN; c0 += 16) {
-        if (n0 + c0 >= n) break;   // whole chunk outside C: nothing to read or write
-        if (Cfg::EPI == EPI_OZAKI) {
-          double v[16];
+      if constexpr (Cfg::EPI == EPI_OZAKI) {
+        // Horner over the levels (l = NLEV-1 .. 0: v = v * 2^-8 + acc_l) for this warp's columns,
+        // four levels per batch of TMEM loads; then the accumulator is handed back to the MMA
+        // warp before the (slower) scaling and global stores.
+        constexpr int CH = HALF / 16;
+        double v[CH][16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = 0.0;
-#pragma unroll 1
-          for (int l = Cfg::NLEV - 1; l >= 0; --l) {
-            uint32_t raw[16];
-            ptx::tmem_ld16(t_row + (uint32_t)(l * Cfg::BN + c0), raw);
+        for (int c = 0; c < CH; ++c) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[c][j] = 0.0;
+#pragma unroll
+          for (int l0 = Cfg::NLEV - 1; l0 >= 0; l0 -= 4) {
+            uint32_t raw[4][16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (l0 - q >= 0) ptx::tmem_ld16(t_row + (uint32_t)((l0 - q) * Cfg::BN + c * 16), raw[q]);
             ptx::tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = v[j] * 0x1p-8 + (double)(int32_t)raw[j];
+            for (int q = 0; q < 4; ++q)
+              if (l0 - q >= 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[c][j] = v[c][j] * 0x1p-8 + (double)(int32_t)raw[q][j];
+              }
           }
-          if (row_ok) {
-            double* Cd = (double*)Cb;
+        }
+        ptx::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[acc]));
+        if (row_ok) {
+          const int32_t ea = exa[gi];
+          double* Cd = (double*)Cb;
+#pragma unroll
+          for (int c = 0; c < CH; ++c)
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-              const long gj = n0 + c0 + j;
+              const long gj = n0 + c * 16 + j;
               if (gj < n) {
-                const double w = scalbn(v[j], ea + exb[gj] + prm.exp_shift);
+                const double w = scalbn(v[c][j], ea + exb[gj] + prm.exp_shift);
                 double* cp = Cd + gi + gj * ldc;
                 const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
                 *cp = fma(w, alpha_d, tb);
               }
             }
-          }
-        } else {
+        }
+        continue;
+      }
+#pragma unroll 1
+      for (int c0 = 0; c0 < HALF; c0 += 16) {
+        if (n0 + c0 >= n) break;   // whole chunk outside C: nothing to read or write
+        {
           uint32_t raw[16];
           ptx::tmem_ld16(t_row + (uint32_t)c0, raw);
           ptx::tmem_wait_ld();

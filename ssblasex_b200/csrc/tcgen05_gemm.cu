@@ -73,7 +73,7 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   prm.total_tiles = (long)prm.tiles_m * prm.tiles_n * prm.batch;
   long grid = prm.total_tiles < num_sms() ? prm.total_tiles : num_sms();
   ProfScope prof(name, st);
-  tc::tc_gemm_kernel<Cfg, false><<<(unsigned)grid, 192, Cfg::SMEM, st>>>(ta, tb, prm);
+  tc::tc_gemm_kernel<Cfg, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
   note_launch();
   return cudaGetLastError();
 }

@@ -15,6 +15,11 @@
 // each row. The reference's packers play the same role for its SVE microkernel
 // (src/include/ACopy/Xgemm_ncopy_sve_v4.hpp, src/include/BCopy/Xgemm_ncopy_sve_1.hpp), but they
 // run per K block inside the tile loop; here each operand is converted once per call.
+//
+// All three kernels follow the same memory plan: every thread issues its global loads for a
+// 32-row x 64-k tile back to back (coalesced along whichever of rows / k is contiguous), converts
+// in registers, transposes the output bytes through shared memory, and writes 16-byte vectors
+// along K. Several CTAs per SM keep enough loads in flight to run at HBM speed.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -25,83 +30,92 @@
 namespace ssb {
 namespace {
 
-constexpr int RT = 32;   // rows per tile
-constexpr int KT = 64;   // k per tile
+constexpr int RT = 32;    // rows per tile
+constexpr int KT = 64;    // k per tile
 constexpr int NTH = 256;
+constexpr int PER = RT * KT / NTH;   // elements per thread per tile (8)
+constexpr int OPITCH = 68;           // smem bytes per staged output row (17 words: conflict-free)
 
-// Loads the RT x KT tile at (row0, k0) of one instance into smem (zero outside the matrix).
-// kcontig: element (r, k) is X[r*ld + k]; else X[r + k*ld].
+// element e of this thread's share of the tile: (row r, column kk)
+__device__ __forceinline__ void tile_coord(bool kcontig, int e, int& r, int& kk) {
+  if (kcontig) {           // 8 threads per row, 8 consecutive k each
+    r = threadIdx.x / 8;
+    kk = (threadIdx.x % 8) * 8 + e;
+  } else {                 // a warp covers 32 consecutive rows at one k
+    r = threadIdx.x % 32;
+    kk = threadIdx.x / 32 + 8 * e;
+  }
+}
+
 template <typename T>
-__device__ __forceinline__ void load_tile(T (&tile)[RT][KT + 1], const T* __restrict__ X, long rows, long K,
-                                          long ld, bool kcontig, long row0, long k0) {
-  constexpr int PER = RT * KT / NTH;
-  T v[PER];   // all loads first, then the smem stores, so the loads overlap
+__device__ __forceinline__ void load_regs(T (&v)[PER], const T* __restrict__ X, long rows, long K, long ld,
+                                          bool kcontig, long row0, long k0) {
 #pragma unroll
   for (int e = 0; e < PER; ++e) {
-    const int idx = threadIdx.x + e * NTH;
     int r, kk;
-    if (kcontig) { r = idx / KT; kk = idx % KT; }
-    else { kk = idx / RT; r = idx % RT; }
+    tile_coord(kcontig, e, r, kk);
     const long gr = row0 + r, gk = k0 + kk;
     v[e] = (gr < rows && gk < K) ? __ldg(kcontig ? X + gr * ld + gk : X + gr + gk * ld) : T(0);
   }
-#pragma unroll
-  for (int e = 0; e < PER; ++e) {
-    const int idx = threadIdx.x + e * NTH;
-    int r, kk;
-    if (kcontig) { r = idx / KT; kk = idx % KT; }
-    else { kk = idx / RT; r = idx % RT; }
-    tile[r][kk] = v[e];
+}
+
+// Writes staged bytes st[p][r][0..KT*bpe) of P planes as 16-byte vectors.
+template <int P, int BPE>
+__device__ __forceinline__ void write_out(const uint8_t* st, uint8_t* out, long plane_stride, long rows,
+                                          long Kp_bytes, long row0, long kbyte0) {
+  constexpr int SEGS = KT * BPE / 16;
+  for (int it = threadIdx.x; it < P * RT * SEGS; it += NTH) {
+    const int p = it / (RT * SEGS), rem = it % (RT * SEGS), r = rem / SEGS, sg = rem % SEGS;
+    const long gr = row0 + r, gb = kbyte0 + 16 * sg;
+    if (gr < rows && gb < Kp_bytes) {
+      const uint32_t* src = (const uint32_t*)(st + (p * RT + r) * (KT * BPE + 4) + 16 * sg);
+      uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+      *(uint4*)(out + p * plane_stride + gr * Kp_bytes + gb) = w;
+    }
   }
 }
 
 __global__ void __launch_bounds__(NTH) pack_i8_kernel(PlaneArgs a) {
-  __shared__ int8_t tile[RT][KT + 1];
+  __shared__ __align__(16) uint8_t st[RT * (KT + 4)];
   const long b = blockIdx.y;
   const long row0 = (long)blockIdx.x * RT;
   const int8_t* X = (const int8_t*)a.X[b];
-  int8_t* out = (int8_t*)a.out + b * a.batch_stride;
+  uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
   for (long k0 = 0; k0 < a.K; k0 += KT) {
-    load_tile<int8_t>(tile, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
-    __syncthreads();
-    // 32 rows x 16 groups of 4 k -> 512 items, 4-byte stores
-    for (int it = threadIdx.x; it < RT * (KT / 4); it += NTH) {
-      const int r = it / (KT / 4), g = it % (KT / 4);
-      const long gr = row0 + r, gk = k0 + 4 * g;
-      if (gr < a.rows && gk < a.Kp) {
-        uint32_t w = (uint32_t)(uint8_t)tile[r][4 * g] | ((uint32_t)(uint8_t)tile[r][4 * g + 1] << 8) |
-                     ((uint32_t)(uint8_t)tile[r][4 * g + 2] << 16) | ((uint32_t)(uint8_t)tile[r][4 * g + 3] << 24);
-        *(uint32_t*)(out + gr * a.Kp + gk) = w;
-      }
+    int8_t v[PER];
+    load_regs<int8_t>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      int r, kk;
+      tile_coord(a.kcontig, e, r, kk);
+      st[r * (KT + 4) + kk] = (uint8_t)v[e];
     }
+    __syncthreads();
+    write_out<1, 1>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
     __syncthreads();
   }
 }
 
 __global__ void __launch_bounds__(NTH) split_bf16_kernel(PlaneArgs a) {
-  __shared__ float tile[RT][KT + 1];
+  __shared__ __align__(16) uint8_t st[2 * RT * (2 * KT + 4)];
   const long b = blockIdx.y;
   const long row0 = (long)blockIdx.x * RT;
   const float* X = (const float*)a.X[b];
-  __nv_bfloat16* hi = (__nv_bfloat16*)((int8_t*)a.out + b * a.batch_stride);
-  __nv_bfloat16* lo = hi + a.plane_stride / 2;
+  uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
   for (long k0 = 0; k0 < a.K; k0 += KT) {
-    load_tile<float>(tile, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
-    __syncthreads();
-    for (int it = threadIdx.x; it < RT * (KT / 2); it += NTH) {
-      const int r = it / (KT / 2), g = it % (KT / 2);
-      const long gr = row0 + r, gk = k0 + 2 * g;
-      if (gr < a.rows && gk < a.Kp) {
-        const float x0 = tile[r][2 * g], x1 = tile[r][2 * g + 1];
-        const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-        const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-        const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-        __nv_bfloat162 hv, lv;
-        hv.x = h0; hv.y = h1; lv.x = l0; lv.y = l1;
-        *(__nv_bfloat162*)(hi + gr * a.Kp + gk) = hv;
-        *(__nv_bfloat162*)(lo + gr * a.Kp + gk) = lv;
-      }
+    float v[PER];
+    load_regs<float>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      int r, kk;
+      tile_coord(a.kcontig, e, r, kk);
+      const __nv_bfloat16 h = __float2bfloat16_rn(v[e]);
+      const __nv_bfloat16 l = __float2bfloat16_rn(v[e] - __bfloat162float(h));
+      *(__nv_bfloat16*)(st + (0 * RT + r) * (2 * KT + 4) + 2 * kk) = h;
+      *(__nv_bfloat16*)(st + (1 * RT + r) * (2 * KT + 4) + 2 * kk) = l;
     }
+    __syncthreads();
+    write_out<2, 2>(st, out, a.plane_stride, a.rows, a.Kp * 2, row0, k0 * 2);
     __syncthreads();
   }
 }
@@ -111,69 +125,68 @@ __global__ void __launch_bounds__(NTH) split_bf16_kernel(PlaneArgs a) {
 // top bit flipped, read as int8), and d_0 = byte_{S-1}(Y) read as int8 -- the carries of the
 // digit-by-digit recurrence d = ((X + 128) mod 256) - 128, X <- (X - d) / 256 are exactly the
 // carries of the single addition.
-constexpr int ORT = 32;    // rows per work item
-constexpr int OKT = 128;   // k per smem tile
-
 template <int S>
-__global__ void __launch_bounds__(NTH, 2) ozaki_slice_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
-  __shared__ double tile[ORT][OKT + 1];
-  __shared__ double rmax[ORT];
-  __shared__ double rscale[ORT][2];
-  const long blocks_per_inst = (a.rows + ORT - 1) / ORT;
+__global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
+  __shared__ __align__(16) uint8_t st[S * RT * OPITCH];
+  __shared__ double red[8][RT];
+  __shared__ double rscale[RT][2];
+  const long blocks_per_inst = (a.rows + RT - 1) / RT;
   const long total = blocks_per_inst * a.batch;
   unsigned long long bias = 0;
 #pragma unroll
   for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
 
-  // persistent loop: ~2 work items per SM in flight keeps both passes of an item inside L2
   for (long w = blockIdx.x; w < total; w += gridDim.x) {
     const long b = w / blocks_per_inst;
-    const long row0 = (w % blocks_per_inst) * ORT;
+    const long row0 = (w % blocks_per_inst) * RT;
     const double* X = (const double*)a.X[b];
-    int8_t* out = (int8_t*)a.out + b * a.batch_stride;
-    if (threadIdx.x < ORT) rmax[threadIdx.x] = 0.0;
-    __syncthreads();
-    // Loads the ORT x OKT tile at k0 into smem: all loads are issued before any smem store so
-    // that they are in flight together (a store to smem between them would serialise them).
-    auto load_tile = [&](long k0, bool absval) {
-      constexpr int PER = ORT * OKT / NTH;
-      double v[PER];
+    uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
+    // pass 1: row maxima of |x| straight from global memory (8 loads in flight per thread)
+    {
+      double mx = 0.0;
+      if (a.kcontig) {
+        const int r = threadIdx.x / 8, part = threadIdx.x % 8;
+        const long gr = row0 + r;
+        if (gr < a.rows) {
+          const double* row = X + gr * a.ld;
+          long k = part;
+          for (; k + 56 < a.K; k += 64) {
+            double t[8];
 #pragma unroll
-      for (int e = 0; e < PER; ++e) {
-        const int idx = threadIdx.x + e * NTH;
-        int r, kk;
-        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
-        else { kk = idx / ORT; r = idx % ORT; }
-        const long gr = row0 + r, gk = k0 + kk;
-        v[e] = (gr < a.rows && gk < a.K) ? __ldg(a.kcontig ? X + gr * a.ld + gk : X + gr + gk * a.ld) : 0.0;
-      }
+            for (int j = 0; j < 8; ++j) t[j] = __ldg(row + k + 8 * j);
 #pragma unroll
-      for (int e = 0; e < PER; ++e) {
-        const int idx = threadIdx.x + e * NTH;
-        int r, kk;
-        if (a.kcontig) { r = idx / OKT; kk = idx % OKT; }
-        else { kk = idx / ORT; r = idx % ORT; }
-        tile[r][kk] = absval ? fabs(v[e]) : v[e];
-      }
-    };
-    // pass 1: row maxima of |x|
-    for (long k0 = 0; k0 < a.K; k0 += OKT) {
-      load_tile(k0, true);
-      __syncthreads();
-      {
-        const int r = threadIdx.x / 8, part = threadIdx.x % 8;   // 8 threads per row
-        double mx = 0.0;
-#pragma unroll
-        for (int j = 0; j < OKT / 8; ++j) mx = fmax(mx, tile[r][part * (OKT / 8) + j]);
+            for (int j = 0; j < 8; ++j) mx = fmax(mx, fabs(t[j]));
+          }
+          for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(row + k)));
+        }
 #pragma unroll
         for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-        if (part == 0) rmax[r] = fmax(rmax[r], mx);
+        if (part == 0) red[0][r] = mx;
+      } else {
+        const int r = threadIdx.x % 32, part = threadIdx.x / 32;
+        const long gr = row0 + r;
+        if (gr < a.rows) {
+          const double* col = X + gr;
+          long k = part;
+          for (; k + 56 < a.K; k += 64) {
+            double t[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) t[j] = __ldg(col + (k + 8 * j) * a.ld);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) mx = fmax(mx, fabs(t[j]));
+          }
+          for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(col + k * a.ld)));
+        }
+        red[part][r] = mx;
       }
-      __syncthreads();
     }
-    if (threadIdx.x < ORT) {
+    __syncthreads();
+    if (threadIdx.x < RT) {
+      double mx = red[0][threadIdx.x];
+      if (!a.kcontig)
+        for (int q = 1; q < 8; ++q) mx = fmax(mx, red[q][threadIdx.x]);
       int e = 0;
-      if (rmax[threadIdx.x] > 0.0) frexp(rmax[threadIdx.x], &e);
+      if (mx > 0.0) frexp(mx, &e);
       const long gr = row0 + threadIdx.x;
       if (gr < a.rows) exps[b * a.rows + gr] = e;
       // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
@@ -183,38 +196,27 @@ __global__ void __launch_bounds__(NTH, 2) ozaki_slice_kernel(PlaneArgs a, int32_
       rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
     }
     __syncthreads();
-    // pass 2: digits (this item's rows were just read, so this pass is served from L2)
-    for (long k0 = 0; k0 < a.K; k0 += OKT) {
-      load_tile(k0, false);
-      __syncthreads();
+    // pass 2: digits, transposed through smem, written as 16-byte vectors along K
+    for (long k0 = 0; k0 < a.K; k0 += KT) {
+      double v[PER];
+      load_regs<double>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
 #pragma unroll
-      for (int it0 = 0; it0 < ORT * (OKT / 4) / NTH; ++it0) {
-        const int it = threadIdx.x + it0 * NTH;
-        const int r = it / (OKT / 4), g = it % (OKT / 4);
-        const long gr = row0 + r, gk = k0 + 4 * g;
-        if (gr < a.rows && gk < a.Kp) {
-          const double s0 = rscale[r][0], s1 = rscale[r][1];
-          uint32_t lo[4], hi[4];
+      for (int e = 0; e < PER; ++e) {
+        int r, kk;
+        tile_coord(a.kcontig, e, r, kk);
+        const unsigned long long Y =
+            (unsigned long long)__double2ll_rn(v[e] * rscale[r][0] * rscale[r][1]) + bias;
+        const uint32_t lo = (uint32_t)Y, hi = (uint32_t)(Y >> 32);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const unsigned long long Y = (unsigned long long)__double2ll_rn(tile[r][4 * g + j] * s0 * s1) + bias;
-            lo[j] = (uint32_t)Y;
-            hi[j] = (uint32_t)(Y >> 32);
-          }
-#pragma unroll
-          for (int p = 0; p < S; ++p) {
-            const int byte = S - 1 - p;
-            const uint32_t flip = (p == 0) ? 0u : 0x80808080u;
-            uint32_t wv = 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const uint32_t src = byte < 4 ? (lo[j] >> (8 * byte)) : (hi[j] >> (8 * (byte - 4)));
-              wv |= (src & 255u) << (8 * j);
-            }
-            *(uint32_t*)(out + p * a.plane_stride + gr * a.Kp + gk) = wv ^ flip;
-          }
+        for (int p = 0; p < S; ++p) {
+          const int byte = S - 1 - p;
+          uint32_t d = (byte < 4 ? (lo >> (8 * byte)) : (hi >> (8 * (byte - 4)))) & 255u;
+          if (p > 0) d ^= 0x80u;
+          st[(p * RT + r) * OPITCH + kk] = (uint8_t)d;
         }
       }
+      __syncthreads();
+      write_out<S, 1>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
       __syncthreads();
     }
   }
@@ -242,8 +244,9 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
   ProfScope prof("ozaki_slice", st);
-  const long items = (a.rows + ORT - 1) / ORT * a.batch;
-  const unsigned grid = (unsigned)(items < 2L * num_sms() ? items : 2L * num_sms());
+  const long items = (a.rows + RT - 1) / RT * a.batch;
+  const long cap = 4L * num_sms();
+  const unsigned grid = (unsigned)(items < cap ? items : cap);
   switch (slices) {
     case 3: ozaki_slice_kernel<3><<<grid, NTH, 0, st>>>(a, exps); break;
     case 4: ozaki_slice_kernel<4><<<grid, NTH, 0, st>>>(a, exps); break;

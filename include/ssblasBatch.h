@@ -124,6 +124,30 @@ ssblasStatus_t ssblasGetProfile(ssblasKernelProfile_t* out, int max_entries, int
 /* Frees the device workspace cached by the library (it is re-created on the next call). */
 ssblasStatus_t ssblasReleaseWorkspace(void);
 
+/* Allocation-free FP64 batched GEMM (no counterpart in the reference).
+ * Same arguments and results as ssblasGemmBatchedEx on the fp64 row in SSBLAS_MATH_FP64_OZAKI
+ * mode, for callers that cannot let a library allocate device memory: services whose pool
+ * allocator owns all of the GPU's memory, and latency-critical loops in which a cudaMalloc or
+ * cudaFree -- which may synchronise the whole device -- is not allowed. It calls no allocating
+ * function: the Ozaki slices and exponents go to one fixed 64 MiB device array that every GPU
+ * loading the library holds until the process exits.
+ *  - A[], B[], C[] must be device arrays of device pointers; other type rows return
+ *    SSBLAS_STATUS_NOTIMPLEMENTED_ERROR.
+ *  - A problem needs S*(m+n)*Kp*batchCount + 4*(m+n)*batchCount bytes (S = Ozaki slices, 7 by
+ *    default; Kp = k rounded up to 16); larger problems, or k > 16384, return
+ *    SSBLAS_STATUS_INVALID_VALUE (with a message on stderr) and leave C untouched.
+ *  - All calls share the array; calls whose GPU work overlaps race on it and must be ordered by
+ *    the caller. Its contents carry over between calls; nothing in it needs to start at zero.
+ *  - The first call on a device looks the array's address up for that device; make it before
+ *    starting any stream capture on the device. */
+ssblasStatus_t ssblasGemmBatchedExNoAlloc(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
+                                          SSINT n, SSINT k, const void* alpha, const void* const A[],
+                                          ssblasDataType_t Atype, const SSINT lda, const void* const B[],
+                                          ssblasDataType_t Btype, const SSINT ldb, const void* beta,
+                                          void* const C[], ssblasDataType_t Ctype, const SSINT ldc,
+                                          const SSINT batchCount, ssblasComputeType_t computeType,
+                                          ssblasGemmAlgo_t algo);
+
 #ifdef __cplusplus
 }
 #endif

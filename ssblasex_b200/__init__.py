@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "ssblasGemmBatchedEx", "ssblasGemmBatchedEx_64", "ssblasGemmGroupedBatchedEx",
     "ssblasSetStream", "ssblasGetStream", "ssblasSetSyncMode", "ssblasSetMathMode",
     "ssblasGetMathMode", "ssblasSetOzakiSlices", "ssblasGetLastRunInfo", "ssblasReleaseWorkspace",
-    "ssblasSetProfiling", "ssblasGetProfile",
+    "ssblasSetProfiling", "ssblasGetProfile", "ssblasGemmBatchedExNoAlloc",
 )
 
 
@@ -65,7 +65,7 @@ def lib() -> ct.CDLL:
         L = ct.CDLL(str(LIB_PATH))
         vp, l, i = ct.c_void_p, ct.c_long, ct.c_int
         gemm_args = [i, i, l, l, l, vp, vp, i, l, vp, i, l, vp, vp, i, l, l, i, i]
-        for name in ("ssblasGemmBatchedEx", "ssblasGemmBatchedEx_64"):
+        for name in ("ssblasGemmBatchedEx", "ssblasGemmBatchedEx_64", "ssblasGemmBatchedExNoAlloc"):
             f = getattr(L, name)
             f.argtypes = gemm_args
             f.restype = i

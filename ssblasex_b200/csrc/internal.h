@@ -57,6 +57,10 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream);
 cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t stream);
 // fp64 via Ozaki int8 slices; slices = per-operand slice count
 cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t stream);
+// the Ozaki GEMM phase alone, on slice planes and exponents already in (caller-provided) memory:
+// planes [batch][S][rows][Kp] for op(A) then op(B), exponents [batch][m] then [batch][n]
+cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int slices, const int8_t* planes_a, const int8_t* planes_b,
+                                 const int32_t* exps, long Kp, cudaStream_t stream);
 // fp32 via three BF16 products
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t stream);
 

@@ -193,6 +193,30 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   }
 }
 
+cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
+                                 long Kp, cudaStream_t st) {
+  if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
+  if (S < 3 || S > 8) return cudaErrorInvalidValue;
+  const long sa = d.m * Kp, sb = d.n * Kp;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, 32, 128, S, 32) ||
+      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, 32, 64, S, 32))
+    return cudaErrorNotSupported;
+  tc::Params prm = base_params(d);
+  prm.exp_a = ex;
+  prm.exp_b = ex + d.m * d.batch;
+  prm.exp_shift = -12;
+  note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
+  switch (S) {
+    case 3: return run_ozaki<3>(ta, tb, prm, st);
+    case 4: return run_ozaki<4>(ta, tb, prm, st);
+    case 5: return run_ozaki<5>(ta, tb, prm, st);
+    case 6: return run_ozaki<6>(ta, tb, prm, st);
+    case 7: return run_ozaki<7>(ta, tb, prm, st);
+    default: return run_ozaki<8>(ta, tb, prm, st);
+  }
+}
+
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (d.m > (1L << 31) || d.n > (1L << 31) || d.k > (1L << 31)) return cudaErrorNotSupported;

@@ -124,6 +124,14 @@ ssblasStatus_t ssblasGetProfile(ssblasKernelProfile_t* out, int max_entries, int
 /* Frees the device workspace cached by the library (it is re-created on the next call). */
 ssblasStatus_t ssblasReleaseWorkspace(void);
 
+/* Kernel configuration (tile shape / pipeline depth) of one path (an ssblasPath_t value):
+ * config >= 0 forces that configuration, -1 returns to automatic choice -- the tuning table
+ * written by the autotuner ($SSBLAS_TUNE_FILE, else tune/ssblas_tune.json next to the library),
+ * keyed by path and power-of-two size bucket, else the built-in default. Configurations a path
+ * does not have fall back to its default. ssblasReloadTuning re-reads the table. */
+ssblasStatus_t ssblasSetKernelConfig(int path, int config);
+ssblasStatus_t ssblasReloadTuning(void);
+
 /* Allocation-free FP64 batched GEMM (no counterpart in the reference).
  * Same arguments and results as ssblasGemmBatchedEx on the fp64 row in SSBLAS_MATH_FP64_OZAKI
  * mode, for callers that cannot let a library allocate device memory: services whose pool

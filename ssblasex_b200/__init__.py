@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "ssblasSetStream", "ssblasGetStream", "ssblasSetSyncMode", "ssblasSetMathMode",
     "ssblasGetMathMode", "ssblasSetOzakiSlices", "ssblasGetLastRunInfo", "ssblasReleaseWorkspace",
     "ssblasSetProfiling", "ssblasGetProfile", "ssblasGemmBatchedExNoAlloc",
+    "ssblasSetKernelConfig", "ssblasReloadTuning",
 )
 
 
@@ -82,6 +83,8 @@ def lib() -> ct.CDLL:
         L.ssblasReleaseWorkspace.argtypes = []
         L.ssblasSetProfiling.argtypes = [i]
         L.ssblasGetProfile.argtypes = [ct.POINTER(KernelProfile), i, ct.POINTER(i)]
+        L.ssblasSetKernelConfig.argtypes = [i, i]
+        L.ssblasReloadTuning.argtypes = []
         for name in EXPORTED_SYMBOLS[3:]:
             getattr(L, name).restype = i
         _lib = L
@@ -149,3 +152,16 @@ def get_profile() -> dict:
     arr = (KernelProfile * max(n.value, 1))()
     lib().ssblasGetProfile(arr, n.value, ct.byref(n))
     return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(n.value)}
+
+
+PATH_IDS = {"simt": 1, "i8_tcgen05": 2, "ozaki_tcgen05": 3, "bf16x3_tcgen05": 4, "grouped": 5}
+
+
+def set_kernel_config(path: str, config: int) -> int:
+    """Force configuration `config` of a kernel family ("i8_tcgen05", "ozaki_tcgen05", ...);
+    -1 returns to the tuned / default choice."""
+    return lib().ssblasSetKernelConfig(PATH_IDS[path], config)
+
+
+def reload_tuning() -> int:
+    return lib().ssblasReloadTuning()

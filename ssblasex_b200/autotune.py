@@ -1,0 +1,118 @@
+"""Autotuner: times every configuration of each tensor-core kernel family on representative
+problems and writes the winners, per power-of-two size bucket, to the library's tuning table
+(ssblasex_b200/tune/ssblas_tune.json, read by csrc/tune.cpp).
+
+    python -m ssblasex_b200.autotune [--out PATH] [--quick]
+
+Each candidate is checked against the default configuration's result before it can win (bit for
+bit on the integer and Ozaki paths, whose arithmetic does not depend on the tiling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import pathlib
+import time
+
+import numpy as np
+
+from . import PATH_IDS, get_profile, lib, set_kernel_config, set_math_mode, set_profiling, set_sync_mode
+from . import SSBLAS_MATH_FP32_BF16X3, SSBLAS_MATH_FP64_OZAKI, SSBLAS_MATH_PLAIN
+from . import runner, workloads as W
+
+OUT = pathlib.Path(__file__).resolve().parent / "tune" / "ssblas_tune.json"
+
+# path -> (math mode, configurations, kernel name, problems)
+FAMILIES = {
+    "ozaki_tcgen05": (SSBLAS_MATH_FP64_OZAKI, [0, 1, 2], "ozaki_gemm", [
+        dict(row="f64", transa=0, transb=1, m=1024, n=1024, k=1024, batch=32, alpha=1.0, beta=0.0,
+             lda=1032, ldb=1032, ldc=1032, dist="expspread"),
+        dict(row="f64", transa=0, transb=0, m=512, n=512, k=512, batch=64, alpha=1.0, beta=0.0,
+             dist="expspread"),
+        dict(row="f64", transa=1, transb=0, m=256, n=256, k=2048, batch=32, alpha=1.0, beta=0.0,
+             dist="expspread"),
+    ]),
+    "i8_tcgen05": (SSBLAS_MATH_PLAIN, [0, 1], "i8_gemm", [
+        dict(row="i8", transa=1, transb=0, m=512, n=512, k=512, batch=512, alpha=1, beta=1,
+             lda=512, ldb=512, ldc=512),
+        dict(row="i8", transa=1, transb=0, m=256, n=256, k=1024, batch=512, alpha=1, beta=0,
+             lda=1024, ldb=1024, ldc=256),
+    ]),
+    "bf16x3_tcgen05": (SSBLAS_MATH_FP32_BF16X3, [0, 1], "bf16x3_gemm", [
+        dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
+             dist="outliers"),
+        dict(row="f32", transa=0, transb=0, m=256, n=256, k=256, batch=256, alpha=1.0, beta=0.0),
+    ]),
+}
+
+
+def bucket(m, n, k, batch):
+    c = lambda x: max(0, int(np.ceil(np.log2(max(x, 1)))))
+    return f"m{c(m)}n{c(n)}k{c(k)}b{c(batch)}"
+
+
+def time_kernel(p, dp, kernel, reps):
+    import torch
+    al = np.array([p.alpha], p.scale_dtype)
+    be = np.array([p.beta], p.scale_dtype)
+    Ah, Bh, Ch = dp.host_arrays()
+    ta, tb, tc = p.types
+    call = lambda: lib().ssblasGemmBatchedEx(p.transa, p.transb, p.m, p.n, p.k, al.ctypes.data, Ah, ta, p.lda,
+                                             Bh, tb, p.ldb, be.ctypes.data, Ch, tc, p.ldc, p.batch, 0, 0)
+    set_sync_mode(False)
+    for _ in range(2):
+        assert call() == 0
+    torch.cuda.synchronize()
+    set_profiling(True)
+    for _ in range(reps):
+        assert call() == 0
+    prof = get_profile()
+    set_profiling(False)
+    set_sync_mode(True)
+    n, ms = prof.get(kernel, (1, float("nan")))
+    return ms / max(n, 1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(OUT))
+    ap.add_argument("--quick", action="store_true")
+    args = ap.parse_args()
+    entries, report = [], []
+    for family, (mode, configs, kernel, probs) in FAMILIES.items():
+        set_math_mode(mode)
+        for kw in probs[: 1 if args.quick else None]:
+            p = W.make_problem(seed=7, **kw)
+            dp = runner.DeviceProblem(p)
+            ref = None
+            times = {}
+            for cfg in configs:
+                set_kernel_config(family, cfg)
+                dp.reset_c()
+                st, C = runner.call(p, mode="host_array", dp=dp)
+                assert st == 0
+                if ref is None:
+                    ref = C
+                elif p.row == "f32":
+                    if not np.allclose(C, ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max()):
+                        continue
+                elif not np.array_equal(C.view(np.uint8), ref.view(np.uint8)):
+                    continue          # a configuration that disagrees never wins
+                times[cfg] = time_kernel(p, dp, kernel, 5)
+            set_kernel_config(family, -1)
+            best = min(times, key=times.get)
+            b = bucket(p.m, p.n, p.k, p.batch)
+            entries.append({"path": PATH_IDS[family], "bucket": b, "config": best})
+            report.append({"family": family, "bucket": b, "ms": times, "best": best})
+            print(json.dumps(report[-1]), flush=True)
+    set_math_mode(SSBLAS_MATH_PLAIN)
+    out = pathlib.Path(args.out)
+    out.parent.mkdir(parents=True, exist_ok=True)
+    lines = [json.dumps(e) for e in entries]
+    out.write_text("{\"version\": 1, \"generated\": \"%s\", \"entries\": [\n%s\n]}\n"
+                   % (time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()), ",\n".join(lines)))
+    print(f"wrote {out}")
+
+
+if __name__ == "__main__":
+    main()

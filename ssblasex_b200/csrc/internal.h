@@ -66,6 +66,9 @@ cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t stream);
 
 int num_sms();
 
+// Configuration index of a kernel family for a problem (tune.cpp): forced, tuned, or `fallback`.
+int choose_config(int path, long m, long n, long k, long batch, int fallback);
+
 // Optional per-kernel CUDA-event timing (ssblasSetProfiling): records an event pair around each
 // launch on its stream; ssblasGetProfile resolves them.
 void prof_start(const char* name, cudaStream_t st);

@@ -222,6 +222,107 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
   }
 }
 
+// Two-kernel form of the slicing for large operands: a streaming pass that only finds the row
+// exponents, then one CTA per (instance, 32 rows, 64 k) chunk for the digits, so that every
+// chunk's loads are in flight at once instead of walking K inside a CTA.
+__global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
+  __shared__ double red[8][RT];
+  const long blocks_per_inst = (a.rows + RT - 1) / RT;
+  const long b = blockIdx.x / blocks_per_inst;
+  const long row0 = (blockIdx.x % blocks_per_inst) * RT;
+  const double* X = (const double*)a.X[b];
+  double mx = 0.0;
+  if (a.kcontig) {
+    const int r = threadIdx.x / 8, part = threadIdx.x % 8;
+    const long gr = row0 + r;
+    if (gr < a.rows) {
+      const double* row = X + gr * a.ld;
+      long k = part;
+      for (; k + 120 < a.K; k += 128) {
+        double t[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) t[j] = __ldg(row + k + 8 * j);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(t[j]));
+      }
+      for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(row + k)));
+    }
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (part == 0) red[0][r] = mx;
+  } else {
+    const int r = threadIdx.x % 32, part = threadIdx.x / 32;
+    const long gr = row0 + r;
+    if (gr < a.rows) {
+      const double* col = X + gr;
+      long k = part;
+      for (; k + 120 < a.K; k += 128) {
+        double t[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) t[j] = __ldg(col + (k + 8 * j) * a.ld);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(t[j]));
+      }
+      for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(col + k * a.ld)));
+    }
+    red[part][r] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < RT) {
+    double m2 = red[0][threadIdx.x];
+    if (!a.kcontig)
+      for (int q = 1; q < 8; ++q) m2 = fmax(m2, red[q][threadIdx.x]);
+    int e = 0;
+    if (m2 > 0.0) frexp(m2, &e);
+    const long gr = row0 + threadIdx.x;
+    if (gr < a.rows) exps[b * a.rows + gr] = e;
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a, const int32_t* __restrict__ exps) {
+  __shared__ __align__(16) uint8_t st[S * RT * OPITCH];
+  __shared__ double rscale[RT][2];
+  const long blocks_per_inst = (a.rows + RT - 1) / RT;
+  const long kchunks = (a.K + KT - 1) / KT;
+  const long item = blockIdx.x / kchunks;
+  const long k0 = (blockIdx.x % kchunks) * KT;
+  const long b = item / blocks_per_inst;
+  const long row0 = (item % blocks_per_inst) * RT;
+  const double* X = (const double*)a.X[b];
+  uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
+  double v[PER];
+  load_regs<double>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+  if (threadIdx.x < RT) {
+    const long gr = row0 + threadIdx.x;
+    const int e = gr < a.rows ? exps[b * a.rows + gr] : 0;
+    const int sh = 8 * S - 2 - e;
+    const int h1 = sh / 2;
+    rscale[threadIdx.x][0] = ldexp(1.0, h1);
+    rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
+  }
+  __syncthreads();
+  unsigned long long bias = 0;
+#pragma unroll
+  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+#pragma unroll
+  for (int e = 0; e < PER; ++e) {
+    int r, kk;
+    tile_coord(a.kcontig, e, r, kk);
+    const unsigned long long Y = (unsigned long long)__double2ll_rn(v[e] * rscale[r][0] * rscale[r][1]) + bias;
+    const uint32_t lo = (uint32_t)Y, hi = (uint32_t)(Y >> 32);
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
+      const int byte = S - 1 - p;
+      uint32_t d = (byte < 4 ? (lo >> (8 * byte)) : (hi >> (8 * (byte - 4)))) & 255u;
+      if (p > 0) d ^= 0x80u;
+      st[(p * RT + r) * OPITCH + kk] = (uint8_t)d;
+    }
+  }
+  __syncthreads();
+  write_out<S, 1>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
+}
+
 dim3 grid_of(const PlaneArgs& a) {
   return dim3((unsigned)((a.rows + RT - 1) / RT), (unsigned)a.batch);
 }
@@ -243,8 +344,29 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
-  ProfScope prof("ozaki_slice", st);
   const long items = (a.rows + RT - 1) / RT * a.batch;
+  const long chunks = items * ((a.K + KT - 1) / KT);
+  if (items >= 2L * num_sms() && chunks < (1L << 31)) {
+    // enough rows to fill the GPU: the two-kernel form (exponents, then digits per chunk)
+    {
+      ProfScope prof("ozaki_rowexp", st);
+      ozaki_rowexp_kernel<<<(unsigned)items, NTH, 0, st>>>(a, exps);
+      note_launch();
+    }
+    ProfScope prof("ozaki_slice", st);
+    switch (slices) {
+      case 3: ozaki_digits_kernel<3><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 4: ozaki_digits_kernel<4><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 5: ozaki_digits_kernel<5><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 6: ozaki_digits_kernel<6><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 7: ozaki_digits_kernel<7><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 8: ozaki_digits_kernel<8><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      default: return cudaErrorInvalidValue;
+    }
+    note_launch();
+    return cudaGetLastError();
+  }
+  ProfScope prof("ozaki_slice", st);
   const long cap = 4L * num_sms();
   const unsigned grid = (unsigned)(items < cap ? items : cap);
   switch (slices) {

@@ -119,9 +119,45 @@ template <> struct OzCfg<6> { using T = tc::Config<tc::KIND_I8, 6, 6, 64, 32, 6,
 template <> struct OzCfg<7> { using T = tc::Config<tc::KIND_I8, 7, 7, 64, 32, 5, 7, 1, tc::EPI_OZAKI, 2>; };
 template <> struct OzCfg<8> { using T = tc::Config<tc::KIND_I8, 8, 8, 64, 32, 4, 8, 1, tc::EPI_OZAKI, 2>; };
 
-template <int S>
-cudaError_t run_ozaki(const CUtensorMap& ta, const CUtensorMap& tb, const tc::Params& prm, cudaStream_t st) {
-  return run_gemm<typename OzCfg<S>::T>(ta, tb, prm, st, "ozaki_gemm");
+// Alternative Ozaki configurations for the default slice count (7), chosen by the autotuner:
+//   1: 64-byte K stages (two MMA K steps per slice pair per stage), 2 stages
+//   2: 128 x 32 tiles with a double-buffered accumulator (the epilogue overlaps the next tile)
+using OzCfg7KB64 = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2>;
+using OzCfg7N32 = tc::Config<tc::KIND_I8, 7, 7, 32, 32, 6, 7, 2, tc::EPI_OZAKI, 2>;
+
+template <class Cfg>
+cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
+                           long Kp, cudaStream_t st) {
+  const long sa = d.m * Kp, sb = d.n * Kp;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, Cfg::KB, 128, S,
+                Cfg::KB) ||
+      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, Cfg::KB, Cfg::BN, S,
+                Cfg::KB))
+    return cudaErrorNotSupported;
+  tc::Params prm = base_params(d);
+  prm.exp_a = ex;
+  prm.exp_b = ex + d.m * d.batch;
+  prm.exp_shift = -12;
+  note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
+  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm");
+}
+
+cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex, long Kp,
+                       cudaStream_t st) {
+  switch (S) {
+    case 3: return ozaki_gemm_cfg<OzCfg<3>::T>(d, S, pa, pb, ex, Kp, st);
+    case 4: return ozaki_gemm_cfg<OzCfg<4>::T>(d, S, pa, pb, ex, Kp, st);
+    case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, ex, Kp, st);
+    case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, ex, Kp, st);
+    case 7: {
+      const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 0);
+      if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, ex, Kp, st);
+      if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, ex, Kp, st);
+      return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, ex, Kp, st);
+    }
+    default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, ex, Kp, st);
+  }
 }
 
 }  // namespace
@@ -134,7 +170,7 @@ cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t st) {
   const bool direct = d.transa == SSBLAS_OP_T && d.transb == SSBLAS_OP_N && uniform && d.lda % 16 == 0 &&
                       d.ldb % 16 == 0 && ((uintptr_t)d.A0 % 16) == 0 && ((uintptr_t)d.B0 % 16) == 0 &&
                       d.strideA % 16 == 0 && d.strideB % 16 == 0;
-  const int BN = d.n <= 128 ? 128 : 256;
+  const int BN = choose_config(SSBLAS_PATH_I8_TCGEN05, d.m, d.n, d.k, d.batch, d.n <= 128 ? 1 : 0) == 1 ? 128 : 256;
   bool ok;
   if (direct) {
     const long psa = d.batch > 1 ? d.strideA : round_up(d.lda * d.m, 16);
@@ -174,47 +210,14 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * S};
   if ((e = launch_ozaki_slice(a, S, ex, st)) != cudaSuccess) return e;
   if ((e = launch_ozaki_slice(b, S, ex + d.m * d.batch, st)) != cudaSuccess) return e;
-  CUtensorMap ta, tb;
-  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, 32, 128, S, 32) ||
-      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, 32, 64, S, 32))
-    return cudaErrorNotSupported;
-  tc::Params prm = base_params(d);
-  prm.exp_a = ex;
-  prm.exp_b = ex + d.m * d.batch;
-  prm.exp_shift = -12;
-  note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
-  switch (S) {
-    case 3: return run_ozaki<3>(ta, tb, prm, st);
-    case 4: return run_ozaki<4>(ta, tb, prm, st);
-    case 5: return run_ozaki<5>(ta, tb, prm, st);
-    case 6: return run_ozaki<6>(ta, tb, prm, st);
-    case 7: return run_ozaki<7>(ta, tb, prm, st);
-    default: return run_ozaki<8>(ta, tb, prm, st);
-  }
+  return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
 }
 
 cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
                                  long Kp, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (S < 3 || S > 8) return cudaErrorInvalidValue;
-  const long sa = d.m * Kp, sb = d.n * Kp;
-  CUtensorMap ta, tb;
-  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, 32, 128, S, 32) ||
-      !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, 32, 64, S, 32))
-    return cudaErrorNotSupported;
-  tc::Params prm = base_params(d);
-  prm.exp_a = ex;
-  prm.exp_b = ex + d.m * d.batch;
-  prm.exp_shift = -12;
-  note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
-  switch (S) {
-    case 3: return run_ozaki<3>(ta, tb, prm, st);
-    case 4: return run_ozaki<4>(ta, tb, prm, st);
-    case 5: return run_ozaki<5>(ta, tb, prm, st);
-    case 6: return run_ozaki<6>(ta, tb, prm, st);
-    case 7: return run_ozaki<7>(ta, tb, prm, st);
-    default: return run_ozaki<8>(ta, tb, prm, st);
-  }
+  return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
 }
 
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
@@ -231,7 +234,7 @@ cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * 2};
   if ((e = launch_split_bf16(a, st)) != cudaSuccess) return e;
   if ((e = launch_split_bf16(b, st)) != cudaSuccess) return e;
-  const int BN = d.n <= 64 ? 64 : 128;
+  const int BN = choose_config(SSBLAS_PATH_BF16X3_TCGEN05, d.m, d.n, d.k, d.batch, d.n <= 64 ? 0 : 1) == 0 ? 64 : 128;
   CUtensorMap ta, tb;
   if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.m, 2, d.batch, Kp * 2, sa, sa * 2, 64, 128, 2, 128) ||
       !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.n, 2, d.batch, Kp * 2, sb, sb * 2, 64, BN, 2, 128))

@@ -130,3 +130,34 @@ def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
         assert np.max(np.abs(got - emu) / nrm) <= 4 * k * 2.0 ** -24
         # stated error of the mode against the FP64-exact result
         assert np.max(np.abs(got - ex) / nrm) <= 2.0 ** -14
+
+
+# ------------------------------------------------------------------------- configurations ---
+@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2),
+                                        ("i8_tcgen05", 0), ("i8_tcgen05", 1),
+                                        ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1)])
+def test_every_kernel_configuration(S, family, cfg):
+    """Each configuration the autotuner may pick gives the right answer on a ragged problem."""
+    from ssblasex_b200 import workloads as W
+    S.set_kernel_config(family, cfg)
+    try:
+        if family == "ozaki_tcgen05":
+            S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+            p = W.make_problem("f64", 0, 1, 300, 170, 333, 3, 0.5, 2.0, seed=40 + cfg, dist="expspread")
+            C = run(p)
+            np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
+        elif family == "i8_tcgen05":
+            p = W.make_problem("i8", 1, 0, 300, 170, 336, 3, 3, -1, lda=336, ldb=336, seed=50 + cfg)
+            C = run(p)
+            np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+        else:
+            S.set_math_mode(S.SSBLAS_MATH_FP32_BF16X3)
+            p = W.make_problem("f32", 1, 0, 300, 170, 200, 2, 0.75, 0.25, seed=60 + cfg)
+            C = run(p)
+            for b in range(p.batch):
+                emu = O.bf16x3_f32(p, b)
+                ex, nrm = O.exact_f64(p, b)
+                assert np.max(np.abs(p.c_view(C, b) - emu) / nrm) <= 4 * p.k * 2.0 ** -24
+        assert S.last_run_info()["path"] == family
+    finally:
+        S.set_kernel_config(family, -1)

@@ -259,31 +259,45 @@ static long uniform_stride(const void* const* ptrs, long batch) {
   return s;
 }
 
-// Pinned host scratch for pointer arrays; reused after the previous upload has completed.
-struct PinnedRing {
+// Pinned host scratch for pointer-array uploads: a ring of slots, so an asynchronous call only
+// waits for the upload issued kPinSlots calls earlier (not for the previous call's kernels, which
+// the previous upload is queued behind).
+constexpr int kPinSlots = 8;
+struct PinnedSlot {
   void* host = nullptr;
   size_t size = 0;
   cudaEvent_t done = nullptr;
+  bool pending = false;
 };
-static PinnedRing g_pin;
+static PinnedSlot g_pins[kPinSlots];
+static int g_pin_cur = 0;
 
 static void* pinned(size_t bytes, cudaError_t* err) {
   *err = cudaSuccess;
-  if (g_pin.done) cudaEventSynchronize(g_pin.done);
-  if (g_pin.size < bytes) {
-    if (g_pin.host) cudaFreeHost(g_pin.host);
-    g_pin.host = nullptr;
-    g_pin.size = 0;
+  g_pin_cur = (g_pin_cur + 1) % kPinSlots;
+  PinnedSlot& s = g_pins[g_pin_cur];
+  if (s.pending) cudaEventSynchronize(s.done);
+  s.pending = false;
+  if (s.size < bytes) {
+    if (s.host) cudaFreeHost(s.host);
+    s.host = nullptr;
+    s.size = 0;
     size_t sz = (bytes + bytes / 4 + 4095) & ~(size_t)4095;
-    *err = cudaMallocHost(&g_pin.host, sz);
+    *err = cudaMallocHost(&s.host, sz);
     if (*err != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
-    g_pin.size = sz;
+    s.size = sz;
   }
-  if (!g_pin.done) cudaEventCreateWithFlags(&g_pin.done, cudaEventDisableTiming);
-  return g_pin.host;
+  if (!s.done && (*err = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)) != cudaSuccess) return nullptr;
+  return s.host;
+}
+
+// marks the current slot as read by an upload just enqueued on `st`
+static void pinned_done(cudaStream_t st) {
+  PinnedSlot& s = g_pins[g_pin_cur];
+  if (cudaEventRecord(s.done, st) == cudaSuccess) s.pending = true;
 }
 
 static ssblasStatus_t map_err(cudaError_t e) {
@@ -444,7 +458,7 @@ static ssblasStatus_t grouped_device(
     void** dp = (void**)workspace(WS_PTRS, 3 * sizeof(void*) * total, &e);
     if (!dp) return map_err(e);
     if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * total, cudaMemcpyHostToDevice, st))) return map_err(e);
-    cudaEventRecord(g_pin.done, st);
+    pinned_done(st);
     g.A = (const void* const*)dp;
     g.B = (const void* const*)(dp + total);
     g.C = (void* const*)(dp + 2 * total);
@@ -558,7 +572,7 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
     if (!dp) return map_err(e);
     if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * batchCount, cudaMemcpyHostToDevice, st)))
       return map_err(e);
-    cudaEventRecord(g_pin.done, st);
+    pinned_done(st);
     d.A = (const void* const*)dp;
     d.B = (const void* const*)(dp + batchCount);
     d.C = (void* const*)(dp + 2 * batchCount);

@@ -151,7 +151,8 @@ cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t
     case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, ex, Kp, st);
     case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, ex, Kp, st);
     case 7: {
-      const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 0);
+      // 64-byte K stages won every bucket the autotuner measured, so they are the default
+      const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 1);
       if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, ex, Kp, st);
       if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, ex, Kp, st);
       return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, ex, Kp, st);

@@ -237,6 +237,28 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           ptx::tc_fence_after();
           const uint32_t sa = ptx::smem_u32(stages + (size_t)s * Cfg::STAGE);
           const uint32_t sb = sa + Cfg::A_STAGE;
+          if constexpr (Cfg::PAIRS == 2) {
+            // Ozaki: slice planes q..q+j-1 of B are contiguous rows of one operand and levels
+            // p+q..p+q+j-1 are adjacent TMEM column blocks, so one MMA with N = j*BN (<= 256)
+            // multiplies A_p by j planes of B at once and adds each product into its own level.
+            // Every level is first written by the p = 0 MMAs of the first K step.
+            constexpr int MAXQ = 256 / Cfg::BN;
+#pragma unroll
+            for (int p = 0; p < Cfg::PA; ++p) {
+#pragma unroll
+              for (int q0 = 0; q0 < Cfg::NLEV - p; q0 += MAXQ) {
+                const int nq = (Cfg::NLEV - p - q0) < MAXQ ? (Cfg::NLEV - p - q0) : MAXQ;
+                const uint32_t idesc = ptx::idesc_i8(128, nq * Cfg::BN, true, true);
+                const uint32_t d = d_base + (uint32_t)((p + q0) * Cfg::BN);
+#pragma unroll
+                for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
+                  const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
+                  const uint64_t bd = ptx::smem_desc_kmajor(sb + q0 * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
+                  ptx::mma_i8(d, ad, bd, idesc, (kb > 0 || kk > 0 || p > 0) ? 1u : 0u);
+                }
+              }
+            }
+          } else {
 #pragma unroll
           for (int p = 0; p < Cfg::PA; ++p) {
 #pragma unroll
@@ -252,6 +274,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 else ptx::mma_f16(d, ad, bd, IDESC, accum);
               }
             }
+          }
           }
           ptx::mma_commit(ptx::smem_u32(&empty[s]));   // frees the stage when these MMAs finish
         }
@@ -344,49 +367,62 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         continue;
       }
+      // Groups of up to 64 columns: all TMEM loads, then all C loads (when beta != 0) are issued
+      // before any use, so each thread keeps up to 64 reads of C in flight.
+      constexpr int G = HALF < 64 ? HALF : 64;
+      constexpr int GC = G / 16;
 #pragma unroll 1
-      for (int c0 = 0; c0 < HALF; c0 += 16) {
-        if (n0 + c0 >= n) break;   // whole chunk outside C: nothing to read or write
-        {
-          uint32_t raw[16];
-          ptx::tmem_ld16(t_row + (uint32_t)c0, raw);
-          ptx::tmem_wait_ld();
-          if (row_ok) {
-            if (Cfg::EPI == EPI_I32) {
-              int32_t* Ci = (int32_t*)Cb;
-              if (beta_i == 0) {
+      for (int g0 = 0; g0 < HALF; g0 += G) {
+        if (n0 + g0 >= n) break;   // whole group outside C: nothing to read or write
+        uint32_t raw[GC][16];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                  const long gj = n0 + c0 + j;
-                  if (gj < n) __stcs(Ci + gi + gj * ldc, (int32_t)(raw[j] * (uint32_t)alpha_i));
-                }
-              } else {
-                uint32_t cv[16];
+        for (int c = 0; c < GC; ++c) ptx::tmem_ld16(t_row + (uint32_t)(g0 + 16 * c), raw[c]);
+        ptx::tmem_wait_ld();
+        if (!row_ok) continue;
+        if (Cfg::EPI == EPI_I32) {
+          int32_t* Ci = (int32_t*)Cb + gi;
+          uint32_t cv[GC][16];
+          if (beta_i != 0) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                  const long gj = n0 + c0 + j;
-                  cv[j] = (gj < n) ? (uint32_t)__ldcs(Ci + gi + gj * ldc) : 0u;
-                }
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                  const long gj = n0 + c0 + j;
-                  if (gj < n)
-                    __stcs(Ci + gi + gj * ldc, (int32_t)((uint32_t)beta_i * cv[j] + raw[j] * (uint32_t)alpha_i));
-                }
-              }
-            } else {
-              float* Cf = (float*)Cb;
+            for (int c = 0; c < GC; ++c)
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
-                const long gj = n0 + c0 + j;
-                if (gj < n) {
-                  float* cp = Cf + gi + gj * ldc;
-                  const float tb = (beta_f == 0.0f) ? 0.0f : beta_f * (*cp);
-                  *cp = fmaf(__uint_as_float(raw[j]), alpha_f, tb);
-                }
+                const long gj = n0 + g0 + 16 * c + j;
+                cv[c][j] = (gj < n) ? (uint32_t)__ldcs(Ci + gj * ldc) : 0u;
+              }
+          }
+#pragma unroll
+          for (int c = 0; c < GC; ++c)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const long gj = n0 + g0 + 16 * c + j;
+              if (gj < n) {
+                const uint32_t t = (beta_i == 0) ? 0u : (uint32_t)beta_i * cv[c][j];
+                __stcs(Ci + gj * ldc, (int32_t)(t + raw[c][j] * (uint32_t)alpha_i));
               }
             }
+        } else {
+          float* Cf = (float*)Cb + gi;
+          float cv[GC][16];
+          if (beta_f != 0.0f) {
+#pragma unroll
+            for (int c = 0; c < GC; ++c)
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                const long gj = n0 + g0 + 16 * c + j;
+                cv[c][j] = (gj < n) ? __ldcs(Cf + gj * ldc) : 0.0f;
+              }
           }
+#pragma unroll
+          for (int c = 0; c < GC; ++c)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const long gj = n0 + g0 + 16 * c + j;
+              if (gj < n) {
+                const float tb = (beta_f == 0.0f) ? 0.0f : beta_f * cv[c][j];
+                __stcs(Cf + gj * ldc, fmaf(__uint_as_float(raw[c][j]), alpha_f, tb));
+              }
+            }
         }
       }
       ptx::tc_fence_before();

@@ -158,7 +158,17 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
       __syncthreads();
     }
 
+    // epilogue: all reads of C (beta != 0) are issued before the first store, so they overlap
     typename Tr::C* __restrict__ Cm = args.C[b];
+    typename Tr::C cv[TM][TN];
+    const bool read_c = !(args.beta == typename Tr::S(0));
+#pragma unroll
+    for (int c = 0; c < TN; ++c)
+#pragma unroll
+      for (int r = 0; r < TM; ++r) {
+        const long gi = m0 + tx + r * TX, gj = n0 + ty + c * TY;
+        cv[r][c] = (read_c && gi < args.m && gj < args.n) ? Cm[gi + gj * args.ldc] : typename Tr::C(0);
+      }
 #pragma unroll
     for (int c = 0; c < TN; ++c) {
       long gj = n0 + ty + c * TY;
@@ -166,10 +176,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
 #pragma unroll
       for (int r = 0; r < TM; ++r) {
         long gi = m0 + tx + r * TX;
-        if (gi < args.m) {
-          typename Tr::C* p = Cm + gi + gj * args.ldc;
-          *p = Tr::epi(acc[r][c], args.alpha, args.beta, p);
-        }
+        if (gi < args.m) Cm[gi + gj * args.ldc] = Tr::epi(acc[r][c], args.alpha, args.beta, &cv[r][c]);
       }
     }
   }
@@ -223,9 +230,11 @@ SimtArgs<T> make_args(const BatchDesc& d) {
 }  // namespace
 
 cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
-  // Large tiles when there is enough work to fill the GPU with them, small tiles otherwise.
+  // Large tiles when both dimensions fill them and there is enough work to occupy the GPU with
+  // them, small tiles otherwise (the tuning table or a forced configuration can override).
   const long big_tiles = ((d.m + 127) / 128) * ((d.n + 127) / 128) * d.batch;
-  const bool big = big_tiles >= 2L * num_sms();
+  const bool big_default = d.m >= 128 && d.n >= 128 && big_tiles >= 2L * num_sms();
+  const bool big = choose_config(SSBLAS_PATH_SIMT, d.m, d.n, d.k, d.batch, big_default ? 1 : 0) == 1;
   switch (d.row) {
     case ROW_F32: {
       auto a = make_args<float>(d);

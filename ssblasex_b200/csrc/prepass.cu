@@ -291,8 +291,21 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a, const in
   const long row0 = (item % blocks_per_inst) * RT;
   const double* X = (const double*)a.X[b];
   uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
+  // this thread's 8 elements: one row, two runs of 4 consecutive k, so that the 4 digits of a
+  // run pack into one 32-bit shared-memory store per plane
+  const int r = a.kcontig ? threadIdx.x / 8 : threadIdx.x % 32;
+  auto kk_of = [&](int e) {
+    return a.kcontig ? (threadIdx.x % 8) * 8 + e : (threadIdx.x / 32) * 4 + (e % 4) + 32 * (e / 4);
+  };
   double v[PER];
-  load_regs<double>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+  {
+    const long gr = row0 + r;
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const long gk = k0 + kk_of(e);
+      v[e] = (gr < a.rows && gk < a.K) ? __ldg(a.kcontig ? X + gr * a.ld + gk : X + gr + gk * a.ld) : 0.0;
+    }
+  }
   if (threadIdx.x < RT) {
     const long gr = row0 + threadIdx.x;
     const int e = gr < a.rows ? exps[b * a.rows + gr] : 0;
@@ -305,18 +318,28 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a, const in
   unsigned long long bias = 0;
 #pragma unroll
   for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+  const double s0 = rscale[r][0], s1 = rscale[r][1];
 #pragma unroll
-  for (int e = 0; e < PER; ++e) {
-    int r, kk;
-    tile_coord(a.kcontig, e, r, kk);
-    const unsigned long long Y = (unsigned long long)__double2ll_rn(v[e] * rscale[r][0] * rscale[r][1]) + bias;
-    const uint32_t lo = (uint32_t)Y, hi = (uint32_t)(Y >> 32);
+  for (int g = 0; g < PER / 4; ++g) {
+    uint32_t lo[4], hi[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const unsigned long long Y = (unsigned long long)__double2ll_rn(v[4 * g + j] * s0 * s1) + bias;
+      lo[j] = (uint32_t)Y;
+      hi[j] = (uint32_t)(Y >> 32);
+    }
+    const int kk = kk_of(4 * g);
 #pragma unroll
     for (int p = 0; p < S; ++p) {
       const int byte = S - 1 - p;
-      uint32_t d = (byte < 4 ? (lo >> (8 * byte)) : (hi >> (8 * (byte - 4)))) & 255u;
-      if (p > 0) d ^= 0x80u;
-      st[(p * RT + r) * OPITCH + kk] = (uint8_t)d;
+      uint32_t w = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t src = byte < 4 ? (lo[j] >> (8 * byte)) : (hi[j] >> (8 * (byte - 4)));
+        w |= (src & 255u) << (8 * j);
+      }
+      if (p > 0) w ^= 0x80808080u;
+      *(uint32_t*)(st + (p * RT + r) * OPITCH + kk) = w;
     }
   }
   __syncthreads();

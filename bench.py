@@ -67,25 +67,32 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []          # (host time, csv line)
+        self.window = None       # (t0, t1) host times of the timed region
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)      # let the sampler start before the timed region
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0: float, t1: float):
+        """Host times bracketing the timed region; samples within 50 ms of it are kept."""
+        self.window = (t0 - 0.05, t1 + 0.05)
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -95,7 +102,9 @@ class ClockSampler:
     def summary(self):
         sms, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if self.window and not (self.window[0] <= ts <= self.window[1]):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -299,7 +308,7 @@ def main():
                                            p.lda, Bh, tb, p.ldb, be.ctypes.data, Ch, tc,
                                            p.ldc, p.batch, 0, 0)
 
-    def timed(math_mode, steps, warmup, profile=False):
+    def timed(math_mode, steps, warmup, profile=False, clk=None):
         S.set_math_mode(math_mode)
         S.set_sync_mode(False)
         for _ in range(warmup):
@@ -310,6 +319,7 @@ def main():
         torch.cuda.synchronize()
         S.set_profiling(profile)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.time()
         with torch.cuda.stream(stream):
             e0.record(stream)
             for _ in range(steps):
@@ -317,6 +327,8 @@ def main():
                 assert st == 0, st
             e1.record(stream)
         torch.cuda.synchronize()
+        if clk is not None:
+            clk.mark(t0, time.time())
         ms = e0.elapsed_time(e1) / steps
         prof = S.get_profile() if profile else {}
         S.set_profiling(False)
@@ -352,7 +364,7 @@ def main():
         mm = {"ozaki": S.SSBLAS_MATH_FP64_OZAKI, "plain": S.SSBLAS_MATH_PLAIN, "bf16x3": S.SSBLAS_MATH_FP32_BF16X3}[md]
         err = error_of(mm)
         with ClockSampler(local) as clk:
-            ms, _, info = timed(mm, args.steps, args.warmup)
+            ms, _, info = timed(mm, args.steps, args.warmup, clk=clk)
         _, prof, _ = timed(mm, max(3, args.steps // 2), 1, profile=True)
         results[md] = dict(ms=ms, err=err, info=info, prof=prof, clocks=clk.summary())
 

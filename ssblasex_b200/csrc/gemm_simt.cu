@@ -59,10 +59,13 @@ struct SimtArgs {
   typename RowTraits<T>::S alpha, beta;
 };
 
-// BM x BN tile, BK deep; NT threads; each thread TM x TN outputs.
-// One BM x BN tile of instance b at (m0, n0).
-template <typename T, int BM, int BN, int BK, int TM, int TN>
+// One BM x BN tile of instance b at (m0, n0), BK deep; each thread computes TM x TN outputs.
+// LAY = (op(A) is T) + 2 * (op(B) is T) when known at compile time (then the staging loads have
+// no layout branches), or -1 to read the layout from args.
+template <typename T, int BM, int BN, int BK, int TM, int TN, int LAY>
 __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long m0, long n0) {
+  const bool a_n = LAY >= 0 ? (LAY & 1) == 0 : args.transa == SSBLAS_OP_N;
+  const bool b_n = LAY >= 0 ? (LAY & 2) == 0 : args.transb == SSBLAS_OP_N;
   using Tr = RowTraits<T>;
   using AB = typename Tr::AB;
   using Acc = typename Tr::Acc;
@@ -89,24 +92,24 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
       for (int e = 0; e < A_PER; ++e) {
         int idx = tid + e * NT;
         int ii, kk;
-        if (args.transa == SSBLAS_OP_N) { ii = idx % BM; kk = idx / BM; }   // rows contiguous
+        if (a_n) { ii = idx % BM; kk = idx / BM; }   // rows contiguous
         else { kk = idx % BK; ii = idx / BK; }                              // k contiguous
         long gi = m0 + ii, gk = k0 + kk;
         AB v = AB(0);
         if (gi < args.m && gk < args.k)
-          v = (args.transa == SSBLAS_OP_N) ? A[gi + gk * args.lda] : A[gi * args.lda + gk];
+          v = (a_n) ? A[gi + gk * args.lda] : A[gi * args.lda + gk];
         ra[e] = v;
       }
 #pragma unroll
       for (int e = 0; e < B_PER; ++e) {
         int idx = tid + e * NT;
         int jj, kk;
-        if (args.transb == SSBLAS_OP_N) { kk = idx % BK; jj = idx / BK; }   // k contiguous
+        if (b_n) { kk = idx % BK; jj = idx / BK; }   // k contiguous
         else { jj = idx % BN; kk = idx / BN; }                              // cols contiguous
         long gj = n0 + jj, gk = k0 + kk;
         AB v = AB(0);
         if (gj < args.n && gk < args.k)
-          v = (args.transb == SSBLAS_OP_N) ? B[gk + gj * args.ldb] : B[gk * args.ldb + gj];
+          v = (b_n) ? B[gk + gj * args.ldb] : B[gk * args.ldb + gj];
         rb[e] = v;
       }
     };
@@ -115,7 +118,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
       for (int e = 0; e < A_PER; ++e) {
         int idx = tid + e * NT;
         int ii, kk;
-        if (args.transa == SSBLAS_OP_N) { ii = idx % BM; kk = idx / BM; }
+        if (a_n) { ii = idx % BM; kk = idx / BM; }
         else { kk = idx % BK; ii = idx / BK; }
         As[buf][kk][ii] = ra[e];
       }
@@ -123,7 +126,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
       for (int e = 0; e < B_PER; ++e) {
         int idx = tid + e * NT;
         int jj, kk;
-        if (args.transb == SSBLAS_OP_N) { kk = idx % BK; jj = idx / BK; }
+        if (b_n) { kk = idx % BK; jj = idx / BK; }
         else { jj = idx % BN; kk = idx / BN; }
         Bs[buf][kk][jj] = rb[e];
       }
@@ -158,36 +161,35 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
       __syncthreads();
     }
 
-    // epilogue: all reads of C (beta != 0) are issued before the first store, so they overlap
+    // epilogue, one column of the thread's sub-tile at a time: its TM reads of C (beta != 0)
+    // are issued before its stores, so they overlap
     typename Tr::C* __restrict__ Cm = args.C[b];
-    typename Tr::C cv[TM][TN];
     const bool read_c = !(args.beta == typename Tr::S(0));
 #pragma unroll
-    for (int c = 0; c < TN; ++c)
+    for (int c = 0; c < TN; ++c) {
+      const long gj = n0 + ty + c * TY;
+      if (gj >= args.n) continue;
+      typename Tr::C cv[TM];
 #pragma unroll
       for (int r = 0; r < TM; ++r) {
-        const long gi = m0 + tx + r * TX, gj = n0 + ty + c * TY;
-        cv[r][c] = (read_c && gi < args.m && gj < args.n) ? Cm[gi + gj * args.ldc] : typename Tr::C(0);
+        const long gi = m0 + tx + r * TX;
+        cv[r] = (read_c && gi < args.m) ? Cm[gi + gj * args.ldc] : typename Tr::C(0);
       }
 #pragma unroll
-    for (int c = 0; c < TN; ++c) {
-      long gj = n0 + ty + c * TY;
-      if (gj >= args.n) continue;
-#pragma unroll
       for (int r = 0; r < TM; ++r) {
-        long gi = m0 + tx + r * TX;
-        if (gi < args.m) Cm[gi + gj * args.ldc] = Tr::epi(acc[r][c], args.alpha, args.beta, &cv[r][c]);
+        const long gi = m0 + tx + r * TX;
+        if (gi < args.m) Cm[gi + gj * args.ldc] = Tr::epi(acc[r][c], args.alpha, args.beta, &cv[r]);
       }
     }
   }
 }
 
-template <typename T, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN)) simt_gemm_kernel(SimtArgs<T> args) {
+template <typename T, int BM, int BN, int BK, int TM, int TN, int LAY>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) simt_gemm_kernel(SimtArgs<T> args) {
   const long tiles_m = (args.m + BM - 1) / BM;
   const long m0 = (blockIdx.x % tiles_m) * BM;
   const long n0 = (blockIdx.x / tiles_m) * BN;
-  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) simt_tile<T, BM, BN, BK, TM, TN>(args, b, m0, n0);
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) simt_tile<T, BM, BN, BK, TM, TN, LAY>(args, b, m0, n0);
 }
 
 // Grouped form: one CTA per (instance, tile) entry of the tile table.
@@ -203,7 +205,7 @@ simt_grouped_kernel(const SimtGInst* __restrict__ inst, const int* __restrict__ 
   a.A = A; a.B = B; a.C = C;
   if constexpr (sizeof(T) == 8) { a.alpha = g.alpha_d; a.beta = g.beta_d; }
   else { a.alpha = g.alpha_f; a.beta = g.beta_f; }
-  simt_tile<T, BM, BN, BK, TM, TN>(a, g.idx, (long)t[1] * BM, (long)t[2] * BN);
+  simt_tile<T, BM, BN, BK, TM, TN, -1>(a, g.idx, (long)t[1] * BM, (long)t[2] * BN);
 }
 
 template <typename T, int BM, int BN, int BK, int TM, int TN>
@@ -211,8 +213,14 @@ cudaError_t launch_tile(const SimtArgs<T>& a, cudaStream_t stream) {
   long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
   if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
   dim3 grid((unsigned)tiles, (unsigned)(a.batch < 65535 ? a.batch : 65535));
+  constexpr int NT = (BM / TM) * (BN / TN);
   ProfScope prof("simt_gemm", stream);
-  simt_gemm_kernel<T, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, stream>>>(a);
+  switch ((a.transa == SSBLAS_OP_T ? 1 : 0) + (a.transb == SSBLAS_OP_T ? 2 : 0)) {
+    case 0: simt_gemm_kernel<T, BM, BN, BK, TM, TN, 0><<<grid, NT, 0, stream>>>(a); break;
+    case 1: simt_gemm_kernel<T, BM, BN, BK, TM, TN, 1><<<grid, NT, 0, stream>>>(a); break;
+    case 2: simt_gemm_kernel<T, BM, BN, BK, TM, TN, 2><<<grid, NT, 0, stream>>>(a); break;
+    default: simt_gemm_kernel<T, BM, BN, BK, TM, TN, 3><<<grid, NT, 0, stream>>>(a); break;
+  }
   note_launch();
   return cudaGetLastError();
 }

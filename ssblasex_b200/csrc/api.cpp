@@ -471,6 +471,91 @@ static ssblasStatus_t grouped_device(
   return SSBLAS_STATUS_SUCCESS;
 }
 
+// Host matrices in equally spaced instances (the usual layout of a reference caller): the batch
+// is split into chunks whose host->device copies, kernels and device->host copies run on three
+// streams, so the copies of one chunk overlap the computation and the copies of the others and
+// both PCIe directions are busy at once. Returns SSBLAS_STATUS_NOT_COMPUTED_ERROR when the layout
+// does not qualify (the caller then stages the whole batch at once).
+static ssblasStatus_t run_host_pipelined(BatchDesc d, const void* const A[], const void* const B[],
+                                         void* const C[], size_t a_bytes, size_t b_bytes, size_t c_bytes,
+                                         size_t ec, cudaStream_t st) {
+  const long batch = d.batch;
+  const long sa = uniform_stride(A, batch), sb = uniform_stride(B, batch);
+  const long sc = uniform_stride((const void* const*)C, batch);
+  auto dense = [](long s, size_t bytes) { return s > 0 && (size_t)s >= bytes && (size_t)s <= 2 * bytes + 4096; };
+  if (!dense(sa, a_bytes) || !dense(sb, b_bytes) || !dense(sc, c_bytes)) return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
+
+  static cudaStream_t s_in = nullptr, s_out = nullptr;
+  constexpr int NCH = 4;
+  static cudaEvent_t ev_start = nullptr, ev_in[NCH], ev_cp[NCH];
+  cudaError_t e;
+  if (!s_in) {
+    if ((e = cudaStreamCreateWithFlags(&s_in, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&s_out, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming)))
+      return map_err(e);
+    for (int c = 0; c < NCH; ++c)
+      if ((e = cudaEventCreateWithFlags(&ev_in[c], cudaEventDisableTiming)) ||
+          (e = cudaEventCreateWithFlags(&ev_cp[c], cudaEventDisableTiming)))
+        return map_err(e);
+  }
+  const bool read_c = d.beta_d != 0.0 || d.beta_f != 0.0f || d.beta_i != 0;
+  char* dA = (char*)workspace(WS_STAGE_A, (size_t)sa * (batch - 1) + a_bytes, &e);
+  if (!dA) return map_err(e);
+  char* dB = (char*)workspace(WS_STAGE_B, (size_t)sb * (batch - 1) + b_bytes, &e);
+  if (!dB) return map_err(e);
+  char* dC = (char*)workspace(WS_STAGE_C, (size_t)sc * (batch - 1) + c_bytes, &e);
+  if (!dC) return map_err(e);
+  void** dp = (void**)workspace(WS_PTRS, 3 * sizeof(void*) * batch, &e);
+  if (!dp) return map_err(e);
+  void** hp = (void**)pinned(3 * sizeof(void*) * batch, &e);
+  if (!hp) return map_err(e);
+  for (long b = 0; b < batch; ++b) {
+    hp[b] = dA + (size_t)b * sa;
+    hp[batch + b] = dB + (size_t)b * sb;
+    hp[2 * batch + b] = dC + (size_t)b * sc;
+  }
+  if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * batch, cudaMemcpyHostToDevice, st))) return map_err(e);
+  pinned_done(st);
+  // the staging buffers may still be in use by earlier work on the library stream
+  if ((e = cudaEventRecord(ev_start, st)) || (e = cudaStreamWaitEvent(s_in, ev_start, 0))) return map_err(e);
+  d.strideA = sa; d.strideB = sb; d.strideC = sc;
+  const long per = (batch + NCH - 1) / NCH;
+  const size_t row_bytes = (size_t)d.m * ec, pitch = (size_t)d.ldc * ec;
+  for (int c = 0; c < NCH; ++c) {
+    const long b0 = c * per, b1 = b0 + per < batch ? b0 + per : batch;
+    if (b0 >= b1) break;
+    const long nb = b1 - b0;
+    if ((e = cudaMemcpyAsync(dA + (size_t)b0 * sa, A[b0], (size_t)sa * (nb - 1) + a_bytes, cudaMemcpyHostToDevice, s_in)) ||
+        (e = cudaMemcpyAsync(dB + (size_t)b0 * sb, B[b0], (size_t)sb * (nb - 1) + b_bytes, cudaMemcpyHostToDevice, s_in)))
+      return map_err(e);
+    if (read_c &&
+        (e = cudaMemcpyAsync(dC + (size_t)b0 * sc, C[b0], (size_t)sc * (nb - 1) + c_bytes, cudaMemcpyHostToDevice, s_in)))
+      return map_err(e);
+    if ((e = cudaEventRecord(ev_in[c], s_in)) || (e = cudaStreamWaitEvent(st, ev_in[c], 0))) return map_err(e);
+    BatchDesc sub = d;
+    sub.batch = nb;
+    sub.A = (const void* const*)(dp + b0);
+    sub.B = (const void* const*)(dp + batch + b0);
+    sub.C = (void* const*)(dp + 2 * batch + b0);
+    sub.A0 = dA + (size_t)b0 * sa; sub.B0 = dB + (size_t)b0 * sb; sub.C0 = dC + (size_t)b0 * sc;
+    if (nb == 1) sub.strideA = sub.strideB = sub.strideC = 0;
+    if ((e = dispatch(sub, st)) != cudaSuccess) return map_err(e);
+    if ((e = cudaEventRecord(ev_cp[c], st)) || (e = cudaStreamWaitEvent(s_out, ev_cp[c], 0))) return map_err(e);
+    // only the m x n part of each C goes back (the caller's ld padding stays untouched)
+    if ((size_t)sc == pitch * d.n) {
+      e = cudaMemcpy2DAsync(C[b0], pitch, dC + (size_t)b0 * sc, pitch, row_bytes, (size_t)d.n * nb,
+                            cudaMemcpyDeviceToHost, s_out);
+    } else {
+      for (long b = b0; b < b1 && e == cudaSuccess; ++b)
+        e = cudaMemcpy2DAsync(C[b], pitch, dC + (size_t)b * sc, pitch, row_bytes, d.n, cudaMemcpyDeviceToHost, s_out);
+    }
+    if (e != cudaSuccess) return map_err(e);
+  }
+  if ((e = cudaStreamSynchronize(s_out)) || (e = cudaStreamSynchronize(st))) return map_err(e);
+  return check_device_error(st);
+}
+
 static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t transb, SSINT m,
                                    SSINT n, SSINT k, const void* alpha, const void* const A[],
                                    ssblasDataType_t Atype, SSINT lda, const void* const B[],
@@ -553,6 +638,10 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
     } else {
       // host matrices, as the reference takes them: stage through device memory
       host_matrices = true;
+      if (batchCount >= 8) {
+        const ssblasStatus_t ps = run_host_pipelined(d, A, B, C, a_bytes, b_bytes, c_bytes, ec, st);
+        if (ps != SSBLAS_STATUS_NOT_COMPUTED_ERROR) return ps;
+      }
       if ((e = stage_operand(WS_STAGE_A, A, batchCount, a_bytes, true, st, da, &d.strideA)) ||
           (e = stage_operand(WS_STAGE_B, B, batchCount, b_bytes, true, st, db, &d.strideB)) ||
           (e = stage_operand(WS_STAGE_C, (const void* const*)C, batchCount, c_bytes,

@@ -59,20 +59,26 @@ __device__ __forceinline__ void load_regs(T (&v)[PER], const T* __restrict__ X, 
   }
 }
 
-// Writes staged bytes st[p][r][0..KT*bpe) of P planes as 16-byte vectors.
-template <int P, int BPE>
-__device__ __forceinline__ void write_out(const uint8_t* st, uint8_t* out, long plane_stride, long rows,
-                                          long Kp_bytes, long row0, long kbyte0) {
-  constexpr int SEGS = KT * BPE / 16;
+// Writes staged bytes st[p][r][0..ROWB) (row pitch ROWB + 4) of P planes as 16-byte vectors.
+template <int P, int ROWB>
+__device__ __forceinline__ void write_rows(const uint8_t* st, uint8_t* out, long plane_stride, long rows,
+                                           long Kp_bytes, long row0, long kbyte0) {
+  constexpr int SEGS = ROWB / 16;
   for (int it = threadIdx.x; it < P * RT * SEGS; it += NTH) {
     const int p = it / (RT * SEGS), rem = it % (RT * SEGS), r = rem / SEGS, sg = rem % SEGS;
     const long gr = row0 + r, gb = kbyte0 + 16 * sg;
     if (gr < rows && gb < Kp_bytes) {
-      const uint32_t* src = (const uint32_t*)(st + (p * RT + r) * (KT * BPE + 4) + 16 * sg);
+      const uint32_t* src = (const uint32_t*)(st + (p * RT + r) * (ROWB + 4) + 16 * sg);
       uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
       *(uint4*)(out + p * plane_stride + gr * Kp_bytes + gb) = w;
     }
   }
+}
+
+template <int P, int BPE>
+__device__ __forceinline__ void write_out(const uint8_t* st, uint8_t* out, long plane_stride, long rows,
+                                          long Kp_bytes, long row0, long kbyte0) {
+  write_rows<P, KT * BPE>(st, out, plane_stride, rows, Kp_bytes, row0, kbyte0);
 }
 
 __global__ void __launch_bounds__(NTH) pack_i8_kernel(PlaneArgs a) {
@@ -223,13 +229,19 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
 }
 
 // Two-kernel form of the slicing for large operands: a streaming pass that only finds the row
-// exponents, then one CTA per (instance, 32 rows, 64 k) chunk for the digits, so that every
-// chunk's loads are in flight at once instead of walking K inside a CTA.
-__global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a, int32_t* __restrict__ exps) {
+// exponents, then one CTA per (instance, 32 rows, 128 k) chunk for the digits, so that every
+// chunk's loads are in flight at once instead of walking K inside a CTA. Both kernels take two
+// operands (op(A) and op(B)): blocks [0, n0) work on the first, the rest on the second.
+__global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a0, int32_t* e0, long n0, PlaneArgs a1,
+                                                           int32_t* e1) {
   __shared__ double red[8][RT];
+  const bool second = blockIdx.x >= n0;
+  const PlaneArgs a = second ? a1 : a0;
+  int32_t* __restrict__ exps = second ? e1 : e0;
+  const long blk = second ? blockIdx.x - n0 : blockIdx.x;
   const long blocks_per_inst = (a.rows + RT - 1) / RT;
-  const long b = blockIdx.x / blocks_per_inst;
-  const long row0 = (blockIdx.x % blocks_per_inst) * RT;
+  const long b = blk / blocks_per_inst;
+  const long row0 = (blk % blocks_per_inst) * RT;
   const double* X = (const double*)a.X[b];
   double mx = 0.0;
   if (a.kcontig) {
@@ -279,24 +291,35 @@ __global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a, int32_t*
   }
 }
 
+constexpr int DKT = 128;                // k per digits chunk
+constexpr int DPER = RT * DKT / NTH;     // 16 elements per thread
+constexpr int DPITCH = DKT + 4;          // 33 words per staged row: conflict-free
+
 template <int S>
-__global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a, const int32_t* __restrict__ exps) {
-  __shared__ __align__(16) uint8_t st[S * RT * OPITCH];
+__global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const int32_t* e0, long n0, PlaneArgs a1,
+                                                           const int32_t* e1) {
+  __shared__ __align__(16) uint8_t st[S * RT * DPITCH];
   __shared__ double rscale[RT][2];
+  const bool second = blockIdx.x >= n0;
+  const PlaneArgs a = second ? a1 : a0;
+  const int32_t* __restrict__ exps = second ? e1 : e0;
+  const long blk = second ? blockIdx.x - n0 : blockIdx.x;
   const long blocks_per_inst = (a.rows + RT - 1) / RT;
-  const long kchunks = (a.K + KT - 1) / KT;
-  const long item = blockIdx.x / kchunks;
-  const long k0 = (blockIdx.x % kchunks) * KT;
+  const long kchunks = (a.K + DKT - 1) / DKT;
+  const long item = blk / kchunks;
+  const long k0 = (blk % kchunks) * DKT;
   const long b = item / blocks_per_inst;
   const long row0 = (item % blocks_per_inst) * RT;
   const double* X = (const double*)a.X[b];
   uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
-  // this thread's 8 elements: one row, two runs of 4 consecutive k, so that the 4 digits of a
+  // this thread's 16 elements: one row, four runs of 4 consecutive k, so that the 4 digits of a
   // run pack into one 32-bit shared-memory store per plane
   const int r = a.kcontig ? threadIdx.x / 8 : threadIdx.x % 32;
   auto kk_of = [&](int e) {
-    return a.kcontig ? (threadIdx.x % 8) * 8 + e : (threadIdx.x / 32) * 4 + (e % 4) + 32 * (e / 4);
+    return a.kcontig ? (threadIdx.x % 8) * 16 + e : (threadIdx.x / 32) * 4 + (e % 4) + 32 * (e / 4);
   };
+  constexpr int PER = DPER;
+  constexpr int OPITCH = DPITCH;
   double v[PER];
   {
     const long gr = row0 + r;
@@ -343,7 +366,7 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a, const in
     }
   }
   __syncthreads();
-  write_out<S, 1>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
+  write_rows<S, DKT>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
 }
 
 dim3 grid_of(const PlaneArgs& a) {
@@ -366,24 +389,53 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
+                                    cudaStream_t st) {
+  const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
+  const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);
+  if (items_a + items_b < 2L * num_sms() || chunks_a + chunks_b >= (1L << 31)) {
+    cudaError_t e = launch_ozaki_slice(a, slices, ea, st);
+    return e != cudaSuccess ? e : launch_ozaki_slice(b, slices, eb, st);
+  }
+  // enough rows to fill the GPU: exponents of both operands, then digits of both, per chunk
+  {
+    ProfScope prof("ozaki_rowexp", st);
+    ozaki_rowexp_kernel<<<(unsigned)(items_a + items_b), NTH, 0, st>>>(a, ea, items_a, b, eb);
+    note_launch();
+  }
+  ProfScope prof("ozaki_slice", st);
+  const unsigned g = (unsigned)(chunks_a + chunks_b);
+  switch (slices) {
+    case 3: ozaki_digits_kernel<3><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 4: ozaki_digits_kernel<4><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 5: ozaki_digits_kernel<5><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 6: ozaki_digits_kernel<6><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 7: ozaki_digits_kernel<7><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 8: ozaki_digits_kernel<8><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    default: return cudaErrorInvalidValue;
+  }
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
   const long items = (a.rows + RT - 1) / RT * a.batch;
-  const long chunks = items * ((a.K + KT - 1) / KT);
+  const long chunks = items * ((a.K + DKT - 1) / DKT);
   if (items >= 2L * num_sms() && chunks < (1L << 31)) {
     // enough rows to fill the GPU: the two-kernel form (exponents, then digits per chunk)
     {
       ProfScope prof("ozaki_rowexp", st);
-      ozaki_rowexp_kernel<<<(unsigned)items, NTH, 0, st>>>(a, exps);
+      ozaki_rowexp_kernel<<<(unsigned)items, NTH, 0, st>>>(a, exps, items, a, exps);
       note_launch();
     }
     ProfScope prof("ozaki_slice", st);
     switch (slices) {
-      case 3: ozaki_digits_kernel<3><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
-      case 4: ozaki_digits_kernel<4><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
-      case 5: ozaki_digits_kernel<5><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
-      case 6: ozaki_digits_kernel<6><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
-      case 7: ozaki_digits_kernel<7><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
-      case 8: ozaki_digits_kernel<8><<<(unsigned)chunks, NTH, 0, st>>>(a, exps); break;
+      case 3: ozaki_digits_kernel<3><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 4: ozaki_digits_kernel<4><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 5: ozaki_digits_kernel<5><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 6: ozaki_digits_kernel<6><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 7: ozaki_digits_kernel<7><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 8: ozaki_digits_kernel<8><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
       default: return cudaErrorInvalidValue;
     }
     note_launch();

@@ -209,8 +209,7 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   if (!ex) return e;
   PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * S};
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * S};
-  if ((e = launch_ozaki_slice(a, S, ex, st)) != cudaSuccess) return e;
-  if ((e = launch_ozaki_slice(b, S, ex + d.m * d.batch, st)) != cudaSuccess) return e;
+  if ((e = launch_ozaki_slice_pair(a, ex, b, ex + d.m * d.batch, S, st)) != cudaSuccess) return e;
   return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
 }
 

@@ -83,6 +83,28 @@ def test_against_restated_oracle(S, row, ta, tb):
         assert O.normalized_error(p, C_o, rows=range(0, 203, 7)) <= tol
 
 
+@pytest.mark.parametrize("row,mode", [("f32", 0), ("f64", 0), ("i8", 0), ("f64", 1), ("f32", 2)])
+def test_host_matrices_pipelined(S, row, mode):
+    """Host matrices (the reference's convention) in a batch large enough for the chunked,
+    overlapped staging: the same result as with device pointers, and the callers' ld padding of
+    C is untouched."""
+    from ssblasex_b200 import runner, workloads as W
+    S.set_math_mode(mode)
+    try:
+        al, be = (2, -1) if row == "i8" else (0.75, 0.5)
+        p = W.make_problem(row, 1, 0, 100, 70, 130, 13, al, be, lda=136, ldb=136, ldc=104, seed=70 + mode,
+                           dist="expspread" if row == "f64" else "uniform")
+        st, C_host = runner.call(p, mode="host_matrices")
+        assert st == 0
+        st, C_dev = runner.call(p, mode="device_array")
+        assert st == 0
+        np.testing.assert_array_equal(C_host.view(np.uint8), C_dev.view(np.uint8))
+        pad = C_host.reshape(p.batch, p.n, p.ldc)[:, :, p.m:]
+        np.testing.assert_array_equal(pad, p.C.reshape(p.batch, p.n, p.ldc)[:, :, p.m:])
+    finally:
+        S.set_math_mode(0)
+
+
 def test_beta_zero_never_reads_c(S):
     """C full of NaN with beta = 0 gives finite results (C is not read)."""
     from ssblasex_b200 import runner, workloads as W

@@ -103,7 +103,11 @@ typedef enum {
   SSBLAS_PATH_I8_TCGEN05 = 2,      /* int8 -> int32 on tcgen05.mma kind::i8, TMA staging */
   SSBLAS_PATH_OZAKI_TCGEN05 = 3,   /* fp64 via int8 slices on tcgen05.mma kind::i8 */
   SSBLAS_PATH_BF16X3_TCGEN05 = 4,  /* fp32 via three BF16 split products, tcgen05 kind::f16 */
-  SSBLAS_PATH_GROUPED = 5          /* grouped persistent launch */
+  SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch */
+  SSBLAS_PATH_DMMA = 6,            /* plain fp64 on the FP64 tensor cores (mma.sync f64) */
+  SSBLAS_PATH_OZAKI_SLICER = 7     /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
+                                      pre-pass (0: one pass with thread-block clusters when
+                                      k <= 2048, 1: exponent pass then digit pass) */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

@@ -33,7 +33,8 @@ SSBLAS_COMPUTE_DEFAULT = 0
 
 # extensions
 SSBLAS_MATH_PLAIN, SSBLAS_MATH_FP64_OZAKI, SSBLAS_MATH_FP32_BF16X3 = 0, 1, 2
-PATH_NAMES = {0: "none", 1: "simt", 2: "i8_tcgen05", 3: "ozaki_tcgen05", 4: "bf16x3_tcgen05", 5: "grouped"}
+PATH_NAMES = {0: "none", 1: "simt", 2: "i8_tcgen05", 3: "ozaki_tcgen05", 4: "bf16x3_tcgen05", 5: "grouped",
+              6: "dmma"}
 
 EXPORTED_SYMBOLS = (
     "ssblasGemmBatchedEx", "ssblasGemmBatchedEx_64", "ssblasGemmGroupedBatchedEx",
@@ -154,7 +155,8 @@ def get_profile() -> dict:
     return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(n.value)}
 
 
-PATH_IDS = {"simt": 1, "i8_tcgen05": 2, "ozaki_tcgen05": 3, "bf16x3_tcgen05": 4, "grouped": 5}
+PATH_IDS = {"simt": 1, "i8_tcgen05": 2, "ozaki_tcgen05": 3, "bf16x3_tcgen05": 4, "grouped": 5, "dmma": 6,
+            "ozaki_slicer": 7}
 
 
 def set_kernel_config(path: str, config: int) -> int:

@@ -38,9 +38,12 @@ FAMILIES = {
         dict(row="i8", transa=1, transb=0, m=256, n=256, k=1024, batch=512, alpha=1, beta=0,
              lda=1024, ldb=1024, ldc=256),
     ]),
-    "simt": (SSBLAS_MATH_PLAIN, [0, 1], "simt_gemm", [
+    "dmma": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4], "dmma_gemm", [
         dict(row="f64", transa=0, transb=1, m=1024, n=1024, k=1024, batch=32, alpha=1.0, beta=0.0,
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
+        dict(row="f64", transa=1, transb=0, m=128, n=128, k=128, batch=256, alpha=1.0, beta=0.5),
+    ]),
+    "simt": (SSBLAS_MATH_PLAIN, [0, 1], "simt_gemm", [
         dict(row="f32", transa=0, transb=0, m=128, n=128, k=128, batch=64, alpha=1.0, beta=0.5),
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),

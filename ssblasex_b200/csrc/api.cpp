@@ -366,6 +366,10 @@ static cudaError_t dispatch(const BatchDesc& d, cudaStream_t st) {
     int s = settings().ozaki_slices;
     cudaError_t e = launch_ozaki_f64(d, s, st);
     if (e != cudaErrorNotSupported) return e;
+  } else if (d.row == ROW_F64 && choose_config(SSBLAS_PATH_DMMA, d.m, d.n, d.k, d.batch, 0) != 2) {
+    // plain fp64: DMMA tiles (configuration 2 selects the DFMA SIMT kernel instead)
+    note_path(SSBLAS_PATH_DMMA);
+    return launch_dmma_f64(d, st);
   } else if (d.row == ROW_F32 && (mode & SSBLAS_MATH_FP32_BF16X3)) {
     cudaError_t e = launch_bf16x3_f32(d, st);
     if (e != cudaErrorNotSupported) {

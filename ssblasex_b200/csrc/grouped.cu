@@ -25,6 +25,7 @@
 
 #include "grouped.h"
 #include "internal.h"
+#include "ozaki_digits.cuh"
 #include "tc_gemm.cuh"
 
 namespace ssb {
@@ -59,7 +60,6 @@ template <int MODE, int S, int KB, int RTILE_A, int RTILE_B>
 __global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict__ items, uint8_t* __restrict__ outA,
                                                     uint8_t* __restrict__ outB, int32_t* __restrict__ exps) {
   constexpr int P = MODE == 0 ? 1 : MODE == 1 ? 2 : S;
-  constexpr int ES = MODE == 0 ? 1 : MODE == 1 ? 4 : 8;     // input element size
   constexpr int KE = MODE == 1 ? KB / 2 : KB;               // K elements per block
   const GPrepInst it = items[blockIdx.x];
   const bool is_b = (blockIdx.x & 1) != 0;
@@ -70,9 +70,6 @@ __global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict_
   const long kpad = (long)it.nk * KE;
   __shared__ double rmax[GRT];
   __shared__ double rscale[GRT][2];
-  unsigned long long bias = 0;
-#pragma unroll
-  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
 
   for (long r0 = 0; r0 < rows_pad; r0 += GRT) {
     if (MODE == 2) {
@@ -152,25 +149,11 @@ __global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict_
         *(__nv_bfloat162*)(chunk + RTILE * KB + so) = lv;
       } else {
         const double s0 = (gr < it.rows) ? rscale[r][0] : 0.0, s1 = (gr < it.rows) ? rscale[r][1] : 0.0;
-        uint32_t lo[4], hi[4];
+        // padding rows/columns are zero digits (value 0 gives Y = bias)
+        uint32_t wd[S];
+        digit_words<S>(vals, s0, s1, wd);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const unsigned long long Y = (unsigned long long)__double2ll_rn(vals[j] * s0 * s1) + bias;
-          lo[j] = (uint32_t)Y;
-          hi[j] = (uint32_t)(Y >> 32);
-        }
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const int byte = S - 1 - p;
-          uint32_t wv = 0;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const uint32_t src = byte < 4 ? (lo[j] >> (8 * byte)) : (hi[j] >> (8 * (byte - 4)));
-            wv |= (src & 255u) << (8 * j);
-          }
-          // padding rows/columns are zero digits (value 0 maps to bytes 0x80 before the flip)
-          *(uint32_t*)(chunk + (long)p * RTILE * KB + so) = wv ^ (p == 0 ? 0u : 0x80808080u);
-        }
+        for (int p = 0; p < P; ++p) *(uint32_t*)(chunk + (long)p * RTILE * KB + so) = wd[p];
       }
     }
     __syncthreads();

@@ -53,6 +53,8 @@ int* device_error_flag();
 
 // ---- kernel entry points (each returns a CUDA error code; launches on `stream`) ----
 cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream);
+// plain fp64 on the FP64 tensor cores (DMMA)
+cudaError_t launch_dmma_f64(const BatchDesc& d, cudaStream_t stream);
 // int8 -> int32 on tcgen05; returns cudaErrorNotSupported when the layout is not eligible.
 cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t stream);
 // fp64 via Ozaki int8 slices; slices = per-operand slice count

@@ -1,0 +1,68 @@
+// Ozaki digit arithmetic shared by the slicing kernels (prepass.cu) and the grouped pre-pass
+// (grouped.cu). A value x of a row with exponent e becomes X = rint(x * 2^(8S-2-e)) and its S
+// balanced base-256 digits d_0..d_{S-1}: with Y = X + 0x80..80 (128 added to each of the S-1 low
+// bytes), d_p = byte_{S-1-p}(Y) with its top bit flipped for p >= 1, d_0 = byte_{S-1}(Y).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ssb {
+
+// 4 x 4 byte transpose: out[b] holds byte b of w[0..3] (byte j of out[b] = byte b of w[j]).
+static __device__ __forceinline__ void byte_transpose4(const uint32_t (&w)[4], uint32_t (&out)[4]) {
+  const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[0], w[1], 0x7362);
+  const uint32_t t2 = __byte_perm(w[2], w[3], 0x5140), t3 = __byte_perm(w[2], w[3], 0x7362);
+  out[0] = __byte_perm(t0, t2, 0x5410);
+  out[1] = __byte_perm(t0, t2, 0x7632);
+  out[2] = __byte_perm(t1, t3, 0x5410);
+  out[3] = __byte_perm(t1, t3, 0x7632);
+}
+
+// Y = rint(x * s0 * s1) + bias (mod 2^64), s0 * s1 = 2^(8S-2-e), |x * s0 * s1| < 2^62, rounding
+// to nearest even -- computed with FP64 additions instead of a double -> int64 conversion (which
+// runs on the narrow XU pipe and would bound the slicing passes):
+//   v  = x * s0 * s1                 exact (power-of-two scaling)
+//   a  = v + 1.5*2^63                a in [2^63, 2^64), ulp 2^11: a = 1.5*2^63 + v1, v1 = v rounded
+//                                    to a multiple of 2^11, and the bits of a hold
+//                                    bits(1.5*2^63) + v1 / 2^11
+//   v2 = v - (a - 1.5*2^63)          exact, |v2| <= 2^10
+//   t2 = v2 + 1.5*2^52               the low word of t2 is rint(v2) (|v2| < 2^51)
+// rint(v) = v1 + rint(v2) (v1 is an even integer), so
+//   Y = (bits(a) << 11) + rint(v2) + bias - (bits(1.5*2^63) << 11)   (mod 2^64).
+static __device__ __forceinline__ unsigned long long slice_y(double x, double s0, double s1, unsigned long long bias) {
+  const double C1 = 0x1.8p63, M = 0x1.8p52;
+  const double v = __dmul_rn(__dmul_rn(x, s0), s1);
+  const double a = __dadd_rn(v, C1);
+  const double v2 = __dsub_rn(v, __dsub_rn(a, C1));
+  const int32_t r2 = (int32_t)__double2loint(__dadd_rn(v2, M));
+  return ((unsigned long long)__double_as_longlong(a) << 11) + (unsigned long long)(long long)r2 +
+         (bias - 0x4000000000000000ull);
+}
+
+// Digit words of 4 consecutive-k values of one row: word p holds digit p of the 4 values (the
+// value with the lowest k in the lowest byte). s0 * s1 = 2^(8S-2-e).
+template <int S>
+static __device__ __forceinline__ void digit_words(const double (&x)[4], double s0, double s1, uint32_t (&wd)[S]) {
+  unsigned long long bias = 0;
+#pragma unroll
+  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+  uint32_t lo[4], hi[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const unsigned long long Y = slice_y(x[i], s0, s1, bias);
+    lo[i] = (uint32_t)Y;
+    hi[i] = (uint32_t)(Y >> 32);
+  }
+  uint32_t L[4], H[4];
+  byte_transpose4(lo, L);
+  byte_transpose4(hi, H);
+#pragma unroll
+  for (int p = 0; p < S; ++p) {
+    const int byte = S - 1 - p;
+    const uint32_t w = byte < 4 ? L[byte] : H[byte - 4];
+    wd[p] = p > 0 ? (w ^ 0x80808080u) : w;
+  }
+}
+
+}  // namespace ssb

@@ -16,15 +16,26 @@
 // (src/include/ACopy/Xgemm_ncopy_sve_v4.hpp, src/include/BCopy/Xgemm_ncopy_sve_1.hpp), but they
 // run per K block inside the tile loop; here each operand is converted once per call.
 //
-// All three kernels follow the same memory plan: every thread issues its global loads for a
-// 32-row x 64-k tile back to back (coalesced along whichever of rows / k is contiguous), converts
-// in registers, transposes the output bytes through shared memory, and writes 16-byte vectors
-// along K. Several CTAs per SM keep enough loads in flight to run at HBM speed.
+// Memory plan: every thread issues all of its global loads for a tile back to back (coalesced
+// along whichever of rows / k is contiguous), converts in registers, transposes the output bytes
+// through shared memory, and writes 16-byte vectors along K. Several CTAs per SM keep enough
+// loads in flight to run at HBM speed.
+//
+// Ozaki slicing has three forms:
+//   K <= 2048   ozaki_cluster_kernel: one pass. A cluster of ceil(K/256) CTAs holds 32 whole rows
+//               in registers, exchanges the partial row maxima through distributed shared memory,
+//               and writes the digits: each operand is read once.
+//   K > 2048    ozaki_rowexp_kernel (row exponents) then ozaki_digits_kernel (one CTA per
+//               32 rows x 128 k chunk) when there are enough rows to fill the GPU, else
+//               ozaki_slice_kernel (both passes inside one CTA per 32 rows).
+// All forms pack the 4 digits of 4 consecutive k into one word per plane with a 4 x 4 byte
+// transpose (byte_perm), and produce identical planes.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "internal.h"
+#include "ozaki_digits.cuh"
 #include "prepass.h"
 
 namespace ssb {
@@ -210,8 +221,7 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
       for (int e = 0; e < PER; ++e) {
         int r, kk;
         tile_coord(a.kcontig, e, r, kk);
-        const unsigned long long Y =
-            (unsigned long long)__double2ll_rn(v[e] * rscale[r][0] * rscale[r][1]) + bias;
+        const unsigned long long Y = slice_y(v[e], rscale[r][0], rscale[r][1], bias);
         const uint32_t lo = (uint32_t)Y, hi = (uint32_t)(Y >> 32);
 #pragma unroll
         for (int p = 0; p < S; ++p) {
@@ -338,35 +348,318 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const i
     rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
   }
   __syncthreads();
-  unsigned long long bias = 0;
-#pragma unroll
-  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
   const double s0 = rscale[r][0], s1 = rscale[r][1];
 #pragma unroll
   for (int g = 0; g < PER / 4; ++g) {
-    uint32_t lo[4], hi[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const unsigned long long Y = (unsigned long long)__double2ll_rn(v[4 * g + j] * s0 * s1) + bias;
-      lo[j] = (uint32_t)Y;
-      hi[j] = (uint32_t)(Y >> 32);
-    }
+    uint32_t wd[S];
+    const double x[4] = {v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]};
+    digit_words<S>(x, s0, s1, wd);
     const int kk = kk_of(4 * g);
 #pragma unroll
-    for (int p = 0; p < S; ++p) {
-      const int byte = S - 1 - p;
-      uint32_t w = 0;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t src = byte < 4 ? (lo[j] >> (8 * byte)) : (hi[j] >> (8 * (byte - 4)));
-        w |= (src & 255u) << (8 * j);
-      }
-      if (p > 0) w ^= 0x80808080u;
-      *(uint32_t*)(st + (p * RT + r) * OPITCH + kk) = w;
-    }
+    for (int p = 0; p < S; ++p) *(uint32_t*)(st + (p * RT + r) * OPITCH + kk) = wd[p];
   }
   __syncthreads();
   write_rows<S, DKT>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
+}
+
+// Single-pass slicing for K <= 2048 with thread-block clusters. An item is 32 rows of one
+// instance; the CS = ceil(K/256) CTAs of a cluster share it, CTA q taking k in [256q, 256q + 256),
+// and the clusters are persistent (one CTA per SM, items strided over the clusters). Per item:
+//   the 32 x 256 fp64 tile, copied into shared memory by cp.async two items ahead, is read into
+//   registers (32 values per thread); partial row maxima go to this CTA's pmax[item parity];
+//   a cluster barrier; every CTA reads all CS partial maxima through distributed shared memory
+//   and derives the row exponents; the copies of the item two ahead are issued into the stage
+//   just read; the digits are staged [plane][row][k] in shared memory and written as 16-byte
+//   vectors (256 contiguous bytes per plane row).
+// Each operand is read from HBM once, and the next item's copies are in flight while the current
+// item is converted.
+//
+// Thread t owns row r and 8 runs of 4 consecutive k: k = 256q + 4c + 32j + i (j < 8, i < 4), with
+//   rows contiguous in memory (element (r, k) at X[r + k*ld]):  r = t % 32, c = t / 32; the tile
+//     is staged [k][32 rows] (256 contiguous bytes per k);
+//   k contiguous (element (r, k) at X[r*ld + k]):               r = t / 8,  c = t % 8; the tile is
+//     staged [32 rows][k].
+constexpr int CL_ROWS = 32;
+constexpr int CL_K = 256;
+constexpr int CL_PW = CL_K / 4 + 4;                    // staged digit words per row (16-byte aligned)
+constexpr int CL_TILE = CL_ROWS * CL_K;                // fp64 values per stage
+
+template <int S>
+constexpr int cluster_smem_bytes() {
+  return 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4 + 8 * CL_ROWS * 8 + 2 * CL_ROWS * 8 + CL_ROWS * 16;
+}
+
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ double ld_cluster_f64(const double* local, uint32_t rank) {
+  uint32_t a = (uint32_t)__cvta_generic_to_shared(local), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(remote) : "r"(a), "r"(rank));
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(remote) : "memory");
+  return v;
+}
+__device__ __forceinline__ void cpa16(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+struct ClusterItem {
+  bool second;     // the item belongs to the second operand
+  long b, row0;
+};
+
+__device__ __forceinline__ ClusterItem cluster_item(long item, const PlaneArgs& a0, int32_t* e0, long n0,
+                                                    const PlaneArgs& a1, int32_t* e1) {
+  ClusterItem ci;
+  ci.second = item >= n0;
+  const long rows = ci.second ? a1.rows : a0.rows;
+  const long rb = ci.second ? item - n0 : item;
+  const long bpi = (rows + CL_ROWS - 1) / CL_ROWS;
+  ci.b = rb / bpi;
+  ci.row0 = (rb % bpi) * CL_ROWS;
+  return ci;
+}
+
+// Copies this CTA's 32 x 256 slab of an item into a stage (zero outside the matrix).
+__device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, const ClusterItem& ci, long kbase) {
+  const double* X = (const double*)a.X[ci.b];
+  const int t = threadIdx.x;
+  const bool vec = (((uintptr_t)X) % 16 == 0) && (a.ld % 2 == 0);
+  if (!a.kcontig) {
+    // [k][32 rows]: chunk = 2 rows at one k
+#pragma unroll 4
+    for (int q = 0; q < CL_TILE / 2 / NTH; ++q) {
+      const int ch = t + q * NTH, kl = ch / 16, rp = 2 * (ch % 16);
+      const long gr = ci.row0 + rp, gk = kbase + kl;
+      const long nr = (gk < a.K) ? (a.rows - gr >= 2 ? 2 : (a.rows - gr > 0 ? a.rows - gr : 0)) : 0;
+      const double* src = nr > 0 ? X + gr + gk * a.ld : X;
+      double* dst = stage + kl * CL_ROWS + rp;
+      if (vec) {
+        cpa16(dst, src, (int)(8 * nr));
+      } else {
+        cpa8(dst, src, nr > 0 ? 8 : 0);
+        cpa8(dst + 1, nr > 1 ? src + 1 : X, nr > 1 ? 8 : 0);
+      }
+    }
+  } else {
+    // [32 rows][k]: chunk = 2 consecutive k of one row
+#pragma unroll 4
+    for (int q = 0; q < CL_TILE / 2 / NTH; ++q) {
+      const int ch = t + q * NTH, rl = ch / (CL_K / 2), kp = 2 * (ch % (CL_K / 2));
+      const long gr = ci.row0 + rl, gk = kbase + kp;
+      const long nk = (gr < a.rows) ? (a.K - gk >= 2 ? 2 : (a.K - gk > 0 ? a.K - gk : 0)) : 0;
+      const double* src = nk > 0 ? X + gr * a.ld + gk : X;
+      double* dst = stage + rl * CL_K + kp;
+      if (vec) {
+        cpa16(dst, src, (int)(8 * nk));
+      } else {
+        cpa8(dst, src, nk > 0 ? 8 : 0);
+        cpa8(dst + 1, nk > 1 ? src + 1 : X, nk > 1 ? 8 : 0);
+      }
+    }
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(PlaneArgs a0, int32_t* e0, long n0, PlaneArgs a1,
+                                                               int32_t* e1, long n_items, int CS) {
+  extern __shared__ __align__(16) uint8_t dyn[];
+  double* stages = (double*)dyn;                                                   // [2][CL_TILE]
+  uint32_t* st = (uint32_t*)(dyn + 2 * CL_TILE * 8);                               // [S][32][CL_PW]
+  double* red = (double*)(dyn + 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4);        // [8][32]
+  double* pmax = red + 8 * CL_ROWS;                                                // [2][32]
+  double* rscale = pmax + 2 * CL_ROWS;                                             // [32][2]
+
+  const int rank = (int)(blockIdx.x % CS);           // rank in the cluster (cluster dims CS x 1 x 1)
+  const long cluster = blockIdx.x / CS, nclusters = gridDim.x / CS;
+  const long kbase = (long)rank * CL_K;
+  const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+  unsigned long long bias = 0;
+#pragma unroll
+  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+
+  // prologue: the first two items of this cluster
+  for (int s = 0; s < 2; ++s) {
+    const long item = cluster + s * nclusters;
+    if (item < n_items) {
+      const ClusterItem ci = cluster_item(item, a0, e0, n0, a1, e1);
+      cluster_load(stages + s * CL_TILE, ci.second ? a1 : a0, ci, kbase);
+    }
+    cpa_commit();
+  }
+
+  long iter = 0;
+  for (long item = cluster; item < n_items; item += nclusters, ++iter) {
+    const int s = (int)(iter & 1);
+    const ClusterItem ci = cluster_item(item, a0, e0, n0, a1, e1);
+    const PlaneArgs a = ci.second ? a1 : a0;
+    int32_t* __restrict__ exps = ci.second ? e1 : e0;
+    const int r = a.kcontig ? t / 8 : lane;
+    const int c = a.kcontig ? t % 8 : warp;
+    cpa_wait1();
+    __syncthreads();
+    const double* tile = stages + s * CL_TILE;
+    double v[32];
+    if (a.kcontig) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double2 x0 = *(const double2*)(tile + r * CL_K + 4 * c + 32 * j);
+        const double2 x1 = *(const double2*)(tile + r * CL_K + 4 * c + 32 * j + 2);
+        v[4 * j] = x0.x; v[4 * j + 1] = x0.y; v[4 * j + 2] = x1.x; v[4 * j + 3] = x1.y;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 32 * j + i) * CL_ROWS + r];
+    }
+
+    // partial row maxima of this CTA's K range
+    double mx = 0.0;
+#pragma unroll
+    for (int e = 0; e < 32; ++e) mx = fmax(mx, fabs(v[e]));
+    double* pm = pmax + s * CL_ROWS;
+    if (a.kcontig) {
+#pragma unroll
+      for (int off = 1; off < 8; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (c == 0) pm[r] = mx;
+    } else {
+      red[warp * CL_ROWS + lane] = mx;
+      __syncthreads();
+      if (t < CL_ROWS) {
+        double m2 = red[t];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) m2 = fmax(m2, red[w * CL_ROWS + t]);
+        pm[t] = m2;
+      }
+    }
+    cluster_arrive();   // every CTA's pmax[s] is visible after the wait
+    cluster_wait();
+    if (t < CL_ROWS) {
+      double m2 = 0.0;
+      for (int q = 0; q < CS; ++q) m2 = fmax(m2, ld_cluster_f64(pm + t, (uint32_t)q));
+      int e = 0;
+      if (m2 > 0.0) frexp(m2, &e);
+      if (rank == 0 && ci.row0 + t < a.rows) exps[ci.b * a.rows + ci.row0 + t] = e;
+      // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
+      const int sh = 8 * S - 2 - e;
+      const int h1 = sh / 2;
+      rscale[2 * t] = ldexp(1.0, h1);
+      rscale[2 * t + 1] = ldexp(1.0, sh - h1);
+    }
+    __syncthreads();   // rscale visible; stage s fully read; the previous write-out is done
+
+    // the item two ahead goes into the stage just read
+    {
+      const long nxt = item + 2 * nclusters;
+      if (nxt < n_items) {
+        const ClusterItem cn = cluster_item(nxt, a0, e0, n0, a1, e1);
+        cluster_load(stages + s * CL_TILE, cn.second ? a1 : a0, cn, kbase);
+      }
+      cpa_commit();
+    }
+
+    // digits: one 32-bit word per plane per run of 4 k, staged [p][r][k/4]
+    const double s0 = rscale[2 * r], s1 = rscale[2 * r + 1];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      uint32_t wd[S];
+      const double x[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
+      digit_words<S>(x, s0, s1, wd);
+#pragma unroll
+      for (int p = 0; p < S; ++p) st[(p * CL_ROWS + r) * CL_PW + c + 8 * j] = wd[p];
+    }
+    __syncthreads();
+
+    // write-out: plane p, row r, this CTA's 256 bytes of K (k >= K holds zero digits, up to Kp)
+    uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride;
+    const long rows_here = a.rows - ci.row0;
+    constexpr int SEGS = CL_K / 16;
+#pragma unroll 2
+    for (int it = t; it < S * CL_ROWS * SEGS; it += NTH) {
+      const int p = it / (CL_ROWS * SEGS), rr = (it / SEGS) % CL_ROWS, sg = it % SEGS;
+      const long kb = kbase + 16L * sg;
+      if (rr < rows_here && kb < a.Kp) {
+        const uint4 w = *(const uint4*)(st + (p * CL_ROWS + rr) * CL_PW + 4 * sg);
+        *(uint4*)(out + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kb) = w;
+      }
+    }
+  }
+  cpa_wait0();
+  // no CTA leaves while another may still read its pmax
+  cluster_arrive();
+  cluster_wait();
+}
+
+template <int S>
+cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const PlaneArgs& a1, int32_t* e1, long n1,
+                             int CS, cudaStream_t st) {
+  constexpr int SMEM = cluster_smem_bytes<S>();
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(ozaki_cluster_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(NTH, 1, 1);
+  cfg.dynamicSmemBytes = SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)CS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  // persistent clusters: as many as fit at once (one CTA per SM), at most one per item
+  static int max_clusters[9] = {0};
+  if (max_clusters[CS] == 0) {
+    cfg.gridDim = dim3((unsigned)(CS * num_sms()), 1, 1);
+    int nc = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, ozaki_cluster_kernel<S>, &cfg);
+    if (e != cudaSuccess || nc <= 0) {
+      cudaGetLastError();
+      nc = num_sms() / CS;
+    }
+    max_clusters[CS] = nc > 0 ? nc : 1;
+  }
+  const long n_items = n0 + n1;
+  const long nclusters = n_items < max_clusters[CS] ? n_items : max_clusters[CS];
+  cfg.gridDim = dim3((unsigned)(nclusters * CS), 1, 1);
+  return cudaLaunchKernelEx(&cfg, ozaki_cluster_kernel<S>, a0, e0, n0, a1, e1, n_items, CS);
+}
+
+// K up to 2048 (clusters of at most 8 CTAs of 256 k each)
+bool cluster_kernel_fits(const PlaneArgs& a) { return a.K <= 8L * CL_K && a.Kp <= 8L * CL_K; }
+
+// One launch for one or two operands (with the same K).
+cudaError_t launch_ozaki_cluster(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
+                                 int slices, cudaStream_t st) {
+  const int CS = (int)((a0.Kp + CL_K - 1) / CL_K);
+  const long n0 = (a0.rows + CL_ROWS - 1) / CL_ROWS * a0.batch;
+  const long n1 = two ? (a1.rows + CL_ROWS - 1) / CL_ROWS * a1.batch : 0;
+  if ((n0 + n1) * CS >= (1L << 31) || CS < 1) return cudaErrorInvalidValue;
+  ProfScope prof("ozaki_slice", st);
+  cudaError_t e;
+  switch (slices) {
+    case 3: e = launch_cluster_s<3>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 4: e = launch_cluster_s<4>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 5: e = launch_cluster_s<5>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 6: e = launch_cluster_s<6>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 7: e = launch_cluster_s<7>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 8: e = launch_cluster_s<8>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  note_launch();
+  return e;
 }
 
 dim3 grid_of(const PlaneArgs& a) {
@@ -391,6 +684,9 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
 
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
                                     cudaStream_t st) {
+  // K up to 2048: one pass over both operands (unless the two-pass form is configured)
+  const bool one_pass = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0) == 0;
+  if (one_pass && cluster_kernel_fits(a) && b.K == a.K) return launch_ozaki_cluster(a, ea, b, eb, true, slices, st);
   const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
   const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);
   if (items_a + items_b < 2L * num_sms() || chunks_a + chunks_b >= (1L << 31)) {
@@ -419,6 +715,8 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
 }
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
+  const bool one_pass = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, a.rows, a.K, a.batch, 0) == 0;
+  if (one_pass && cluster_kernel_fits(a)) return launch_ozaki_cluster(a, exps, a, exps, false, slices, st);
   const long items = (a.rows + RT - 1) / RT * a.batch;
   const long chunks = items * ((a.K + DKT - 1) / DKT);
   if (items >= 2L * num_sms() && chunks < (1L << 31)) {

@@ -102,6 +102,26 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
+@pytest.mark.parametrize("ta,tb,m,n,k,batch", [
+    (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 CTAs, K contiguous, 16-byte loads
+    (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2, odd ld (8-byte loads)
+    (0, 1, 300, 33, 1030, 2),     # single pass, rows contiguous, ragged last row block
+    (0, 1, 64, 48, 2500, 2),      # K > 2048 with few rows: one-kernel slicer
+    (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows: exponent pass, then digit chunks
+])
+def test_ozaki_slicer_paths(S, ta, tb, m, n, k, batch):
+    """Every slicing kernel produces the planes the CPU restatement produces: the product is
+    bit-exact against oracle.ozaki_f64 whichever kernel sliced the operands."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", ta, tb, m, n, k, batch, 1.5, -0.5, seed=m + k, dist="expspread")
+    C = run(p)
+    assert S.last_run_info()["path"] == "ozaki_tcgen05"
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+
+
 def test_ozaki_zero_rows_and_tiny_shapes(S):
     from ssblasex_b200 import workloads as W
     S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
@@ -135,7 +155,8 @@ def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
 # ------------------------------------------------------------------------- configurations ---
 @pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2),
                                         ("i8_tcgen05", 0), ("i8_tcgen05", 1),
-                                        ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1)])
+                                        ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1),
+                                        ("dmma", 0), ("dmma", 1), ("dmma", 2), ("dmma", 3), ("dmma", 4)])
 def test_every_kernel_configuration(S, family, cfg):
     """Each configuration the autotuner may pick gives the right answer on a ragged problem."""
     from ssblasex_b200 import workloads as W
@@ -150,6 +171,14 @@ def test_every_kernel_configuration(S, family, cfg):
             p = W.make_problem("i8", 1, 0, 300, 170, 336, 3, 3, -1, lda=336, ldb=336, seed=50 + cfg)
             C = run(p)
             np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+        elif family == "dmma":
+            # plain fp64: DMMA tiles (0: 64x64, 1, 3, 4: 128x128) or the DFMA SIMT kernel (2)
+            S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+            p = W.make_problem("f64", 1, 1, 300, 170, 333, 3, 0.5, 2.0, seed=70 + cfg, dist="expspread")
+            C = run(p)
+            assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
+            assert S.last_run_info()["path"] == ("simt" if cfg == 2 else "dmma")
+            return
         else:
             S.set_math_mode(S.SSBLAS_MATH_FP32_BF16X3)
             p = W.make_problem("f32", 1, 0, 300, 170, 200, 2, 0.75, 0.25, seed=60 + cfg)
@@ -161,3 +190,39 @@ def test_every_kernel_configuration(S, family, cfg):
         assert S.last_run_info()["path"] == family
     finally:
         S.set_kernel_config(family, -1)
+
+
+# ------------------------------------------------------------------------- plain fp64 (DMMA)
+@pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_dmma_layouts_and_alignment(S, transa, transb, aligned):
+    """Plain fp64 on the DMMA tiles for every op(A)/op(B) pair, with 16-byte aligned instances and
+    even leading dimensions (16-byte copies) or instances at odd 8-byte offsets with odd leading
+    dimensions (8-byte copies), ragged edges in m, n and k, beta != 0."""
+    import torch
+    from ssblasex_b200 import workloads as W
+    m, n, k, batch = 131, 77, 203, 3
+    arows, brows = (m if transa == 0 else k), (k if transb == 0 else n)
+    pad = 0 if aligned else 1
+    lda, ldb, ldc = arows + (2 if aligned else 1), brows + (2 if aligned else 1), m + 3
+    p = W.make_problem("f64", transa, transb, m, n, k, batch, -1.25, 0.5, lda=lda, ldb=ldb, ldc=ldc,
+                       seed=80 + 2 * transa + transb)
+    bufs, ptrs = [], []
+    for X in (p.A, p.B, p.C):
+        per = X[0].size + pad
+        flat = torch.zeros(pad + per * batch, dtype=torch.float64, device="cuda")
+        for b in range(batch):
+            flat[pad + b * per: pad + b * per + X[b].size] = torch.from_numpy(X[b].reshape(-1))
+        bufs.append(flat)
+        ptrs.append((ct.c_void_p * batch)(*[flat.data_ptr() + 8 * (pad + b * per) for b in range(batch)]))
+    al, be = np.array([p.alpha]), np.array([p.beta])
+    st = S.lib().ssblasGemmBatchedEx(p.transa, p.transb, m, n, k, al.ctypes.data, ptrs[0], S.SSBLAS_R_64F, lda,
+                                     ptrs[1], S.SSBLAS_R_64F, ldb, be.ctypes.data, ptrs[2], S.SSBLAS_R_64F, ldc,
+                                     batch, 0, 0)
+    assert st == 0 and S.last_run_info()["path"] == "dmma"
+    flat = bufs[2].cpu().numpy()
+    per = p.C[0].size + pad
+    C = np.stack([flat[pad + b * per: pad + b * per + p.C[0].size] for b in range(batch)]).reshape(p.C.shape)
+    assert O.normalized_error(p, C) <= 4 * k * 2.0 ** -53
+    # rows m..ldc-1 of every column keep their value
+    np.testing.assert_array_equal(C.reshape(batch, n, ldc)[:, :, m:], p.C.reshape(batch, n, ldc)[:, :, m:])

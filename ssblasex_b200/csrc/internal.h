@@ -1,6 +1,7 @@
 // Internal interfaces shared by the host layer (api.cpp) and the kernel files.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -67,6 +68,12 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int slices, const int8_t* p
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t stream);
 
 int num_sms();
+
+// Tiled TMA tensor map of `rank` dimensions (dims[0] innermost; strides_bytes[i] is the stride
+// of dimension i + 1), box `box`, swizzle 0 / 32 / 64 / 128 bytes, zero fill outside the tensor.
+// False if the driver entry point is missing or the encoder rejects the arguments.
+bool make_tiled_map(CUtensorMap* map, CUtensorMapDataType dt, int rank, const void* base, const long* dims,
+                    const long* strides_bytes, const int* box, int swz_bytes);
 
 // Configuration index of a kernel family for a problem (tune.cpp): forced, tuned, or `fallback`.
 int choose_config(int path, long m, long n, long k, long batch, int fallback);

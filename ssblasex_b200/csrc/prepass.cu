@@ -22,9 +22,11 @@
 // loads in flight to run at HBM speed.
 //
 // Ozaki slicing has three forms:
-//   K <= 2048   ozaki_cluster_kernel: one pass. A cluster of ceil(K/256) CTAs holds 32 whole rows
-//               in registers, exchanges the partial row maxima through distributed shared memory,
-//               and writes the digits: each operand is read once.
+//   K <= 2048   ozaki_cluster_kernel: one pass, persistent thread-block clusters. The ceil(K/256)
+//               CTAs of a cluster share 32 rows, exchange their partial row maxima through
+//               distributed shared memory and write the digits; tiles arrive by TMA (equally
+//               spaced instances) or cp.async two items ahead, digit rows leave by bulk copies.
+//               Each operand is read once.
 //   K > 2048    ozaki_rowexp_kernel (row exponents) then ozaki_digits_kernel (one CTA per
 //               32 rows x 128 k chunk) when there are enough rows to fill the GPU, else
 //               ozaki_slice_kernel (both passes inside one CTA per 32 rows).
@@ -37,6 +39,7 @@
 #include "internal.h"
 #include "ozaki_digits.cuh"
 #include "prepass.h"
+#include "ptx.cuh"
 
 namespace ssb {
 namespace {
@@ -386,7 +389,7 @@ constexpr int CL_TILE = CL_ROWS * CL_K;                // fp64 values per stage
 
 template <int S>
 constexpr int cluster_smem_bytes() {
-  return 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4 + 8 * CL_ROWS * 8 + 2 * CL_ROWS * 8 + CL_ROWS * 16;
+  return 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4 + 8 * CL_ROWS * 8 + 2 * CL_ROWS * 8 + CL_ROWS * 16 + 16;
 }
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
@@ -467,32 +470,72 @@ __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, c
   }
 }
 
-template <int S>
-__global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(PlaneArgs a0, int32_t* e0, long n0, PlaneArgs a1,
-                                                               int32_t* e1, long n_items, int CS) {
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reinterpret_cast<uint64_t>(gdst)),
+               "r"((uint32_t)__cvta_generic_to_shared(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// TMA: the item's 32 x 256 tile of one operand through its 3-D tensor map (zero outside).
+__device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const CUtensorMap* tm, bool kcontig,
+                                            const ClusterItem& ci, long kbase) {
+  const uint32_t b = ptx::smem_u32(bar);
+  ptx::mbar_arrive_expect_tx(b, CL_TILE * 8);
+  if (kcontig) tma_load_3d(ptx::smem_u32(stage), tm, b, (int)kbase, (int)ci.row0, (int)ci.b);
+  else tma_load_3d(ptx::smem_u32(stage), tm, b, (int)ci.row0, (int)kbase, (int)ci.b);
+}
+
+// TMA: the tiles come through the operands' tensor maps (equally spaced, 16-byte aligned
+// instances), the wait is an mbarrier per stage; otherwise cp.async by every thread.
+template <int S, bool TMA>
+__global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
+                                                               const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
+                                                               int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
+                                                               long n_items, int CS, int* err) {
   extern __shared__ __align__(16) uint8_t dyn[];
   double* stages = (double*)dyn;                                                   // [2][CL_TILE]
   uint32_t* st = (uint32_t*)(dyn + 2 * CL_TILE * 8);                               // [S][32][CL_PW]
   double* red = (double*)(dyn + 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4);        // [8][32]
   double* pmax = red + 8 * CL_ROWS;                                                // [2][32]
   double* rscale = pmax + 2 * CL_ROWS;                                             // [32][2]
+  uint64_t* full = (uint64_t*)(rscale + 2 * CL_ROWS);                              // [2] (TMA)
 
   const int rank = (int)(blockIdx.x % CS);           // rank in the cluster (cluster dims CS x 1 x 1)
   const long cluster = blockIdx.x / CS, nclusters = gridDim.x / CS;
   const long kbase = (long)rank * CL_K;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
-  unsigned long long bias = 0;
-#pragma unroll
-  for (int j = 0; j < S - 1; ++j) bias |= 0x80ull << (8 * j);
+
+  if (TMA && t == 0) {
+    ptx::mbar_init(ptx::smem_u32(&full[0]), 1);
+    ptx::mbar_init(ptx::smem_u32(&full[1]), 1);
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
 
   // prologue: the first two items of this cluster
   for (int s = 0; s < 2; ++s) {
     const long item = cluster + s * nclusters;
     if (item < n_items) {
       const ClusterItem ci = cluster_item(item, a0, e0, n0, a1, e1);
-      cluster_load(stages + s * CL_TILE, ci.second ? a1 : a0, ci, kbase);
+      if (TMA) {
+        if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], ci.second ? &tm1 : &tm0,
+                                ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
+      } else {
+        cluster_load(stages + s * CL_TILE, ci.second ? a1 : a0, ci, kbase);
+      }
     }
-    cpa_commit();
+    if (!TMA) cpa_commit();
   }
 
   long iter = 0;
@@ -503,7 +546,14 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(PlaneArgs a0, int
     int32_t* __restrict__ exps = ci.second ? e1 : e0;
     const int r = a.kcontig ? t / 8 : lane;
     const int c = a.kcontig ? t % 8 : warp;
-    cpa_wait1();
+    if (TMA) {
+      // a wait that gives up records the error and carries on (every CTA of the cluster must
+      // take the same barriers, and every copy is waited for); the host reports the call as failed
+      ptx::mbar_wait(ptx::smem_u32(&full[s]), (uint32_t)((iter >> 1) & 1), err, 41);
+    } else {
+      cpa_wait1();
+    }
+    if (t < S * CL_ROWS) bulk_wait_read0();   // the previous item's digit rows have left st
     __syncthreads();
     const double* tile = stages + s * CL_TILE;
     double v[32];
@@ -554,16 +604,21 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(PlaneArgs a0, int
       rscale[2 * t] = ldexp(1.0, h1);
       rscale[2 * t + 1] = ldexp(1.0, sh - h1);
     }
-    __syncthreads();   // rscale visible; stage s fully read; the previous write-out is done
+    __syncthreads();   // rscale visible; stage s fully read into registers
 
     // the item two ahead goes into the stage just read
     {
       const long nxt = item + 2 * nclusters;
       if (nxt < n_items) {
         const ClusterItem cn = cluster_item(nxt, a0, e0, n0, a1, e1);
-        cluster_load(stages + s * CL_TILE, cn.second ? a1 : a0, cn, kbase);
+        if (TMA) {
+          if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], cn.second ? &tm1 : &tm0,
+                                  cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
+        } else {
+          cluster_load(stages + s * CL_TILE, cn.second ? a1 : a0, cn, kbase);
+        }
       }
-      cpa_commit();
+      if (!TMA) cpa_commit();
     }
 
     // digits: one 32-bit word per plane per run of 4 k, staged [p][r][k/4]
@@ -578,33 +633,42 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(PlaneArgs a0, int
     }
     __syncthreads();
 
-    // write-out: plane p, row r, this CTA's 256 bytes of K (k >= K holds zero digits, up to Kp)
-    uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride;
-    const long rows_here = a.rows - ci.row0;
-    constexpr int SEGS = CL_K / 16;
-#pragma unroll 2
-    for (int it = t; it < S * CL_ROWS * SEGS; it += NTH) {
-      const int p = it / (CL_ROWS * SEGS), rr = (it / SEGS) % CL_ROWS, sg = it % SEGS;
-      const long kb = kbase + 16L * sg;
-      if (rr < rows_here && kb < a.Kp) {
-        const uint4 w = *(const uint4*)(st + (p * CL_ROWS + rr) * CL_PW + 4 * sg);
-        *(uint4*)(out + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kb) = w;
+    // write-out: one bulk copy per (plane, row) of this CTA's 256 bytes of K (k >= K holds zero
+    // digits, up to Kp)
+    if (t < S * CL_ROWS) {
+      const int p = t / CL_ROWS, rr = t % CL_ROWS;
+      const long bytes = a.Kp - kbase < CL_K ? a.Kp - kbase : CL_K;
+      if (ci.row0 + rr < a.rows && bytes > 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kbase;
+        bulk_store(out, st + (p * CL_ROWS + rr) * CL_PW, (uint32_t)bytes);
       }
+      bulk_commit();
     }
   }
-  cpa_wait0();
+  if (t < S * CL_ROWS) bulk_wait0();
+  if (!TMA) cpa_wait0();
+  if (TMA && t == 0) {
+    // no copy may still be in flight when the CTA exits (bounded, like every wait here)
+    const long n_mine = iter;
+    for (long j = n_mine; j < n_mine + 2; ++j) {
+      const long item = cluster + j * nclusters;
+      if (item < n_items) ptx::mbar_wait(ptx::smem_u32(&full[j & 1]), (uint32_t)((j >> 1) & 1), err, 42);
+    }
+  }
   // no CTA leaves while another may still read its pmax
   cluster_arrive();
   cluster_wait();
 }
 
-template <int S>
-cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const PlaneArgs& a1, int32_t* e1, long n1,
-                             int CS, cudaStream_t st) {
+template <int S, bool TMA>
+cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, const PlaneArgs& a0, int32_t* e0,
+                              long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st) {
   constexpr int SMEM = cluster_smem_bytes<S>();
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(ozaki_cluster_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    cudaError_t e =
+        cudaFuncSetAttribute(ozaki_cluster_kernel<S, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -624,7 +688,7 @@ cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const Pl
   if (max_clusters[CS] == 0) {
     cfg.gridDim = dim3((unsigned)(CS * num_sms()), 1, 1);
     int nc = 0;
-    cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, ozaki_cluster_kernel<S>, &cfg);
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, ozaki_cluster_kernel<S, TMA>, &cfg);
     if (e != cudaSuccess || nc <= 0) {
       cudaGetLastError();
       nc = num_sms() / CS;
@@ -634,7 +698,36 @@ cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const Pl
   const long n_items = n0 + n1;
   const long nclusters = n_items < max_clusters[CS] ? n_items : max_clusters[CS];
   cfg.gridDim = dim3((unsigned)(nclusters * CS), 1, 1);
-  return cudaLaunchKernelEx(&cfg, ozaki_cluster_kernel<S>, a0, e0, n0, a1, e1, n_items, CS);
+  return cudaLaunchKernelEx(&cfg, ozaki_cluster_kernel<S, TMA>, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS,
+                            device_error_flag());
+}
+
+// 3-D map (innermost dimension first) over an equally spaced fp64 operand with a 32 x 256 box.
+bool slicer_map(CUtensorMap* m, const PlaneArgs& a) {
+  if (!a.X0 || a.xstride <= 0 || ((uintptr_t)a.X0 % 16) != 0 || (a.ld * 8) % 16 != 0 || a.xstride % 16 != 0)
+    return false;
+  if (a.rows >= (1L << 31) || a.K >= (1L << 31) || a.batch >= (1L << 31)) return false;
+  long dims[3], strides[2];
+  int box[3];
+  if (a.kcontig) {
+    dims[0] = a.K; dims[1] = a.rows; box[0] = CL_K; box[1] = CL_ROWS;
+  } else {
+    dims[0] = a.rows; dims[1] = a.K; box[0] = CL_ROWS; box[1] = CL_K;
+  }
+  dims[2] = a.batch; box[2] = 1;
+  strides[0] = a.ld * 8;
+  strides[1] = a.xstride;
+  return make_tiled_map(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, a.X0, dims, strides, box, 0);
+}
+
+template <int S>
+cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const PlaneArgs& a1, int32_t* e1, long n1,
+                             int CS, cudaStream_t st) {
+  CUtensorMap tm0, tm1;
+  const bool tma = slicer_map(&tm0, a0) && (n1 == 0 || slicer_map(&tm1, a1));
+  if (n1 == 0) tm1 = tm0;
+  if (tma) return launch_cluster_st<S, true>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  return launch_cluster_st<S, false>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
 }
 
 // K up to 2048 (clusters of at most 8 CTAs of 256 k each)

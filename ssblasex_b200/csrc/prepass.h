@@ -17,6 +17,10 @@ struct PlaneArgs {
   long Kp;                // padded K (elements) = row pitch of a plane
   long plane_stride;      // bytes between planes = rows * Kp * elem
   long batch_stride;      // bytes between instances = P * plane_stride
+  // When the instances are equally spaced (X[b] = X0 + b * xstride bytes), a pre-pass may address
+  // the whole batch through one tensor map; X0 = nullptr if not.
+  const void* X0 = nullptr;
+  long xstride = 0;
 };
 
 cudaError_t launch_pack_i8(const PlaneArgs& a, cudaStream_t st);

@@ -163,6 +163,26 @@ cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t
 
 }  // namespace
 
+bool make_tiled_map(CUtensorMap* map, CUtensorMapDataType dt, int rank, const void* base, const long* dims,
+                    const long* strides_bytes, const int* box, int swz_bytes) {
+  EncodeFn enc = encoder();
+  if (!enc || rank < 1 || rank > 5) return false;
+  cuuint64_t d[5], s[4];
+  cuuint32_t b[5], es[5];
+  for (int i = 0; i < rank; ++i) {
+    d[i] = (cuuint64_t)dims[i];
+    b[i] = (cuuint32_t)box[i];
+    es[i] = 1;
+    if (i + 1 < rank) s[i] = (cuuint64_t)strides_bytes[i];
+  }
+  CUtensorMapSwizzle sw = swz_bytes == 128  ? CU_TENSOR_MAP_SWIZZLE_128B
+                          : swz_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                          : swz_bytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                            : CU_TENSOR_MAP_SWIZZLE_NONE;
+  return enc(map, dt, (cuuint32_t)rank, const_cast<void*>(base), d, s, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (d.k > (1L << 31) || d.m > (1L << 31) || d.n > (1L << 31)) return cudaErrorNotSupported;
@@ -209,6 +229,8 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   if (!ex) return e;
   PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * S};
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * S};
+  if (d.A0 && (d.batch == 1 || d.strideA > 0)) { a.X0 = d.A0; a.xstride = d.batch == 1 ? 16 : d.strideA; }
+  if (d.B0 && (d.batch == 1 || d.strideB > 0)) { b.X0 = d.B0; b.xstride = d.batch == 1 ? 16 : d.strideB; }
   if ((e = launch_ozaki_slice_pair(a, ex, b, ex + d.m * d.batch, S, st)) != cudaSuccess) return e;
   return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
 }

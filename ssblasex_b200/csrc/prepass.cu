@@ -367,23 +367,28 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const i
 
 // Single-pass slicing for K <= 2048 with thread-block clusters. An item is 32 rows of one
 // instance; the CS = ceil(K/256) CTAs of a cluster share it, CTA q taking k in [256q, 256q + 256),
-// and the clusters are persistent (one CTA per SM, items strided over the clusters). Per item:
-//   the 32 x 256 fp64 tile, copied into shared memory by cp.async two items ahead, is read into
-//   registers (32 values per thread); partial row maxima go to this CTA's pmax[item parity];
-//   a cluster barrier; every CTA reads all CS partial maxima through distributed shared memory
-//   and derives the row exponents; the copies of the item two ahead are issued into the stage
-//   just read; the digits are staged [plane][row][k] in shared memory and written as 16-byte
-//   vectors (256 contiguous bytes per plane row).
-// Each operand is read from HBM once, and the next item's copies are in flight while the current
-// item is converted.
+// and the clusters are persistent (one 512-thread CTA per SM, items strided over the clusters).
+// Per item:
+//   the 32 x 256 fp64 tile -- brought into shared memory two items ahead, by TMA when the
+//   instances are equally spaced and 16-byte aligned, else by cp.async -- is read into registers
+//   (16 values per thread); partial row maxima go to this CTA's pmax[item parity]; a cluster
+//   barrier; every CTA reads all CS partial maxima through distributed shared memory and derives
+//   the row exponents; the copies of the item two ahead are issued into the stage just read; the
+//   digits are staged [plane][row][k] in shared memory and leave by one bulk copy per plane row
+//   (256 contiguous bytes).
+// Each operand is read from HBM once, and the next item's tile is in flight while the current
+// one is converted.
 //
-// Thread t owns row r and 8 runs of 4 consecutive k: k = 256q + 4c + 32j + i (j < 8, i < 4), with
-//   rows contiguous in memory (element (r, k) at X[r + k*ld]):  r = t % 32, c = t / 32; the tile
-//     is staged [k][32 rows] (256 contiguous bytes per k);
-//   k contiguous (element (r, k) at X[r*ld + k]):               r = t / 8,  c = t % 8; the tile is
-//     staged [32 rows][k].
+// Thread t (warp w, lane l) owns row r and 4 runs of 4 consecutive k: k = 256q + 4c + 64j + i
+// (j < 4, i < 4), with
+//   rows contiguous in memory (element (r, k) at X[r + k*ld]):  r = l % 16 + 16 (w % 2),
+//     c = l / 16 + 2 (w / 2); the tile is staged [k][32 rows] (256 contiguous bytes per k), so a
+//     half-warp reads 16 consecutive rows: no bank conflicts;
+//   k contiguous (element (r, k) at X[r*ld + k]):               r = t / 16, c = t % 16; the tile
+//     is staged [32 rows][k].
 constexpr int CL_ROWS = 32;
 constexpr int CL_K = 256;
+constexpr int CL_NTH = 512;
 constexpr int CL_PW = CL_K / 4 + 4;                    // staged digit words per row (16-byte aligned)
 constexpr int CL_TILE = CL_ROWS * CL_K;                // fp64 values per stage
 
@@ -393,6 +398,9 @@ constexpr int cluster_smem_bytes() {
 }
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+}
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ double ld_cluster_f64(const double* local, uint32_t rank) {
   uint32_t a = (uint32_t)__cvta_generic_to_shared(local), remote;
@@ -418,19 +426,19 @@ struct ClusterItem {
   long b, row0;
 };
 
-__device__ __forceinline__ ClusterItem cluster_item(long item, const PlaneArgs& a0, int32_t* e0, long n0,
-                                                    const PlaneArgs& a1, int32_t* e1) {
+// item -> (operand, instance, first row); 32-bit division (item counts are below 2^31)
+__device__ __forceinline__ ClusterItem cluster_item(long item, long n0, uint32_t bpi0, uint32_t bpi1) {
   ClusterItem ci;
   ci.second = item >= n0;
-  const long rows = ci.second ? a1.rows : a0.rows;
-  const long rb = ci.second ? item - n0 : item;
-  const long bpi = (rows + CL_ROWS - 1) / CL_ROWS;
-  ci.b = rb / bpi;
-  ci.row0 = (rb % bpi) * CL_ROWS;
+  const uint32_t rb = (uint32_t)(ci.second ? item - n0 : item);
+  const uint32_t bpi = ci.second ? bpi1 : bpi0;
+  const uint32_t b = rb / bpi;
+  ci.b = b;
+  ci.row0 = (long)(rb - b * bpi) * CL_ROWS;
   return ci;
 }
 
-// Copies this CTA's 32 x 256 slab of an item into a stage (zero outside the matrix).
+// cp.async: this CTA's 32 x 256 slab of an item into a stage (zero outside the matrix).
 __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, const ClusterItem& ci, long kbase) {
   const double* X = (const double*)a.X[ci.b];
   const int t = threadIdx.x;
@@ -438,8 +446,8 @@ __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, c
   if (!a.kcontig) {
     // [k][32 rows]: chunk = 2 rows at one k
 #pragma unroll 4
-    for (int q = 0; q < CL_TILE / 2 / NTH; ++q) {
-      const int ch = t + q * NTH, kl = ch / 16, rp = 2 * (ch % 16);
+    for (int q = 0; q < CL_TILE / 2 / CL_NTH; ++q) {
+      const int ch = t + q * CL_NTH, kl = ch / 16, rp = 2 * (ch % 16);
       const long gr = ci.row0 + rp, gk = kbase + kl;
       const long nr = (gk < a.K) ? (a.rows - gr >= 2 ? 2 : (a.rows - gr > 0 ? a.rows - gr : 0)) : 0;
       const double* src = nr > 0 ? X + gr + gk * a.ld : X;
@@ -454,8 +462,8 @@ __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, c
   } else {
     // [32 rows][k]: chunk = 2 consecutive k of one row
 #pragma unroll 4
-    for (int q = 0; q < CL_TILE / 2 / NTH; ++q) {
-      const int ch = t + q * NTH, rl = ch / (CL_K / 2), kp = 2 * (ch % (CL_K / 2));
+    for (int q = 0; q < CL_TILE / 2 / CL_NTH; ++q) {
+      const int ch = t + q * CL_NTH, rl = ch / (CL_K / 2), kp = 2 * (ch % (CL_K / 2));
       const long gr = ci.row0 + rl, gk = kbase + kp;
       const long nk = (gr < a.rows) ? (a.K - gk >= 2 ? 2 : (a.K - gk > 0 ? a.K - gk : 0)) : 0;
       const double* src = nk > 0 ? X + gr * a.ld + gk : X;
@@ -496,13 +504,11 @@ __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const 
   else tma_load_3d(ptx::smem_u32(stage), tm, b, (int)ci.row0, (int)kbase, (int)ci.b);
 }
 
-// TMA: the tiles come through the operands' tensor maps (equally spaced, 16-byte aligned
-// instances), the wait is an mbarrier per stage; otherwise cp.async by every thread.
 template <int S, bool TMA>
-__global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
-                                                               const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
-                                                               int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
-                                                               long n_items, int CS, int* err) {
+__global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
+                                                                  const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
+                                                                  int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
+                                                                  long n_items, int CS, int* err) {
   extern __shared__ __align__(16) uint8_t dyn[];
   double* stages = (double*)dyn;                                                   // [2][CL_TILE]
   uint32_t* st = (uint32_t*)(dyn + 2 * CL_TILE * 8);                               // [S][32][CL_PW]
@@ -515,6 +521,8 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
   const long cluster = blockIdx.x / CS, nclusters = gridDim.x / CS;
   const long kbase = (long)rank * CL_K;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+  const uint32_t bpi0 = (uint32_t)((a0.rows + CL_ROWS - 1) / CL_ROWS);
+  const uint32_t bpi1 = (uint32_t)((a1.rows + CL_ROWS - 1) / CL_ROWS);
 
   if (TMA && t == 0) {
     ptx::mbar_init(ptx::smem_u32(&full[0]), 1);
@@ -527,7 +535,7 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
   for (int s = 0; s < 2; ++s) {
     const long item = cluster + s * nclusters;
     if (item < n_items) {
-      const ClusterItem ci = cluster_item(item, a0, e0, n0, a1, e1);
+      const ClusterItem ci = cluster_item(item, n0, bpi0, bpi1);
       if (TMA) {
         if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], ci.second ? &tm1 : &tm0,
                                 ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
@@ -541,11 +549,11 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
   long iter = 0;
   for (long item = cluster; item < n_items; item += nclusters, ++iter) {
     const int s = (int)(iter & 1);
-    const ClusterItem ci = cluster_item(item, a0, e0, n0, a1, e1);
+    const ClusterItem ci = cluster_item(item, n0, bpi0, bpi1);
     const PlaneArgs a = ci.second ? a1 : a0;
     int32_t* __restrict__ exps = ci.second ? e1 : e0;
-    const int r = a.kcontig ? t / 8 : lane;
-    const int c = a.kcontig ? t % 8 : warp;
+    const int r = a.kcontig ? t / 16 : lane % 16 + 16 * (warp % 2);
+    const int c = a.kcontig ? t % 16 : lane / 16 + 2 * (warp / 2);
     if (TMA) {
       // a wait that gives up records the error and carries on (every CTA of the cluster must
       // take the same barriers, and every copy is waited for); the host reports the call as failed
@@ -556,32 +564,35 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
     if (t < S * CL_ROWS) bulk_wait_read0();   // the previous item's digit rows have left st
     __syncthreads();
     const double* tile = stages + s * CL_TILE;
-    double v[32];
+    double v[16];
     if (a.kcontig) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const double2 x0 = *(const double2*)(tile + r * CL_K + 4 * c + 32 * j);
-        const double2 x1 = *(const double2*)(tile + r * CL_K + 4 * c + 32 * j + 2);
+      for (int j = 0; j < 4; ++j) {
+        const double2 x0 = *(const double2*)(tile + r * CL_K + 4 * c + 64 * j);
+        const double2 x1 = *(const double2*)(tile + r * CL_K + 4 * c + 64 * j + 2);
         v[4 * j] = x0.x; v[4 * j + 1] = x0.y; v[4 * j + 2] = x1.x; v[4 * j + 3] = x1.y;
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 32 * j + i) * CL_ROWS + r];
+        for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 64 * j + i) * CL_ROWS + r];
     }
 
     // partial row maxima of this CTA's K range
     double mx = 0.0;
 #pragma unroll
-    for (int e = 0; e < 32; ++e) mx = fmax(mx, fabs(v[e]));
+    for (int e = 0; e < 16; ++e) mx = fmax(mx, fabs(v[e]));
     double* pm = pmax + s * CL_ROWS;
     if (a.kcontig) {
+      // the 16 threads of row r are lanes 16 (r % 2) .. +15 of warp r / 2
 #pragma unroll
-      for (int off = 1; off < 8; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      for (int off = 1; off < 16; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
       if (c == 0) pm[r] = mx;
     } else {
-      red[warp * CL_ROWS + lane] = mx;
+      // row r: lanes l and l + 16 of the 8 warps with w % 2 == r / 16
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+      if (lane < 16) red[(warp / 2) * CL_ROWS + r] = mx;
       __syncthreads();
       if (t < CL_ROWS) {
         double m2 = red[t];
@@ -610,7 +621,7 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
     {
       const long nxt = item + 2 * nclusters;
       if (nxt < n_items) {
-        const ClusterItem cn = cluster_item(nxt, a0, e0, n0, a1, e1);
+        const ClusterItem cn = cluster_item(nxt, n0, bpi0, bpi1);
         if (TMA) {
           if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], cn.second ? &tm1 : &tm0,
                                   cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
@@ -624,13 +635,15 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
     // digits: one 32-bit word per plane per run of 4 k, staged [p][r][k/4]
     const double s0 = rscale[2 * r], s1 = rscale[2 * r + 1];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < 4; ++j) {
       uint32_t wd[S];
       const double x[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
       digit_words<S>(x, s0, s1, wd);
 #pragma unroll
-      for (int p = 0; p < S; ++p) st[(p * CL_ROWS + r) * CL_PW + c + 8 * j] = wd[p];
+      for (int p = 0; p < S; ++p) st[(p * CL_ROWS + r) * CL_PW + c + 16 * j] = wd[p];
     }
+    // the bulk copies read st through the async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
     // write-out: one bulk copy per (plane, row) of this CTA's 256 bytes of K (k >= K holds zero
@@ -639,7 +652,6 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
       const int p = t / CL_ROWS, rr = t % CL_ROWS;
       const long bytes = a.Kp - kbase < CL_K ? a.Kp - kbase : CL_K;
       if (ci.row0 + rr < a.rows && bytes > 0) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kbase;
         bulk_store(out, st + (p * CL_ROWS + rr) * CL_PW, (uint32_t)bytes);
       }
@@ -650,14 +662,13 @@ __global__ void __launch_bounds__(NTH, 1) ozaki_cluster_kernel(const __grid_cons
   if (!TMA) cpa_wait0();
   if (TMA && t == 0) {
     // no copy may still be in flight when the CTA exits (bounded, like every wait here)
-    const long n_mine = iter;
-    for (long j = n_mine; j < n_mine + 2; ++j) {
+    for (long j = iter; j < iter + 2; ++j) {
       const long item = cluster + j * nclusters;
       if (item < n_items) ptx::mbar_wait(ptx::smem_u32(&full[j & 1]), (uint32_t)((j >> 1) & 1), err, 42);
     }
   }
   // no CTA leaves while another may still read its pmax
-  cluster_arrive();
+  cluster_arrive_relaxed();
   cluster_wait();
 }
 
@@ -673,7 +684,7 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
     attr = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.blockDim = dim3(NTH, 1, 1);
+  cfg.blockDim = dim3(CL_NTH, 1, 1);
   cfg.dynamicSmemBytes = SMEM;
   cfg.stream = st;
   cudaLaunchAttribute at[1];

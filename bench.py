@@ -130,6 +130,12 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
+# DRAM traffic per launch of the dominant kernel (dram__bytes_read.sum + dram__bytes_write.sum from
+# one ncu capture). The 32-instance launch is too large to capture under ncu, so an 8-instance
+# launch of the same kernel was captured (156 MB) and scaled by the instances it processes.
+NCU_TRAFFIC = {("f64_batch32_1024", "ozaki"): 156.0e6 * 4}
+
+
 def cpu_threads():
     n = os.cpu_count() or 1
     return n if n not in (2, 3, 4, 6) else 1
@@ -383,9 +389,20 @@ def main():
         ops = 2.0 * p.m * p.n * p.k * p.batch * pairs / launches_per_step
         int8_peak = 2.0 * pk["bf16_tflops"]
         achieved = ops / (per_launch_ms * 1e-3) / 1e12
+        traffic = NCU_TRAFFIC.get((args.workload, mode)) if p.batch == 32 else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TOPS (int8)",
-                "frac": achieved / int8_peak, "traffic": None, "kernel": dom_name,
+                "frac": achieved / int8_peak, "traffic": traffic, "kernel": dom_name,
                 "peak_source": f"2 x bf16_tflops ({pk['source']}): dense int8 rate is twice bf16 on B200"}
+        # the slicing pre-pass is HBM-bound: its algorithmic bytes are the fp64 operands read once
+        # and the int8 slices written once
+        sl = head["prof"].get("ozaki_slice")
+        if sl:
+            sl_bytes = (8.0 * (p.m + p.n) * p.k + head["info"]["slices"] * (p.m + p.n) * p.k) * p.batch
+            sl_ms = sl[1] / sl[0]
+            roof["pre_pass"] = {"kernel": "ozaki_slice", "bound": "hbm", "unit": "GB/s",
+                                "achieved": sl_bytes / (sl_ms * 1e-3) / 1e9, "peak": pk["hbm_gbs"],
+                                "frac": sl_bytes / (sl_ms * 1e-3) / 1e9 / pk["hbm_gbs"],
+                                "ms_per_launch": sl_ms}
     elif p.row == "i8":
         bytes_ = p.algorithmic_bytes() / launches_per_step
         achieved = bytes_ / (per_launch_ms * 1e-3) / 1e9

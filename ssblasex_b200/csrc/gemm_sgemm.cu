@@ -1,0 +1,245 @@
+// Plain FP32 batched GEMM (FFMA) with a cp.async pipeline, for the fp32 row in its plain form.
+//
+// Semantics follow the reference (hirokitokura/ssblasEx): C <- beta*C, not read when beta == 0
+// (src/include/CScale/Xgemm_scale_kernel.hpp:164-176), then C <- C + acc*alpha with one fused
+// multiply-add (src/include/GemmCore/Xgemm_kernel_sve_v4x5_1.hpp:93-127). The reference adds
+// alpha*acc once per 512-wide K block; here it is added once, which differs only by rounding.
+//
+// Design: one CTA per (BM x BN tile, instance). op(A) and op(B) tiles reach shared memory through
+// a STAGES-deep cp.async ring, always staged [k][mn] (mn contiguous) so that every thread reads
+// its TM (TN) consecutive values with 16-byte loads:
+//   - an operand whose rows (m or n) are contiguous in global memory is copied in 16-byte chunks
+//     along mn (when 16-byte aligned; 4-byte copies otherwise);
+//   - an operand whose K is contiguous is transposed by the copy itself: one 4-byte cp.async per
+//     element, consecutive threads taking consecutive k of one row.
+// Small problems (the 64^3 instances of a 4096-instance batch) keep the whole K in flight from
+// the start: with K <= STAGES * BK every stage is issued in the prologue.
+// Each thread owns a TM x TN block of C (rows tx*TM.., columns ty*TN..); a warp covers 4 x 8
+// threads, so its A reads are 4 distinct 16-byte vectors and its B reads 8 (broadcasts).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace ssb {
+namespace {
+
+struct SgemmArgs {
+  long m, n, k, lda, ldb, ldc, batch;
+  const float* const* A;
+  const float* const* B;
+  float* const* C;
+  float alpha, beta;
+};
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp16s(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp4s(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void commit_s() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void wait_s() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Copies the (ROWS x BK) slab of one operand at (r0, k0) into a stage buffer staged [k][r]
+// (pitch ROWS + 4 floats). MN: element (r, k) at X[r + k*ld]; otherwise at X[r*ld + k].
+template <int ROWS, int BK, int NT, bool MN>
+__device__ __forceinline__ void sload(float* dst, const float* __restrict__ X, long nrows, long K, long ld, long r0,
+                                      long k0, bool vec) {
+  constexpr int P = ROWS + 4;
+  const int t = threadIdx.x;
+  if (MN) {
+    if (vec) {
+      constexpr int CH = ROWS * BK / 4;   // 16-byte chunks along r
+#pragma unroll
+      for (int q = 0; q < (CH + NT - 1) / NT; ++q) {
+        const int idx = t + q * NT;
+        if (CH % NT != 0 && idx >= CH) break;
+        const int kk = idx / (ROWS / 4), rr = 4 * (idx % (ROWS / 4));
+        const long gr = r0 + rr, gk = k0 + kk;
+        long nv = (gk < K) ? nrows - gr : 0;
+        nv = nv < 0 ? 0 : (nv > 4 ? 4 : nv);
+        cp16s(saddr(dst + kk * P + rr), nv > 0 ? X + gr + gk * ld : X, (int)(4 * nv));
+      }
+    } else {
+      constexpr int EL = ROWS * BK;
+#pragma unroll
+      for (int q = 0; q < (EL + NT - 1) / NT; ++q) {
+        const int idx = t + q * NT;
+        if (EL % NT != 0 && idx >= EL) break;
+        const int kk = idx / ROWS, rr = idx % ROWS;
+        const long gr = r0 + rr, gk = k0 + kk;
+        const bool ok = gr < nrows && gk < K;
+        cp4s(saddr(dst + kk * P + rr), ok ? X + gr + gk * ld : X, ok ? 4 : 0);
+      }
+    }
+  } else {
+    // transpose by the copy: consecutive threads take consecutive k of one row
+    constexpr int EL = ROWS * BK;
+#pragma unroll
+    for (int q = 0; q < (EL + NT - 1) / NT; ++q) {
+      const int idx = t + q * NT;
+      if (EL % NT != 0 && idx >= EL) break;
+      const int rr = idx / BK, kk = idx % BK;
+      const long gr = r0 + rr, gk = k0 + kk;
+      const bool ok = gr < nrows && gk < K;
+      cp4s(saddr(dst + kk * P + rr), ok ? X + gr * ld + gk : X, ok ? 4 : 0);
+    }
+  }
+}
+
+template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_async_kernel(SgemmArgs args) {
+  constexpr int TX = BM / TM, TY = BN / TN, NT = TX * TY;
+  constexpr int PA = BM + 4, PB = BN + 4;
+  constexpr int STAGE = BK * (PA + PB);
+  extern __shared__ __align__(16) float sm[];
+
+  const long tiles_m = (args.m + BM - 1) / BM;
+  const long m0 = (blockIdx.x % tiles_m) * BM;
+  const long n0 = (blockIdx.x / tiles_m) * BN;
+  // warp = 4 (m) x 8 (n) threads
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  constexpr int WX = TX / 4;   // warps along m
+  const int tx = (warp % WX) * 4 + lane % 4;
+  const int ty = (warp / WX) * 8 + lane / 4;
+
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) {
+    const float* __restrict__ A = args.A[b];
+    const float* __restrict__ B = args.B[b];
+    const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
+    const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 4 == 0);
+    float acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
+
+    const long ktiles = (args.k + BK - 1) / BK;
+    auto issue = [&](long kt) {
+      float* sa = sm + (kt % STAGES) * STAGE;
+      float* sb = sa + BK * PA;
+      sload<BM, BK, NT, A_MN>(sa, A, args.m, args.k, args.lda, m0, kt * BK, vecA);
+      sload<BN, BK, NT, B_MN>(sb, B, args.n, args.k, args.ldb, n0, kt * BK, vecB);
+    };
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < ktiles) issue(s);
+      commit_s();
+    }
+    for (long kt = 0; kt < ktiles; ++kt) {
+      wait_s<STAGES - 2>();
+      __syncthreads();
+      if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
+      commit_s();
+      const float* sa = sm + (kt % STAGES) * STAGE;
+      const float* sb = sa + BK * PA;
+#pragma unroll 4
+      for (int kk = 0; kk < BK; ++kk) {
+        float av[TM], bv[TN];
+#pragma unroll
+        for (int i = 0; i < TM; i += 4) {
+          const float4 x = *(const float4*)(sa + kk * PA + tx * TM + i);
+          av[i] = x.x; av[i + 1] = x.y; av[i + 2] = x.z; av[i + 3] = x.w;
+        }
+#pragma unroll
+        for (int j = 0; j < TN; j += 4) {
+          const float4 x = *(const float4*)(sb + kk * PB + ty * TN + j);
+          bv[j] = x.x; bv[j + 1] = x.y; bv[j + 2] = x.z; bv[j + 3] = x.w;
+        }
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      }
+    }
+    wait_s<0>();
+    __syncthreads();   // the next instance's copies reuse the stage buffers
+
+    // epilogue: C rows m0 + tx*TM + i (contiguous per thread), columns n0 + ty*TN + j; 16-byte
+    // reads and writes when the thread's rows are inside C and C is 16-byte aligned
+    float* __restrict__ C = args.C[b];
+    const bool read_c = args.beta != 0.0f;
+    const long gi0 = m0 + tx * TM;
+    const bool cvec = (((uintptr_t)C) % 16 == 0) && (args.ldc % 4 == 0) && gi0 + TM <= args.m;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + ty * TN + j;
+      if (gj >= args.n) continue;
+      float* cp = C + gi0 + gj * args.ldc;
+      if (cvec) {
+        float4 cv[TM / 4];
+#pragma unroll
+        for (int i = 0; i < TM; i += 4) cv[i / 4] = read_c ? *(const float4*)(cp + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < TM; i += 4) {
+          float4 o;
+          o.x = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[i / 4].x : 0.0f);
+          o.y = fmaf(acc[i + 1][j], args.alpha, read_c ? args.beta * cv[i / 4].y : 0.0f);
+          o.z = fmaf(acc[i + 2][j], args.alpha, read_c ? args.beta * cv[i / 4].z : 0.0f);
+          o.w = fmaf(acc[i + 3][j], args.alpha, read_c ? args.beta * cv[i / 4].w : 0.0f);
+          *(float4*)(cp + i) = o;
+        }
+      } else {
+        float cv[TM];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) cv[i] = (read_c && gi0 + i < args.m) ? cp[i] : 0.0f;
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+          if (gi0 + i < args.m) cp[i] = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[i] : 0.0f);
+      }
+    }
+  }
+}
+
+template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB, bool A_MN, bool B_MN>
+cudaError_t launch_s(const SgemmArgs& a, cudaStream_t st) {
+  constexpr int NT = (BM / TM) * (BN / TN);
+  constexpr int SMEM = STAGES * BK * (BM + 4 + BN + 4) * 4;
+  auto kern = sgemm_async_kernel<BM, BN, BK, TM, TN, STAGES, MINB, A_MN, B_MN>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
+  if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)tiles, (unsigned)(a.batch < 65535 ? a.batch : 65535));
+  kern<<<grid, NT, SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB>
+cudaError_t launch_sl(const SgemmArgs& a, bool a_mn, bool b_mn, cudaStream_t st) {
+  if (a_mn && b_mn) return launch_s<BM, BN, BK, TM, TN, STAGES, MINB, true, true>(a, st);
+  if (a_mn) return launch_s<BM, BN, BK, TM, TN, STAGES, MINB, true, false>(a, st);
+  if (b_mn) return launch_s<BM, BN, BK, TM, TN, STAGES, MINB, false, true>(a, st);
+  return launch_s<BM, BN, BK, TM, TN, STAGES, MINB, false, false>(a, st);
+}
+
+}  // namespace
+
+cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t st) {
+  SgemmArgs a;
+  a.m = d.m; a.n = d.n; a.k = d.k; a.lda = d.lda; a.ldb = d.ldb; a.ldc = d.ldc; a.batch = d.batch;
+  a.A = (const float* const*)d.A;
+  a.B = (const float* const*)d.B;
+  a.C = (float* const*)d.C;
+  a.alpha = d.alpha_f;
+  a.beta = d.beta_f;
+  const bool a_mn = d.transa == SSBLAS_OP_N;   // op(A) rows (m) contiguous
+  const bool b_mn = d.transb == SSBLAS_OP_T;   // op(B) columns (n) contiguous
+  ProfScope prof("sgemm_async", st);
+  cudaError_t e;
+  // 3: 64 x 64 tiles, 256 threads of 4 x 4, 32-deep K stages x 2 (k <= 64 entirely in flight)
+  // 4: 128 x 128 tiles, 256 threads of 8 x 8, 16-deep K stages x 3
+  if (config == 4) e = launch_sl<128, 128, 16, 8, 8, 3, 1>(a, a_mn, b_mn, st);
+  else e = launch_sl<64, 64, 32, 4, 4, 2, 3>(a, a_mn, b_mn, st);
+  note_launch();
+  return e;
+}
+
+}  // namespace ssb

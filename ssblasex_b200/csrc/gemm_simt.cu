@@ -242,7 +242,11 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
   // them, small tiles otherwise (the tuning table or a forced configuration can override).
   const long big_tiles = ((d.m + 127) / 128) * ((d.n + 127) / 128) * d.batch;
   const bool big_default = d.m >= 128 && d.n >= 128 && big_tiles >= 2L * num_sms();
-  const bool big = choose_config(SSBLAS_PATH_SIMT, d.m, d.n, d.k, d.batch, big_default ? 1 : 0) == 1;
+  const int cfg = choose_config(SSBLAS_PATH_SIMT, d.m, d.n, d.k, d.batch,
+                                d.row == ROW_F32 ? (big_default ? 4 : 3) : (big_default ? 1 : 0));
+  // fp32: configurations 3 and 4 are the cp.async-pipelined kernel (gemm_sgemm.cu)
+  if (d.row == ROW_F32 && cfg >= 3) return launch_sgemm_async(d, cfg, stream);
+  const bool big = cfg == 1;
   switch (d.row) {
     case ROW_F32: {
       auto a = make_args<float>(d);

@@ -226,3 +226,45 @@ def test_dmma_layouts_and_alignment(S, transa, transb, aligned):
     assert O.normalized_error(p, C) <= 4 * k * 2.0 ** -53
     # rows m..ldc-1 of every column keep their value
     np.testing.assert_array_equal(C.reshape(batch, n, ldc)[:, :, m:], p.C.reshape(batch, n, ldc)[:, :, m:])
+
+
+# ------------------------------------------------------------------------- plain fp32 (cp.async)
+@pytest.mark.parametrize("cfg", [3, 4])
+@pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
+    """Plain fp32 on the cp.async-pipelined kernel (configuration 3: 64 x 64 tiles, 4: 128 x 128)
+    for every op(A)/op(B) pair, with 16-byte aligned instances and leading dimensions that are
+    multiples of 4 (16-byte copies) or instances at odd 4-byte offsets with odd leading dimensions
+    (4-byte copies), ragged edges in m, n and k, beta != 0."""
+    import torch
+    from ssblasex_b200 import workloads as W
+    m, n, k, batch = 141, 77, 203, 3
+    arows, brows = (m if transa == 0 else k), (k if transb == 0 else n)
+    pad = 0 if aligned else 1
+    lda, ldb, ldc = arows + (3 if aligned else 2), brows + (1 if aligned else 2), m + (3 if aligned else 2)
+    lda, ldb, ldc = ((lda + 3) // 4 * 4, (ldb + 3) // 4 * 4, (ldc + 3) // 4 * 4) if aligned else (lda | 1, ldb | 1, ldc | 1)
+    p = W.make_problem("f32", transa, transb, m, n, k, batch, 0.75, 0.25, lda=lda, ldb=ldb, ldc=ldc,
+                       seed=90 + 2 * transa + transb + 4 * cfg, dist="outliers")
+    bufs, ptrs = [], []
+    for X in (p.A, p.B, p.C):
+        per = X[0].size + pad
+        flat = torch.zeros(pad + per * batch, dtype=torch.float32, device="cuda")
+        for b in range(batch):
+            flat[pad + b * per: pad + b * per + X[b].size] = torch.from_numpy(X[b].reshape(-1))
+        bufs.append(flat)
+        ptrs.append((ct.c_void_p * batch)(*[flat.data_ptr() + 4 * (pad + b * per) for b in range(batch)]))
+    al, be = np.array([p.alpha], np.float32), np.array([p.beta], np.float32)
+    S.set_kernel_config("simt", cfg)
+    try:
+        st = S.lib().ssblasGemmBatchedEx(p.transa, p.transb, m, n, k, al.ctypes.data, ptrs[0], S.SSBLAS_R_32F, lda,
+                                         ptrs[1], S.SSBLAS_R_32F, ldb, be.ctypes.data, ptrs[2], S.SSBLAS_R_32F, ldc,
+                                         batch, 0, 0)
+        assert st == 0 and S.last_run_info()["path"] == "simt"
+    finally:
+        S.set_kernel_config("simt", -1)
+    flat = bufs[2].cpu().numpy()
+    per = p.C[0].size + pad
+    C = np.stack([flat[pad + b * per: pad + b * per + p.C[0].size] for b in range(batch)]).reshape(p.C.shape)
+    assert O.normalized_error(p, C) <= 4 * k * 2.0 ** -24
+    np.testing.assert_array_equal(C.reshape(batch, n, ldc)[:, :, m:], p.C.reshape(batch, n, ldc)[:, :, m:])

@@ -52,109 +52,166 @@ struct GPrepInst {
   long eoff;             // exponent offset (Ozaki)
 };
 
-constexpr int GRT = 32;   // rows per pass
+constexpr int GRT = 32;   // rows per work item
 constexpr int GNT = 256;
 
-// One CTA per (instance, operand). MODE 0: int8 copy; 1: BF16 hi/lo; 2: Ozaki slices (S planes).
+// One CTA per work item = (operand of an instance, block of 32 rows of its padded row range).
+// MODE 0: int8 copy (1 plane); 1: BF16 hi/lo (2 planes); 2: Ozaki slices (S planes).
+//
+// The item's rows are converted in K chunks of KC elements. Each thread handles runs of 4
+// consecutive k of one row; with the rows contiguous in memory (element (r, k) at X[r + k*ld]) the
+// 32 lanes of a warp take the 32 rows (coalesced loads), with K contiguous the lanes take
+// consecutive runs of one row. Ozaki items first find their row maxima over all of K (the second
+// read, for the digits, mostly hits the caches: an item is at most 32 x 16384 values and usually
+// 32 x 512). The converted words are staged per (K block, plane) as [32 rows][KB + 4 bytes]
+// (conflict-free word stores) and leave as 16-byte vectors into the pre-swizzled tile layout the
+// grouped GEMM stages with bulk copies: for each (row tile, K block) of the instance, P planes of
+// [RTILE rows][KB bytes], 16-byte chunks permuted by the hardware swizzle of a KB-byte span.
 template <int MODE, int S, int KB, int RTILE_A, int RTILE_B>
-__global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict__ items, uint8_t* __restrict__ outA,
-                                                    uint8_t* __restrict__ outB, int32_t* __restrict__ exps) {
+__global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
+                                                    uint8_t* __restrict__ outA, uint8_t* __restrict__ outB,
+                                                    int32_t* __restrict__ exps) {
   constexpr int P = MODE == 0 ? 1 : MODE == 1 ? 2 : S;
-  constexpr int KE = MODE == 1 ? KB / 2 : KB;               // K elements per block
-  const GPrepInst it = items[blockIdx.x];
-  const bool is_b = (blockIdx.x & 1) != 0;
+  constexpr int OB = MODE == 1 ? 2 : 1;                     // output bytes per element and plane
+  constexpr int KE = KB / OB;                               // K elements per block
+  constexpr int KC = MODE == 0 ? 128 : 64;                  // K elements per chunk
+  constexpr int NKB = KC / KE;                              // K blocks per chunk
+  constexpr int RPR = KC / 4;                               // runs of 4 k per row and chunk
+  constexpr int PER = GRT * RPR / GNT;                      // runs per thread and chunk
+  constexpr int PB = KB + 4;                                // staged row pitch (bytes)
+  static_assert(NKB >= 1 && PER >= 1 && RPR >= 8, "chunk shape");
+  __shared__ __align__(16) uint8_t stage[NKB * P * GRT * PB];
+  __shared__ double red[8][GRT];
+  __shared__ double rscale[GRT][2];
+
+  const uint2 wk = work[blockIdx.x];
+  const GPrepInst it = items[wk.x];
+  const bool is_b = (wk.x & 1) != 0;
   const int RTILE = is_b ? RTILE_B : RTILE_A;
   uint8_t* out = (is_b ? outB : outA) + it.off;
   const uint8_t* X = (const uint8_t*)it.X[it.idx];
-  const long rows_pad = (long)it.tiles * RTILE;
+  const long gr0 = (long)wk.y * GRT;                        // first row (of the padded range)
+  const int rt = (int)(gr0 / RTILE), rr0 = (int)(gr0 % RTILE);
   const long kpad = (long)it.nk * KE;
-  __shared__ double rmax[GRT];
-  __shared__ double rscale[GRT][2];
+  const int t = threadIdx.x, lane = t % 32, warp = t / 32;
 
-  for (long r0 = 0; r0 < rows_pad; r0 += GRT) {
-    if (MODE == 2) {
-      if (threadIdx.x < GRT) rmax[threadIdx.x] = 0.0;
-      __syncthreads();
-      // row maxima: 8 threads per row stride over K
-      const int r = threadIdx.x / 8, part = threadIdx.x % 8;
-      const long gr = r0 + r;
-      double mx = 0.0;
-      if (gr < it.rows) {
-        const double* Xd = (const double*)X;
-        for (long k = part; k < it.K; k += 8)
-          mx = fmax(mx, fabs(it.kcontig ? Xd[gr * it.ld + k] : Xd[gr + k * it.ld]));
-      }
-#pragma unroll
-      for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (part == 0) rmax[r] = mx;
-      __syncthreads();
-      if (threadIdx.x < GRT) {
-        int e = 0;
-        if (rmax[threadIdx.x] > 0.0) frexp(rmax[threadIdx.x], &e);
-        const long g2 = r0 + threadIdx.x;
-        if (g2 < it.rows) exps[it.eoff + g2] = e;
-        const int sh = 8 * S - 2 - e;
-        const int h1 = sh / 2;
-        rscale[threadIdx.x][0] = ldexp(1.0, h1);
-        rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
-      }
-      __syncthreads();
+  // (row, first k) of this thread's q-th run in a chunk
+  auto run_of = [&](int q, int& r, int& kl) {
+    if (it.kcontig) {
+      const int idx = t + q * GNT;
+      r = idx / RPR;
+      kl = 4 * (idx % RPR);
+    } else {
+      r = lane;
+      kl = 4 * (warp + 8 * q);
     }
-    // each thread emits 4 output bytes per plane: (row, 4 consecutive int8 k) or (row, 2 bf16 k)
-    constexpr int EPW = MODE == 1 ? 2 : 4;          // elements per 4-byte word
-    const long words_per_row = kpad / EPW;
-    for (long w = threadIdx.x; w < GRT * words_per_row; w += GNT) {
-      const int r = (int)(w / words_per_row);
-      const long kw = w % words_per_row;
-      const long gr = r0 + r;
-      if (gr >= rows_pad) break;
-      const long k0 = kw * EPW;
-      const int rt = (int)(gr / RTILE), rr = (int)(gr % RTILE);
-      const long kb = k0 / KE;
-      const int cbyte = (int)((k0 % KE) * (MODE == 1 ? 2 : 1));
-      uint8_t* chunk = out + ((long)rt * it.nk + kb) * (long)P * RTILE * KB;
-      const uint32_t so = swz(rr, cbyte, KB);
-      double vals[4];
+  };
+  auto load = [&](long gr, long k) -> double {
+    if (gr >= it.rows || k >= it.K) return 0.0;
+    const long off = it.kcontig ? gr * it.ld + k : gr + k * it.ld;
+    if (MODE == 0) return (double)((const int8_t*)X)[off];
+    if (MODE == 1) return (double)((const float*)X)[off];
+    return ((const double*)X)[off];
+  };
+
+  if (MODE == 2) {
+    // row maxima over all of K
+    double mx[PER];
 #pragma unroll
-      for (int j = 0; j < EPW; ++j) {
-        const long k = k0 + j;
-        double v = 0.0;
-        if (gr < it.rows && k < it.K) {
-          if (MODE == 0) {
-            const int8_t* Xi = (const int8_t*)X;
-            v = (double)(it.kcontig ? Xi[gr * it.ld + k] : Xi[gr + k * it.ld]);
-          } else if (MODE == 1) {
-            const float* Xf = (const float*)X;
-            v = (double)(it.kcontig ? Xf[gr * it.ld + k] : Xf[gr + k * it.ld]);
-          } else {
-            const double* Xd = (const double*)X;
-            v = it.kcontig ? Xd[gr * it.ld + k] : Xd[gr + k * it.ld];
-          }
-        }
-        vals[j] = v;
+    for (int q = 0; q < PER; ++q) mx[q] = 0.0;
+    for (long k0 = 0; k0 < it.K; k0 += KC) {
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        int r, kl;
+        run_of(q, r, kl);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) mx[q] = fmax(mx[q], fabs(load(gr0 + r, k0 + kl + i)));
       }
+    }
+    if (it.kcontig) {
+      // the RPR threads of a row are consecutive lanes
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+#pragma unroll
+        for (int off = 1; off < RPR && off < 32; off <<= 1) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
+        int r, kl;
+        run_of(q, r, kl);
+        if (kl == 0) red[0][r] = mx[q];
+      }
+    } else {
+      double m = mx[0];
+#pragma unroll
+      for (int q = 1; q < PER; ++q) m = fmax(m, mx[q]);
+      red[warp][lane] = m;
+    }
+    __syncthreads();
+    if (t < GRT) {
+      double m2 = red[0][t];
+      if (!it.kcontig)
+        for (int w = 1; w < 8; ++w) m2 = fmax(m2, red[w][t]);
+      int e = 0;
+      if (m2 > 0.0) frexp(m2, &e);
+      if (gr0 + t < it.rows) exps[it.eoff + gr0 + t] = e;
+      const int sh = 8 * S - 2 - e;
+      const int h1 = sh / 2;
+      rscale[t][0] = ldexp(1.0, h1);
+      rscale[t][1] = ldexp(1.0, sh - h1);
+    }
+    __syncthreads();
+  }
+
+  for (long k0 = 0; k0 < kpad; k0 += KC) {
+    // convert PER runs per thread into the staging buffer
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      int r, kl;
+      run_of(q, r, kl);
+      double x[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) x[i] = load(gr0 + r, k0 + kl + i);
+      const int kb = kl / KE, cbyte = (kl % KE) * OB;
+      uint8_t* row = stage + (kb * P) * GRT * PB + r * PB + cbyte;
       if (MODE == 0) {
-        uint32_t wv = 0;
+        uint32_t w = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) wv |= ((uint32_t)(uint8_t)(int8_t)vals[j]) << (8 * j);
-        *(uint32_t*)(chunk + so) = wv;
+        for (int i = 0; i < 4; ++i) w |= ((uint32_t)(uint8_t)(int8_t)x[i]) << (8 * i);
+        *(uint32_t*)row = w;
       } else if (MODE == 1) {
-        const float x0 = (float)vals[0], x1 = (float)vals[1];
-        const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-        const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-        const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-        __nv_bfloat162 hv, lv;
-        hv.x = h0; hv.y = h1; lv.x = l0; lv.y = l1;
-        *(__nv_bfloat162*)(chunk + so) = hv;
-        *(__nv_bfloat162*)(chunk + RTILE * KB + so) = lv;
-      } else {
-        const double s0 = (gr < it.rows) ? rscale[r][0] : 0.0, s1 = (gr < it.rows) ? rscale[r][1] : 0.0;
-        // padding rows/columns are zero digits (value 0 gives Y = bias)
-        uint32_t wd[S];
-        digit_words<S>(vals, s0, s1, wd);
+        __nv_bfloat16 h[4], l[4];
 #pragma unroll
-        for (int p = 0; p < P; ++p) *(uint32_t*)(chunk + (long)p * RTILE * KB + so) = wd[p];
+        for (int i = 0; i < 4; ++i) {
+          const float f = (float)x[i];
+          h[i] = __float2bfloat16_rn(f);
+          l[i] = __float2bfloat16_rn(f - __bfloat162float(h[i]));
+        }
+        __nv_bfloat162 h01, h23, l01, l23;
+        h01.x = h[0]; h01.y = h[1]; h23.x = h[2]; h23.y = h[3];
+        l01.x = l[0]; l01.y = l[1]; l23.x = l[2]; l23.y = l[3];
+        *(__nv_bfloat162*)row = h01;
+        *(__nv_bfloat162*)(row + 4) = h23;
+        *(__nv_bfloat162*)(row + GRT * PB) = l01;
+        *(__nv_bfloat162*)(row + GRT * PB + 4) = l23;
+      } else {
+        // rows beyond the matrix are zero digits (a zero value gives Y = bias)
+        uint32_t wd[S];
+        digit_words<S>(x, rscale[r][0], rscale[r][1], wd);
+#pragma unroll
+        for (int p = 0; p < P; ++p) *(uint32_t*)(row + p * GRT * PB) = wd[p];
       }
+    }
+    __syncthreads();
+    // write-out: per (K block, plane), 32 rows x KB bytes of the tile, 16-byte chunks swizzled
+    constexpr int CPR = KB / 16;                       // 16-byte chunks per row
+    constexpr int NCH = NKB * P * GRT * CPR;
+    for (int ch = t; ch < NCH; ch += GNT) {
+      const int c = ch % CPR, r = (ch / CPR) % GRT, bp = ch / (CPR * GRT);
+      const int kb = bp / P, pl = bp % P;
+      const long kbg = k0 / KE + kb;
+      if (kbg >= it.nk) continue;
+      const uint32_t* src = (const uint32_t*)(stage + bp * GRT * PB + r * PB + 16 * c);
+      const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+      uint8_t* chunk = out + ((long)rt * it.nk + kbg) * (long)P * RTILE * KB + (long)pl * RTILE * KB;
+      *(uint4*)(chunk + swz(rr0 + r, 16 * c, KB)) = w;
     }
     __syncthreads();
   }
@@ -166,6 +223,7 @@ struct KindPlan {
   std::vector<GInst> inst;
   std::vector<GTile> tiles;
   std::vector<GPrepInst> prep;   // 2 per instance: A then B
+  std::vector<uint2> work;       // pre-pass work items: (prep index, 32-row block)
   long bytesA = 0, bytesB = 0, nexp = 0;
 };
 
@@ -194,7 +252,9 @@ void plan_kind(const GroupedDesc& g, const std::vector<int>& members, KindPlan<C
       for (int b = 0; b < tn; ++b) kp.tiles.push_back(GTile{li, a, b});
     GPrepInst pa{g.A, in.idx, in.m, in.k, in.lda, in.transa == SSBLAS_OP_T, tm, gi.nk, gi.offA, gi.offEA};
     GPrepInst pb{(const void* const*)g.B, in.idx, in.n, in.k, in.ldb, in.transb == SSBLAS_OP_N, tn, gi.nk, gi.offB, gi.offEB};
+    for (long rb = 0; rb < (long)tm * Cfg::BM / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pa);
+    for (long rb = 0; rb < (long)tn * Cfg::BN / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pb);
   }
   // longest K first: the persistent CTAs then finish close together
@@ -212,21 +272,24 @@ struct DevBuf {
 };
 
 struct KindDev {
-  DevBuf inst, tiles, prep, packA, packB, exps;
-  long ninst = 0, ntiles = 0;
+  DevBuf inst, tiles, prep, work, packA, packB, exps;
+  long ninst = 0, ntiles = 0, nwork = 0;
 };
 
 template <class Cfg>
 cudaError_t upload_kind(const KindPlan<Cfg>& kp, KindDev& kd, cudaStream_t st) {
   cudaError_t e;
   if ((e = kd.inst.alloc(sizeof(GInst) * kp.inst.size())) || (e = kd.tiles.alloc(sizeof(GTile) * kp.tiles.size())) ||
-      (e = kd.prep.alloc(sizeof(GPrepInst) * kp.prep.size())) || (e = kd.packA.alloc(kp.bytesA)) ||
+      (e = kd.prep.alloc(sizeof(GPrepInst) * kp.prep.size())) || (e = kd.work.alloc(sizeof(uint2) * kp.work.size())) ||
+      (e = kd.packA.alloc(kp.bytesA)) ||
       (e = kd.packB.alloc(kp.bytesB)) || (e = kd.exps.alloc(sizeof(int32_t) * (kp.nexp + 1))))
     return e;
   if ((e = cudaMemcpyAsync(kd.inst.p, kp.inst.data(), sizeof(GInst) * kp.inst.size(), cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemcpyAsync(kd.tiles.p, kp.tiles.data(), sizeof(GTile) * kp.tiles.size(), cudaMemcpyHostToDevice, st)) ||
-      (e = cudaMemcpyAsync(kd.prep.p, kp.prep.data(), sizeof(GPrepInst) * kp.prep.size(), cudaMemcpyHostToDevice, st)))
+      (e = cudaMemcpyAsync(kd.prep.p, kp.prep.data(), sizeof(GPrepInst) * kp.prep.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(kd.work.p, kp.work.data(), sizeof(uint2) * kp.work.size(), cudaMemcpyHostToDevice, st)))
     return e;
+  kd.nwork = (long)kp.work.size();
   kd.ninst = (long)kp.inst.size();
   kd.ntiles = (long)kp.tiles.size();
   return cudaStreamSynchronize(st);   // the host tables are temporaries
@@ -238,8 +301,10 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
   if (kd.ninst == 0) return cudaSuccess;
   {
     ProfScope prof(prep_name, st);
-    gprep_kernel<MODE, S, Cfg::KB, Cfg::BM, Cfg::BN><<<(unsigned)(2 * kd.ninst), GNT, 0, st>>>(
-        (const GPrepInst*)kd.prep.p, (uint8_t*)kd.packA.p, (uint8_t*)kd.packB.p, (int32_t*)kd.exps.p);
+    if (kd.nwork >= (1L << 31)) return cudaErrorInvalidValue;
+    gprep_kernel<MODE, S, Cfg::KB, Cfg::BM, Cfg::BN><<<(unsigned)kd.nwork, GNT, 0, st>>>(
+        (const GPrepInst*)kd.prep.p, (const uint2*)kd.work.p, (uint8_t*)kd.packA.p, (uint8_t*)kd.packB.p,
+        (int32_t*)kd.exps.p);
     note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -73,3 +73,28 @@ def test_grouped_status_conventions():
     gd.reset_c()
     assert gd.call() == 0
     np.testing.assert_array_equal(gd.results()[0], probs[0].C)
+
+
+def test_grouped_long_k_instances():
+    """Instances whose K spans many pre-pass chunks (and an odd number of K blocks), in every
+    layout, next to small ones: Ozaki bit-exact, BF16x3 and int8 within their bounds."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    probs = []
+    for i, (ta, tb) in enumerate([(0, 0), (0, 1), (1, 0), (1, 1)]):
+        probs.append(W.make_problem("f64", ta, tb, 70 + 31 * i, 45 + 17 * i, 1100 - 97 * i, 1, 1.0, 0.0,
+                                    seed=300 + i, dist="expspread"))
+        probs.append(W.make_problem("f32", ta, tb, 90 + 13 * i, 33 + 29 * i, 900 + 61 * i, 1, 0.5, 0.25,
+                                    seed=400 + i))
+        probs.append(W.make_problem("i8", ta, tb, 40 + 9 * i, 70 + 5 * i, 1000 + 33 * i, 1, 1, 1, seed=500 + i))
+    probs += W.grouped_problems(count=12, seed=3, lo=1, hi=64)
+    S.set_math_mode(3)
+    try:
+        gd = runner.GroupedDevice(probs)
+        for rep in range(2):
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            for p, C in zip(probs, gd.results()):
+                _check(p, C, 3)
+    finally:
+        S.set_math_mode(0)

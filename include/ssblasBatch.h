@@ -106,8 +106,9 @@ typedef enum {
   SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch */
   SSBLAS_PATH_DMMA = 6,            /* plain fp64 on the FP64 tensor cores (mma.sync f64) */
   SSBLAS_PATH_OZAKI_SLICER = 7     /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
-                                      pre-pass (0: one pass with thread-block clusters when
-                                      k <= 2048, 1: exponent pass then digit pass) */
+                                      pre-pass. 0 (default) and 3: one pass with thread-block
+                                      clusters of 16 rows x 512 k per CTA when k <= 2048; 2: the
+                                      same with 32 rows x 256 k; 1: exponent pass then digit pass */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

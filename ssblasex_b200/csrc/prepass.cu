@@ -365,37 +365,45 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const i
   write_rows<S, DKT>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
 }
 
-// Single-pass slicing for K <= 2048 with thread-block clusters. An item is 32 rows of one
-// instance; the CS = ceil(K/256) CTAs of a cluster share it, CTA q taking k in [256q, 256q + 256),
-// and the clusters are persistent (one 512-thread CTA per SM, items strided over the clusters).
+// Single-pass slicing with thread-block clusters. An item is R rows of one instance; the
+// CS = ceil(K/KC) CTAs of a cluster share it, CTA q taking k in [KC q, KC q + KC), and the clusters
+// are persistent (one 512-thread CTA per SM, items strided over the clusters). Two item shapes,
+// both 8192 fp64 values (64 KB) per CTA: 32 rows x 256 k (256-byte row segments when the rows are
+// contiguous in memory) and 16 rows x 512 k (half the cluster size, so clusters fit on all SMs).
 // Per item:
-//   the 32 x 256 fp64 tile -- brought into shared memory two items ahead, by TMA when the
+//   the R x KC fp64 tile -- brought into shared memory two items ahead, by TMA when the
 //   instances are equally spaced and 16-byte aligned, else by cp.async -- is read into registers
 //   (16 values per thread); partial row maxima go to this CTA's pmax[item parity]; a cluster
 //   barrier; every CTA reads all CS partial maxima through distributed shared memory and derives
 //   the row exponents; the copies of the item two ahead are issued into the stage just read; the
 //   digits are staged [plane][row][k] in shared memory and leave by one bulk copy per plane row
-//   (256 contiguous bytes).
+//   (KC contiguous bytes).
 // Each operand is read from HBM once, and the next item's tile is in flight while the current
 // one is converted.
 //
-// Thread t (warp w, lane l) owns row r and 4 runs of 4 consecutive k: k = 256q + 4c + 64j + i
-// (j < 4, i < 4), with
-//   rows contiguous in memory (element (r, k) at X[r + k*ld]):  r = l % 16 + 16 (w % 2),
-//     c = l / 16 + 2 (w / 2); the tile is staged [k][32 rows] (256 contiguous bytes per k), so a
-//     half-warp reads 16 consecutive rows: no bank conflicts;
-//   k contiguous (element (r, k) at X[r*ld + k]):               r = t / 16, c = t % 16; the tile
-//     is staged [32 rows][k].
-constexpr int CL_ROWS = 32;
-constexpr int CL_K = 256;
+// Thread t (warp w, lane l) owns row r and 4 runs of 4 consecutive k: k = KC q + 4c + 4 NC j + i
+// (j < 4, i < 4, NC = KC / 16 runs per row), with
+//   rows contiguous in memory (element (r, k) at X[r + k*ld]): r = l % 16 + 16 (w % (R/16)),
+//     c = l / 16 + 2 (w / (R/16)); the tile is staged [k][R rows], so a half-warp reads 16
+//     consecutive rows: no bank conflicts;
+//   k contiguous (element (r, k) at X[r*ld + k]): r = t / NC, c = t % NC; the tile is staged
+//     [k / 256][R rows][256 k] (one TMA box per 256 k).
 constexpr int CL_NTH = 512;
-constexpr int CL_PW = CL_K / 4 + 4;                    // staged digit words per row (16-byte aligned)
-constexpr int CL_TILE = CL_ROWS * CL_K;                // fp64 values per stage
 
-template <int S>
-constexpr int cluster_smem_bytes() {
-  return 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4 + 8 * CL_ROWS * 8 + 2 * CL_ROWS * 8 + CL_ROWS * 16 + 16;
-}
+template <int R, int KC>
+struct ClShape {
+  static constexpr int TILE = R * KC;                // fp64 values per stage (8192)
+  static constexpr int NC = KC / 16;                 // runs of 4 k per row (per thread group)
+  static constexpr int LR = R < 16 ? R : 16;         // rows per half-warp (rows contiguous)
+  static constexpr int RG = R / LR;                  // row groups
+  static constexpr int NW = 16 / RG;                 // warps sharing a row (rows contiguous)
+  static constexpr int PW = KC / 4 + 4;              // staged digit words per row (16-byte aligned)
+  static_assert(TILE == 8192 && TILE / CL_NTH == 16, "tile shape");
+  template <int S>
+  static constexpr int smem_bytes() { return 2 * TILE * 8 + S * R * PW * 4 + 16 * 32 * 8 + 2 * R * 8 + R * 16 + 16; }
+  // position of element (r, k) of a tile staged with K contiguous
+  static __device__ __forceinline__ int kc_index(int r, int k) { return (k / 256) * R * 256 + r * 256 + (k % 256); }
+};
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void cluster_arrive_relaxed() {
@@ -427,6 +435,7 @@ struct ClusterItem {
 };
 
 // item -> (operand, instance, first row); 32-bit division (item counts are below 2^31)
+template <int R>
 __device__ __forceinline__ ClusterItem cluster_item(long item, long n0, uint32_t bpi0, uint32_t bpi1) {
   ClusterItem ci;
   ci.second = item >= n0;
@@ -434,24 +443,26 @@ __device__ __forceinline__ ClusterItem cluster_item(long item, long n0, uint32_t
   const uint32_t bpi = ci.second ? bpi1 : bpi0;
   const uint32_t b = rb / bpi;
   ci.b = b;
-  ci.row0 = (long)(rb - b * bpi) * CL_ROWS;
+  ci.row0 = (long)(rb - b * bpi) * R;
   return ci;
 }
 
-// cp.async: this CTA's 32 x 256 slab of an item into a stage (zero outside the matrix).
+// cp.async: this CTA's R x KC slab of an item into a stage (zero outside the matrix).
+template <int R, int KC>
 __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, const ClusterItem& ci, long kbase) {
+  using Sh = ClShape<R, KC>;
   const double* X = (const double*)a.X[ci.b];
   const int t = threadIdx.x;
   const bool vec = (((uintptr_t)X) % 16 == 0) && (a.ld % 2 == 0);
   if (!a.kcontig) {
-    // [k][32 rows]: chunk = 2 rows at one k
+    // [k][R rows]: chunk = 2 rows at one k
 #pragma unroll 4
-    for (int q = 0; q < CL_TILE / 2 / CL_NTH; ++q) {
-      const int ch = t + q * CL_NTH, kl = ch / 16, rp = 2 * (ch % 16);
+    for (int q = 0; q < Sh::TILE / 2 / CL_NTH; ++q) {
+      const int ch = t + q * CL_NTH, kl = ch / (R / 2), rp = 2 * (ch % (R / 2));
       const long gr = ci.row0 + rp, gk = kbase + kl;
       const long nr = (gk < a.K) ? (a.rows - gr >= 2 ? 2 : (a.rows - gr > 0 ? a.rows - gr : 0)) : 0;
       const double* src = nr > 0 ? X + gr + gk * a.ld : X;
-      double* dst = stage + kl * CL_ROWS + rp;
+      double* dst = stage + kl * R + rp;
       if (vec) {
         cpa16(dst, src, (int)(8 * nr));
       } else {
@@ -460,14 +471,14 @@ __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, c
       }
     }
   } else {
-    // [32 rows][k]: chunk = 2 consecutive k of one row
+    // [k / 256][R rows][256 k]: chunk = 2 consecutive k of one row
 #pragma unroll 4
-    for (int q = 0; q < CL_TILE / 2 / CL_NTH; ++q) {
-      const int ch = t + q * CL_NTH, rl = ch / (CL_K / 2), kp = 2 * (ch % (CL_K / 2));
+    for (int q = 0; q < Sh::TILE / 2 / CL_NTH; ++q) {
+      const int ch = t + q * CL_NTH, rl = ch / (KC / 2), kp = 2 * (ch % (KC / 2));
       const long gr = ci.row0 + rl, gk = kbase + kp;
       const long nk = (gr < a.rows) ? (a.K - gk >= 2 ? 2 : (a.K - gk > 0 ? a.K - gk : 0)) : 0;
       const double* src = nk > 0 ? X + gr * a.ld + gk : X;
-      double* dst = stage + rl * CL_K + kp;
+      double* dst = stage + Sh::kc_index(rl, kp);
       if (vec) {
         cpa16(dst, src, (int)(8 * nk));
       } else {
@@ -495,34 +506,42 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// TMA: the item's 32 x 256 tile of one operand through its 3-D tensor map (zero outside).
+// TMA: the item's R x KC tile of one operand through its 3-D tensor map (box: R rows x 256 k,
+// zero outside), one box per 256 k.
+template <int R, int KC>
 __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const CUtensorMap* tm, bool kcontig,
                                             const ClusterItem& ci, long kbase) {
   const uint32_t b = ptx::smem_u32(bar);
-  ptx::mbar_arrive_expect_tx(b, CL_TILE * 8);
-  if (kcontig) tma_load_3d(ptx::smem_u32(stage), tm, b, (int)kbase, (int)ci.row0, (int)ci.b);
-  else tma_load_3d(ptx::smem_u32(stage), tm, b, (int)ci.row0, (int)kbase, (int)ci.b);
+  ptx::mbar_arrive_expect_tx(b, ClShape<R, KC>::TILE * 8);
+#pragma unroll
+  for (int h = 0; h < KC / 256; ++h) {
+    const uint32_t dst = ptx::smem_u32(stage + h * R * 256);
+    if (kcontig) tma_load_3d(dst, tm, b, (int)(kbase + 256 * h), (int)ci.row0, (int)ci.b);
+    else tma_load_3d(dst, tm, b, (int)ci.row0, (int)(kbase + 256 * h), (int)ci.b);
+  }
 }
 
-template <int S, bool TMA>
+template <int S, bool TMA, int R, int KC>
 __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
                                                                   const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
                                                                   int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
                                                                   long n_items, int CS, int* err) {
+  using Sh = ClShape<R, KC>;
+  constexpr int NC = Sh::NC, LR = Sh::LR, RG = Sh::RG, NW = Sh::NW, PW = Sh::PW, TILE = Sh::TILE;
   extern __shared__ __align__(16) uint8_t dyn[];
-  double* stages = (double*)dyn;                                                   // [2][CL_TILE]
-  uint32_t* st = (uint32_t*)(dyn + 2 * CL_TILE * 8);                               // [S][32][CL_PW]
-  double* red = (double*)(dyn + 2 * CL_TILE * 8 + S * CL_ROWS * CL_PW * 4);        // [8][32]
-  double* pmax = red + 8 * CL_ROWS;                                                // [2][32]
-  double* rscale = pmax + 2 * CL_ROWS;                                             // [32][2]
-  uint64_t* full = (uint64_t*)(rscale + 2 * CL_ROWS);                              // [2] (TMA)
+  double* stages = (double*)dyn;                                                   // [2][TILE]
+  uint32_t* st = (uint32_t*)(dyn + 2 * TILE * 8);                                  // [S][R][PW]
+  double* red = (double*)(dyn + 2 * TILE * 8 + S * R * PW * 4);                    // [16][32]
+  double* pmax = red + 16 * 32;                                                    // [2][R]
+  double* rscale = pmax + 2 * R;                                                   // [R][2]
+  uint64_t* full = (uint64_t*)(rscale + 2 * R);                                    // [2] (TMA)
 
   const int rank = (int)(blockIdx.x % CS);           // rank in the cluster (cluster dims CS x 1 x 1)
   const long cluster = blockIdx.x / CS, nclusters = gridDim.x / CS;
-  const long kbase = (long)rank * CL_K;
+  const long kbase = (long)rank * KC;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
-  const uint32_t bpi0 = (uint32_t)((a0.rows + CL_ROWS - 1) / CL_ROWS);
-  const uint32_t bpi1 = (uint32_t)((a1.rows + CL_ROWS - 1) / CL_ROWS);
+  const uint32_t bpi0 = (uint32_t)((a0.rows + R - 1) / R);
+  const uint32_t bpi1 = (uint32_t)((a1.rows + R - 1) / R);
 
   if (TMA && t == 0) {
     ptx::mbar_init(ptx::smem_u32(&full[0]), 1);
@@ -535,12 +554,12 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
   for (int s = 0; s < 2; ++s) {
     const long item = cluster + s * nclusters;
     if (item < n_items) {
-      const ClusterItem ci = cluster_item(item, n0, bpi0, bpi1);
+      const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
       if (TMA) {
-        if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], ci.second ? &tm1 : &tm0,
-                                ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
+        if (t == 0) cluster_tma<R, KC>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
+                                       ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
       } else {
-        cluster_load(stages + s * CL_TILE, ci.second ? a1 : a0, ci, kbase);
+        cluster_load<R, KC>(stages + s * TILE, ci.second ? a1 : a0, ci, kbase);
       }
     }
     if (!TMA) cpa_commit();
@@ -549,11 +568,11 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
   long iter = 0;
   for (long item = cluster; item < n_items; item += nclusters, ++iter) {
     const int s = (int)(iter & 1);
-    const ClusterItem ci = cluster_item(item, n0, bpi0, bpi1);
+    const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
     const PlaneArgs a = ci.second ? a1 : a0;
     int32_t* __restrict__ exps = ci.second ? e1 : e0;
-    const int r = a.kcontig ? t / 16 : lane % 16 + 16 * (warp % 2);
-    const int c = a.kcontig ? t % 16 : lane / 16 + 2 * (warp / 2);
+    const int r = a.kcontig ? t / NC : lane % LR + LR * (warp % RG);
+    const int c = a.kcontig ? t % NC : lane / LR + (32 / LR) * (warp / RG);
     if (TMA) {
       // a wait that gives up records the error and carries on (every CTA of the cluster must
       // take the same barriers, and every copy is waited for); the host reports the call as failed
@@ -561,49 +580,62 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
     } else {
       cpa_wait1();
     }
-    if (t < S * CL_ROWS) bulk_wait_read0();   // the previous item's digit rows have left st
+    if (t < S * R) bulk_wait_read0();   // the previous item's digit rows have left st
     __syncthreads();
-    const double* tile = stages + s * CL_TILE;
+    const double* tile = stages + s * TILE;
     double v[16];
     if (a.kcontig) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const double2 x0 = *(const double2*)(tile + r * CL_K + 4 * c + 64 * j);
-        const double2 x1 = *(const double2*)(tile + r * CL_K + 4 * c + 64 * j + 2);
+        const int k = 4 * c + 4 * NC * j;
+        const double2 x0 = *(const double2*)(tile + Sh::kc_index(r, k));
+        const double2 x1 = *(const double2*)(tile + Sh::kc_index(r, k) + 2);
         v[4 * j] = x0.x; v[4 * j + 1] = x0.y; v[4 * j + 2] = x1.x; v[4 * j + 3] = x1.y;
       }
     } else {
 #pragma unroll
       for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 64 * j + i) * CL_ROWS + r];
+        for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 4 * NC * j + i) * R + r];
     }
 
     // partial row maxima of this CTA's K range
     double mx = 0.0;
 #pragma unroll
     for (int e = 0; e < 16; ++e) mx = fmax(mx, fabs(v[e]));
-    double* pm = pmax + s * CL_ROWS;
-    if (a.kcontig) {
-      // the 16 threads of row r are lanes 16 (r % 2) .. +15 of warp r / 2
+    double* pm = pmax + s * R;
+    if (a.kcontig && NC <= 32) {
+      // the NC threads of row r are consecutive lanes
 #pragma unroll
-      for (int off = 1; off < 16; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      for (int off = 1; off < NC; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
       if (c == 0) pm[r] = mx;
-    } else {
-      // row r: lanes l and l + 16 of the 8 warps with w % 2 == r / 16
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
-      if (lane < 16) red[(warp / 2) * CL_ROWS + r] = mx;
+    } else if (a.kcontig) {
+      // row r spans the NC / 32 warps r * NC / 32 ..
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane == 0) red[warp] = mx;
       __syncthreads();
-      if (t < CL_ROWS) {
+      if (t < R) {
+        double m2 = red[t * (NC / 32)];
+        for (int w = 1; w < NC / 32; ++w) m2 = fmax(m2, red[t * (NC / 32) + w]);
+        pm[t] = m2;
+      }
+    } else {
+      // row r: lanes with lane % LR == r % LR of the NW warps with w % RG == r / LR
+#pragma unroll
+      for (int off = LR; off < 32; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane < LR) red[(warp / RG) * 32 + r] = mx;
+      __syncthreads();
+      if (t < R) {
         double m2 = red[t];
 #pragma unroll
-        for (int w = 1; w < 8; ++w) m2 = fmax(m2, red[w * CL_ROWS + t]);
+        for (int w = 1; w < NW; ++w) m2 = fmax(m2, red[w * 32 + t]);
         pm[t] = m2;
       }
     }
     cluster_arrive();   // every CTA's pmax[s] is visible after the wait
     cluster_wait();
-    if (t < CL_ROWS) {
+    if (t < R) {
       double m2 = 0.0;
       for (int q = 0; q < CS; ++q) m2 = fmax(m2, ld_cluster_f64(pm + t, (uint32_t)q));
       int e = 0;
@@ -621,12 +653,12 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
     {
       const long nxt = item + 2 * nclusters;
       if (nxt < n_items) {
-        const ClusterItem cn = cluster_item(nxt, n0, bpi0, bpi1);
+        const ClusterItem cn = cluster_item<R>(nxt, n0, bpi0, bpi1);
         if (TMA) {
-          if (t == 0) cluster_tma(stages + s * CL_TILE, &full[s], cn.second ? &tm1 : &tm0,
-                                  cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
+          if (t == 0) cluster_tma<R, KC>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
+                                         cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
         } else {
-          cluster_load(stages + s * CL_TILE, cn.second ? a1 : a0, cn, kbase);
+          cluster_load<R, KC>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
         }
       }
       if (!TMA) cpa_commit();
@@ -640,25 +672,25 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
       const double x[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
       digit_words<S>(x, s0, s1, wd);
 #pragma unroll
-      for (int p = 0; p < S; ++p) st[(p * CL_ROWS + r) * CL_PW + c + 16 * j] = wd[p];
+      for (int p = 0; p < S; ++p) st[(p * R + r) * PW + c + NC * j] = wd[p];
     }
     // the bulk copies read st through the async proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
-    // write-out: one bulk copy per (plane, row) of this CTA's 256 bytes of K (k >= K holds zero
+    // write-out: one bulk copy per (plane, row) of this CTA's KC bytes of K (k >= K holds zero
     // digits, up to Kp)
-    if (t < S * CL_ROWS) {
-      const int p = t / CL_ROWS, rr = t % CL_ROWS;
-      const long bytes = a.Kp - kbase < CL_K ? a.Kp - kbase : CL_K;
+    if (t < S * R) {
+      const int p = t / R, rr = t % R;
+      const long bytes = a.Kp - kbase < KC ? a.Kp - kbase : KC;
       if (ci.row0 + rr < a.rows && bytes > 0) {
         uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kbase;
-        bulk_store(out, st + (p * CL_ROWS + rr) * CL_PW, (uint32_t)bytes);
+        bulk_store(out, st + (p * R + rr) * PW, (uint32_t)bytes);
       }
       bulk_commit();
     }
   }
-  if (t < S * CL_ROWS) bulk_wait0();
+  if (t < S * R) bulk_wait0();
   if (!TMA) cpa_wait0();
   if (TMA && t == 0) {
     // no copy may still be in flight when the CTA exits (bounded, like every wait here)
@@ -672,14 +704,14 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
   cluster_wait();
 }
 
-template <int S, bool TMA>
+template <int S, bool TMA, int R, int KC>
 cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, const PlaneArgs& a0, int32_t* e0,
                               long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st) {
-  constexpr int SMEM = cluster_smem_bytes<S>();
+  constexpr int SMEM = ClShape<R, KC>::template smem_bytes<S>();
+  auto kern = ozaki_cluster_kernel<S, TMA, R, KC>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e =
-        cudaFuncSetAttribute(ozaki_cluster_kernel<S, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -699,7 +731,7 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   if (max_clusters[CS] == 0) {
     cfg.gridDim = dim3((unsigned)(CS * num_sms()), 1, 1);
     int nc = 0;
-    cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, ozaki_cluster_kernel<S, TMA>, &cfg);
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, kern, &cfg);
     if (e != cudaSuccess || nc <= 0) {
       cudaGetLastError();
       nc = num_sms() / CS;
@@ -709,21 +741,20 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   const long n_items = n0 + n1;
   const long nclusters = n_items < max_clusters[CS] ? n_items : max_clusters[CS];
   cfg.gridDim = dim3((unsigned)(nclusters * CS), 1, 1);
-  return cudaLaunchKernelEx(&cfg, ozaki_cluster_kernel<S, TMA>, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS,
-                            device_error_flag());
+  return cudaLaunchKernelEx(&cfg, kern, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS, device_error_flag());
 }
 
-// 3-D map (innermost dimension first) over an equally spaced fp64 operand with a 32 x 256 box.
-bool slicer_map(CUtensorMap* m, const PlaneArgs& a) {
+// 3-D map (innermost dimension first) over an equally spaced fp64 operand with an R x 256 box.
+bool slicer_map(CUtensorMap* m, const PlaneArgs& a, int R) {
   if (!a.X0 || a.xstride <= 0 || ((uintptr_t)a.X0 % 16) != 0 || (a.ld * 8) % 16 != 0 || a.xstride % 16 != 0)
     return false;
   if (a.rows >= (1L << 31) || a.K >= (1L << 31) || a.batch >= (1L << 31)) return false;
   long dims[3], strides[2];
   int box[3];
   if (a.kcontig) {
-    dims[0] = a.K; dims[1] = a.rows; box[0] = CL_K; box[1] = CL_ROWS;
+    dims[0] = a.K; dims[1] = a.rows; box[0] = 256; box[1] = R;
   } else {
-    dims[0] = a.rows; dims[1] = a.K; box[0] = CL_ROWS; box[1] = CL_K;
+    dims[0] = a.rows; dims[1] = a.K; box[0] = R; box[1] = 256;
   }
   dims[2] = a.batch; box[2] = 1;
   strides[0] = a.ld * 8;
@@ -731,35 +762,44 @@ bool slicer_map(CUtensorMap* m, const PlaneArgs& a) {
   return make_tiled_map(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, a.X0, dims, strides, box, 0);
 }
 
-template <int S>
-cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, long n0, const PlaneArgs& a1, int32_t* e1, long n1,
-                             int CS, cudaStream_t st) {
+template <int S, int R, int KC>
+cudaError_t launch_cluster_shape(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
+                                 cudaStream_t st) {
+  const int CS = (int)((a0.Kp + KC - 1) / KC);
+  const long n0 = (a0.rows + R - 1) / R * a0.batch;
+  const long n1 = two ? (a1.rows + R - 1) / R * a1.batch : 0;
+  if ((n0 + n1) * CS >= (1L << 31) || CS < 1 || CS > 8) return cudaErrorInvalidValue;
   CUtensorMap tm0, tm1;
-  const bool tma = slicer_map(&tm0, a0) && (n1 == 0 || slicer_map(&tm1, a1));
-  if (n1 == 0) tm1 = tm0;
-  if (tma) return launch_cluster_st<S, true>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
-  return launch_cluster_st<S, false>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  const bool tma = slicer_map(&tm0, a0, R) && (!two || slicer_map(&tm1, a1, R));
+  if (!two) tm1 = tm0;
+  if (tma) return launch_cluster_st<S, true, R, KC>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  return launch_cluster_st<S, false, R, KC>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
 }
 
-// K up to 2048 (clusters of at most 8 CTAs of 256 k each)
-bool cluster_kernel_fits(const PlaneArgs& a) { return a.K <= 8L * CL_K && a.Kp <= 8L * CL_K; }
+// Item shape: 16 x 512 (configuration 3, the default), 32 x 256 (2) or 8 x 1024 (4).
+template <int S>
+cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two, int shape,
+                             cudaStream_t st) {
+  if (shape == 2) return launch_cluster_shape<S, 32, 256>(a0, e0, a1, e1, two, st);
+  if (shape == 4) return launch_cluster_shape<S, 8, 1024>(a0, e0, a1, e1, two, st);
+  return launch_cluster_shape<S, 16, 512>(a0, e0, a1, e1, two, st);
+}
+
+// K up to 2048 with clusters of at most 8 CTAs of 256 k (at most 4 of 512 k)
+bool cluster_kernel_fits(const PlaneArgs& a) { return a.K <= 2048 && a.Kp <= 2048; }
 
 // One launch for one or two operands (with the same K).
 cudaError_t launch_ozaki_cluster(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
-                                 int slices, cudaStream_t st) {
-  const int CS = (int)((a0.Kp + CL_K - 1) / CL_K);
-  const long n0 = (a0.rows + CL_ROWS - 1) / CL_ROWS * a0.batch;
-  const long n1 = two ? (a1.rows + CL_ROWS - 1) / CL_ROWS * a1.batch : 0;
-  if ((n0 + n1) * CS >= (1L << 31) || CS < 1) return cudaErrorInvalidValue;
+                                 int slices, int shape, cudaStream_t st) {
   ProfScope prof("ozaki_slice", st);
   cudaError_t e;
   switch (slices) {
-    case 3: e = launch_cluster_s<3>(a0, e0, n0, a1, e1, n1, CS, st); break;
-    case 4: e = launch_cluster_s<4>(a0, e0, n0, a1, e1, n1, CS, st); break;
-    case 5: e = launch_cluster_s<5>(a0, e0, n0, a1, e1, n1, CS, st); break;
-    case 6: e = launch_cluster_s<6>(a0, e0, n0, a1, e1, n1, CS, st); break;
-    case 7: e = launch_cluster_s<7>(a0, e0, n0, a1, e1, n1, CS, st); break;
-    case 8: e = launch_cluster_s<8>(a0, e0, n0, a1, e1, n1, CS, st); break;
+    case 3: e = launch_cluster_s<3>(a0, e0, a1, e1, two, shape, st); break;
+    case 4: e = launch_cluster_s<4>(a0, e0, a1, e1, two, shape, st); break;
+    case 5: e = launch_cluster_s<5>(a0, e0, a1, e1, two, shape, st); break;
+    case 6: e = launch_cluster_s<6>(a0, e0, a1, e1, two, shape, st); break;
+    case 7: e = launch_cluster_s<7>(a0, e0, a1, e1, two, shape, st); break;
+    case 8: e = launch_cluster_s<8>(a0, e0, a1, e1, two, shape, st); break;
     default: return cudaErrorInvalidValue;
   }
   note_launch();
@@ -789,8 +829,9 @@ cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
                                     cudaStream_t st) {
   // K up to 2048: one pass over both operands (unless the two-pass form is configured)
-  const bool one_pass = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0) == 0;
-  if (one_pass && cluster_kernel_fits(a) && b.K == a.K) return launch_ozaki_cluster(a, ea, b, eb, true, slices, st);
+  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0);
+  if (form != 1 && cluster_kernel_fits(a) && b.K == a.K)
+    return launch_ozaki_cluster(a, ea, b, eb, true, slices, form, st);
   const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
   const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);
   if (items_a + items_b < 2L * num_sms() || chunks_a + chunks_b >= (1L << 31)) {
@@ -819,8 +860,8 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
 }
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
-  const bool one_pass = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, a.rows, a.K, a.batch, 0) == 0;
-  if (one_pass && cluster_kernel_fits(a)) return launch_ozaki_cluster(a, exps, a, exps, false, slices, st);
+  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, a.rows, a.K, a.batch, 0);
+  if (form != 1 && cluster_kernel_fits(a)) return launch_ozaki_cluster(a, exps, a, exps, false, slices, form, st);
   const long items = (a.rows + RT - 1) / RT * a.batch;
   const long chunks = items * ((a.K + DKT - 1) / DKT);
   if (items >= 2L * num_sms() && chunks < (1L << 31)) {

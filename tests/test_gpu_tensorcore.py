@@ -102,20 +102,28 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
+@pytest.mark.parametrize("form", [2, 3, 4])
 @pytest.mark.parametrize("ta,tb,m,n,k,batch", [
-    (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 CTAs, K contiguous, 16-byte loads
-    (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2, odd ld (8-byte loads)
+    (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 (4) CTAs, K contiguous, 16-byte loads
+    (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2 (1), odd ld (8-byte loads)
     (0, 1, 300, 33, 1030, 2),     # single pass, rows contiguous, ragged last row block
     (0, 1, 64, 48, 2500, 2),      # K > 2048 with few rows: one-kernel slicer
     (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows: exponent pass, then digit chunks
 ])
-def test_ozaki_slicer_paths(S, ta, tb, m, n, k, batch):
-    """Every slicing kernel produces the planes the CPU restatement produces: the product is
-    bit-exact against oracle.ozaki_f64 whichever kernel sliced the operands."""
+def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
+    """Every slicing kernel (and both item shapes of the one-pass kernel: form 2 = 32 rows x 256 k
+    per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k) produces the planes the CPU restatement produces: the product
+    is bit-exact against oracle.ozaki_f64 whichever kernel sliced the operands."""
     from ssblasex_b200 import workloads as W
+    if k > 2048 and form in (2, 4):
+        pytest.skip("the one-pass forms apply to k <= 2048")
     S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_slicer", form)
     p = W.make_problem("f64", ta, tb, m, n, k, batch, 1.5, -0.5, seed=m + k, dist="expspread")
-    C = run(p)
+    try:
+        C = run(p)
+    finally:
+        S.set_kernel_config("ozaki_slicer", -1)
     assert S.last_run_info()["path"] == "ozaki_tcgen05"
     st, C_o = O.ozaki_f64(p, 7)
     assert st == 0

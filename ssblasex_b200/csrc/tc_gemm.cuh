@@ -358,7 +358,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             for (int j = 0; j < 16; ++j) {
               const long gj = n0 + c * 16 + j;
               if (gj < n) {
-                const double w = scalbn(v[c][j], ea + exb[gj] + prm.exp_shift);
+                // v * 2^E: one multiplication by the exact power of two when 2^E is a normal
+                // double (correctly rounded, so equal to scalbn), scalbn otherwise
+                const int E = ea + exb[gj] + prm.exp_shift;
+                const double w = (E >= -1022 && E <= 1023)
+                                     ? v[c][j] * __longlong_as_double((long long)(E + 1023) << 52)
+                                     : scalbn(v[c][j], E);
                 double* cp = Cd + gi + gj * ldc;
                 const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
                 *cp = fma(w, alpha_d, tb);

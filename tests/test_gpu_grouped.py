@@ -98,3 +98,24 @@ def test_grouped_long_k_instances():
                 _check(p, C, 3)
     finally:
         S.set_math_mode(0)
+
+
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_grouped_ozaki_tile_configurations(cfg):
+    """Both Ozaki tile configurations of the grouped path (0: 128 x 64 tiles, one accumulator;
+    1: 128 x 32 tiles, two accumulators) give the bit-exact Ozaki result, fresh and replayed."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner
+    S.set_math_mode(3)
+    S.set_kernel_config("grouped", cfg)
+    try:
+        probs = _mixed(count=40, seed=17)
+        gd = runner.GroupedDevice(probs)
+        for rep in range(3):
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            for p, C in zip(probs, gd.results()):
+                _check(p, C, 3)
+    finally:
+        S.set_kernel_config("grouped", -1)
+        S.set_math_mode(0)

@@ -43,7 +43,7 @@ FAMILIES = {
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=1, transb=0, m=128, n=128, k=128, batch=256, alpha=1.0, beta=0.5),
     ]),
-    "simt": (SSBLAS_MATH_PLAIN, [0, 1], "simt_gemm", [
+    "simt": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4], "(all)", [
         dict(row="f32", transa=0, transb=0, m=128, n=128, k=128, batch=64, alpha=1.0, beta=0.5),
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),
@@ -79,8 +79,11 @@ def time_kernel(p, dp, kernel, reps):
     prof = get_profile()
     set_profiling(False)
     set_sync_mode(True)
-    n, ms = prof.get(kernel, (1, float("nan")))
-    return ms / max(n, 1)
+    if kernel in prof:
+        n, ms = prof[kernel]
+        return ms / max(n, 1)
+    # configurations of one family may run different kernels: time the whole call
+    return sum(ms for _, ms in prof.values()) / reps
 
 
 def main():

@@ -490,7 +490,7 @@ static ssblasStatus_t run_host_pipelined(BatchDesc d, const void* const A[], con
   if (!dense(sa, a_bytes) || !dense(sb, b_bytes) || !dense(sc, c_bytes)) return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
 
   static cudaStream_t s_in = nullptr, s_out = nullptr;
-  constexpr int NCH = 8;   // chunks: copies of chunk c+1 overlap the GEMM of chunk c and the copy-back of c-1
+  constexpr int NCH = 16;  // chunks: copies of chunk c+1 overlap the GEMM of chunk c and the copy-back of c-1
   static cudaEvent_t ev_start = nullptr, ev_in[NCH], ev_cp[NCH];
   cudaError_t e;
   if (!s_in) {

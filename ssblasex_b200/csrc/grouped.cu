@@ -55,7 +55,8 @@ struct GPrepInst {
 constexpr int GRT = 32;   // rows per work item
 constexpr int GNT = 256;
 
-// One CTA per work item = (operand of an instance, block of 32 rows of its padded row range).
+// One CTA per work item = (operand of an instance, block of 32 rows of it). Only rows and K
+// blocks of the matrix are written; the tile padding around them was zeroed when the plan was made.
 // MODE 0: int8 copy (1 plane); 1: BF16 hi/lo (2 planes); 2: Ozaki slices (S planes).
 //
 // The item's rows are converted in K chunks of KC elements. Each thread handles runs of 4
@@ -68,7 +69,7 @@ constexpr int GNT = 256;
 // grouped GEMM stages with bulk copies: for each (row tile, K block) of the instance, P planes of
 // [RTILE rows][KB bytes], 16-byte chunks permuted by the hardware swizzle of a KB-byte span.
 template <int MODE, int S, int KB, int RTILE_A, int RTILE_B>
-__global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
+__global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
                                                     uint8_t* __restrict__ outA, uint8_t* __restrict__ outB,
                                                     int32_t* __restrict__ exps) {
   constexpr int P = MODE == 0 ? 1 : MODE == 1 ? 2 : S;
@@ -207,7 +208,8 @@ __global__ void __launch_bounds__(GNT) gprep_kernel(const GPrepInst* __restrict_
       const int c = ch % CPR, r = (ch / CPR) % GRT, bp = ch / (CPR * GRT);
       const int kb = bp / P, pl = bp % P;
       const long kbg = k0 / KE + kb;
-      if (kbg >= it.nk) continue;
+      // K blocks past K and rows past the matrix are padding, zero since the plan was created
+      if (kbg >= it.nk || kbg * KE >= it.K || gr0 + r >= it.rows) continue;
       const uint32_t* src = (const uint32_t*)(stage + bp * GRT * PB + r * PB + 16 * c);
       const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
       uint8_t* chunk = out + ((long)rt * it.nk + kbg) * (long)P * RTILE * KB + (long)pl * RTILE * KB;
@@ -252,9 +254,11 @@ void plan_kind(const GroupedDesc& g, const std::vector<int>& members, KindPlan<C
       for (int b = 0; b < tn; ++b) kp.tiles.push_back(GTile{li, a, b});
     GPrepInst pa{g.A, in.idx, in.m, in.k, in.lda, in.transa == SSBLAS_OP_T, tm, gi.nk, gi.offA, gi.offEA};
     GPrepInst pb{(const void* const*)g.B, in.idx, in.n, in.k, in.ldb, in.transb == SSBLAS_OP_N, tn, gi.nk, gi.offB, gi.offEB};
-    for (long rb = 0; rb < (long)tm * Cfg::BM / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
+    // only row blocks that hold rows of the matrix: the padding of the tiles is zeroed once, when
+    // the plan's buffers are created, and no call writes it again
+    for (long rb = 0; rb < (in.m + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pa);
-    for (long rb = 0; rb < (long)tn * Cfg::BN / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
+    for (long rb = 0; rb < (in.n + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pb);
   }
   // longest K first: the persistent CTAs then finish close together
@@ -288,6 +292,8 @@ cudaError_t upload_kind(const KindPlan<Cfg>& kp, KindDev& kd, cudaStream_t st) {
       (e = cudaMemcpyAsync(kd.tiles.p, kp.tiles.data(), sizeof(GTile) * kp.tiles.size(), cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemcpyAsync(kd.prep.p, kp.prep.data(), sizeof(GPrepInst) * kp.prep.size(), cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemcpyAsync(kd.work.p, kp.work.data(), sizeof(uint2) * kp.work.size(), cudaMemcpyHostToDevice, st)))
+    return e;
+  if ((e = cudaMemsetAsync(kd.packA.p, 0, kp.bytesA, st)) || (e = cudaMemsetAsync(kd.packB.p, 0, kp.bytesB, st)))
     return e;
   kd.nwork = (long)kp.work.size();
   kd.ninst = (long)kp.inst.size();

@@ -170,6 +170,10 @@ WORKLOADS = {
     "fp32_batch4096_64": dict(row="f32", transa=OP_T, transb=OP_T, m=64, n=64, k=64, batch=4096,
                               alpha=0.75, beta=0.25, lda=64, ldb=64, ldc=64, seed=3,
                               dist="outliers"),
+    # not a configuration of the task: a compute-bound shape for the int8 tensor-core kernel
+    # (the 512^3 beta=1 batch is bound by HBM bandwidth)
+    "i8_batch8_4096": dict(row="i8", transa=OP_T, transb=OP_N, m=4096, n=4096, k=4096, batch=8,
+                           alpha=1, beta=0, lda=4096, ldb=4096, ldc=4096, seed=4),
 }
 
 

@@ -80,7 +80,9 @@ ssblasStatus_t ssblasGetStream(void** stream);
  * matrices are all in device memory return after enqueueing their work on the stream. */
 ssblasStatus_t ssblasSetSyncMode(int synchronous);
 
-/* Bitwise OR of ssblasMathMode_t flags for the fp64 and fp32 rows. */
+/* Bitwise OR of ssblasMathMode_t flags for the fp64 and fp32 rows.
+ * In SSBLAS_MATH_FP64_OZAKI mode, a row of op(A) or a column of op(B) that holds an Inf or a NaN
+ * makes every C(i, j) it touches a quiet NaN (the plain paths follow IEEE arithmetic). */
 ssblasStatus_t ssblasSetMathMode(int mode);
 ssblasStatus_t ssblasGetMathMode(int* mode);
 

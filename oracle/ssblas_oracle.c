@@ -206,19 +206,26 @@ static void oz_digits(long long X, int S, int8_t* d) {
   d[0] = (int8_t)X;
 }
 
+/* Rows (columns of op(B)) holding an Inf or a NaN get exponent OZ_NONFINITE and zero digits, and
+ * every C(i, j) they touch is the quiet NaN 0x7ff8000000000000 (the library's policy). */
+#define OZ_NONFINITE 4096
+
 static void oz_slice(int trans, long rows, long k, const double* X, long ld, int rows_are_cols, int S,
                      int8_t* dig /* [S][rows][k] */, int* ex) {
   for (long r = 0; r < rows; ++r) {
     double mx = 0.0;
+    int finite = 1;
     for (long kk = 0; kk < k; ++kk) {
       double v = rows_are_cols ? X[at(trans, kk, r, ld)] : X[at(trans, r, kk, ld)];
-      mx = fmax(mx, fabs(v));
+      if (!isfinite(v)) finite = 0;
+      else mx = fmax(mx, fabs(v));
     }
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
-    ex[r] = e;
+    ex[r] = finite ? e : OZ_NONFINITE;
     for (long kk = 0; kk < k; ++kk) {
       double v = rows_are_cols ? X[at(trans, kk, r, ld)] : X[at(trans, r, kk, ld)];
+      if (!finite) v = 0.0;
       long long Xi = llrint(scalbn(v, 8 * S - 2 - e));
       int8_t d[8];
       oz_digits(Xi, S, d);
@@ -253,6 +260,11 @@ int oracle_ozaki_f64(int transa, int transb, long m, long n, long k, double alph
       for (int l = S - 1; l >= 0; --l) {
         if (acc[l] > 2147483647LL || acc[l] < -2147483648LL) status = -1;
         v = v * 0x1p-8 + (double)acc[l];
+      }
+      if (ea[i] == OZ_NONFINITE || eb[j] == OZ_NONFINITE) {
+        const uint64_t qnan = 0x7ff8000000000000ull;
+        memcpy(&C[i + j * ldc], &qnan, 8);
+        continue;
       }
       double w = scalbn(v, ea[i] + eb[j] - 12);
       double t = (beta == 0.0) ? 0.0 : beta * C[i + j * ldc];

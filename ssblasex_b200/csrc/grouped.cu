@@ -116,17 +116,17 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
   };
 
   if (MODE == 2) {
-    // row maxima over all of K
-    double mx[PER];
+    // row maxima over all of K (bit patterns of |x|, stored in the double buffers bit for bit)
+    unsigned long long mx[PER];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) mx[q] = 0.0;
+    for (int q = 0; q < PER; ++q) mx[q] = 0;
     for (long k0 = 0; k0 < it.K; k0 += KC) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
         int r, kl;
         run_of(q, r, kl);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) mx[q] = fmax(mx[q], fabs(load(gr0 + r, k0 + kl + i)));
+        for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(load(gr0 + r, k0 + kl + i)));
       }
     }
     if (it.kcontig) {
@@ -134,29 +134,25 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
 #pragma unroll
-        for (int off = 1; off < RPR && off < 32; off <<= 1) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
+        for (int off = 1; off < RPR && off < 32; off <<= 1) mx[q] = max_u64(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
         int r, kl;
         run_of(q, r, kl);
-        if (kl == 0) red[0][r] = mx[q];
+        if (kl == 0) red[0][r] = __longlong_as_double((long long)mx[q]);
       }
     } else {
-      double m = mx[0];
+      unsigned long long m = mx[0];
 #pragma unroll
-      for (int q = 1; q < PER; ++q) m = fmax(m, mx[q]);
-      red[warp][lane] = m;
+      for (int q = 1; q < PER; ++q) m = max_u64(m, mx[q]);
+      red[warp][lane] = __longlong_as_double((long long)m);
     }
     __syncthreads();
     if (t < GRT) {
-      double m2 = red[0][t];
+      unsigned long long m2 = (unsigned long long)__double_as_longlong(red[0][t]);
       if (!it.kcontig)
-        for (int w = 1; w < 8; ++w) m2 = fmax(m2, red[w][t]);
-      int e = 0;
-      if (m2 > 0.0) frexp(m2, &e);
+        for (int w = 1; w < 8; ++w) m2 = max_u64(m2, (unsigned long long)__double_as_longlong(red[w][t]));
+      const int e = row_exponent(m2);
       if (gr0 + t < it.rows) exps[it.eoff + gr0 + t] = e;
-      const int sh = 8 * S - 2 - e;
-      const int h1 = sh / 2;
-      rscale[t][0] = ldexp(1.0, h1);
-      rscale[t][1] = ldexp(1.0, sh - h1);
+      row_scale(S, e, rscale[t][0], rscale[t][1]);
     }
     __syncthreads();
   }
@@ -193,7 +189,9 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
         *(__nv_bfloat162*)(row + GRT * PB) = l01;
         *(__nv_bfloat162*)(row + GRT * PB + 4) = l23;
       } else {
-        // rows beyond the matrix are zero digits (a zero value gives Y = bias)
+        // rows beyond the matrix are zero digits (a zero value gives Y = bias), and so are rows
+        // holding an Inf or a NaN (zero scale)
+        if (rscale[r][0] == 0.0) x[0] = x[1] = x[2] = x[3] = 0.0;
         uint32_t wd[S];
         digit_words<S>(x, rscale[r][0], rscale[r][1], wd);
 #pragma unroll

@@ -9,6 +9,38 @@
 
 namespace ssb {
 
+// Rows (of op(A)) and columns (of op(B)) holding an Inf or a NaN get this exponent and zero
+// digits; every C(i, j) they touch becomes a quiet NaN (kOzakiNaN). The row maximum is taken over
+// the bit patterns of |x| as unsigned integers, which orders finite values like their magnitudes
+// and puts every Inf and NaN above them.
+constexpr int kNonFiniteExp = 4096;
+constexpr unsigned long long kOzakiNaN = 0x7FF8000000000000ull;
+static __device__ __forceinline__ unsigned long long abs_bits(double x) {
+  return (unsigned long long)__double_as_longlong(x) & 0x7FFFFFFFFFFFFFFFull;
+}
+static __device__ __forceinline__ unsigned long long max_u64(unsigned long long a, unsigned long long b) {
+  return a > b ? a : b;
+}
+// e with max|x| < 2^e (0 for an all-zero row), or kNonFiniteExp
+static __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
+  if (maxbits >= 0x7FF0000000000000ull) return kNonFiniteExp;
+  int e = 0;
+  const double m = __longlong_as_double((long long)maxbits);
+  if (m > 0.0) frexp(m, &e);
+  return e;
+}
+// the two power-of-two factors of 2^(8S-2-e) (0 for a non-finite row: its digits are zero)
+static __device__ __forceinline__ void row_scale(int S, int e, double& s0, double& s1) {
+  if (e == kNonFiniteExp) {
+    s0 = s1 = 0.0;
+    return;
+  }
+  const int sh = 8 * S - 2 - e;
+  const int h1 = sh / 2;
+  s0 = ldexp(1.0, h1);
+  s1 = ldexp(1.0, sh - h1);
+}
+
 // 4 x 4 byte transpose: out[b] holds byte b of w[0..3] (byte j of out[b] = byte b of w[j]).
 static __device__ __forceinline__ void byte_transpose4(const uint32_t (&w)[4], uint32_t (&out)[4]) {
   const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[0], w[1], 0x7362);

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
     uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
     // pass 1: row maxima of |x| straight from global memory (8 loads in flight per thread)
     {
-      double mx = 0.0;
+      unsigned long long mx = 0;
       if (a.kcontig) {
         const int r = threadIdx.x / 8, part = threadIdx.x % 8;
         const long gr = row0 + r;
@@ -175,13 +175,13 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
 #pragma unroll
             for (int j = 0; j < 8; ++j) t[j] = __ldg(row + k + 8 * j);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) mx = fmax(mx, fabs(t[j]));
+            for (int j = 0; j < 8; ++j) mx = max_u64(mx, abs_bits(t[j]));
           }
-          for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(row + k)));
+          for (; k < a.K; k += 8) mx = max_u64(mx, abs_bits(__ldg(row + k)));
         }
 #pragma unroll
-        for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-        if (part == 0) red[0][r] = mx;
+        for (int off = 4; off >= 1; off >>= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (part == 0) red[0][r] = __longlong_as_double((long long)mx);
       } else {
         const int r = threadIdx.x % 32, part = threadIdx.x / 32;
         const long gr = row0 + r;
@@ -193,27 +193,23 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
 #pragma unroll
             for (int j = 0; j < 8; ++j) t[j] = __ldg(col + (k + 8 * j) * a.ld);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) mx = fmax(mx, fabs(t[j]));
+            for (int j = 0; j < 8; ++j) mx = max_u64(mx, abs_bits(t[j]));
           }
-          for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(col + k * a.ld)));
+          for (; k < a.K; k += 8) mx = max_u64(mx, abs_bits(__ldg(col + k * a.ld)));
         }
-        red[part][r] = mx;
+        red[part][r] = __longlong_as_double((long long)mx);
       }
     }
     __syncthreads();
     if (threadIdx.x < RT) {
-      double mx = red[0][threadIdx.x];
+      unsigned long long mx = (unsigned long long)__double_as_longlong(red[0][threadIdx.x]);
       if (!a.kcontig)
-        for (int q = 1; q < 8; ++q) mx = fmax(mx, red[q][threadIdx.x]);
-      int e = 0;
-      if (mx > 0.0) frexp(mx, &e);
+        for (int q = 1; q < 8; ++q) mx = max_u64(mx, (unsigned long long)__double_as_longlong(red[q][threadIdx.x]));
+      const int e = row_exponent(mx);
       const long gr = row0 + threadIdx.x;
       if (gr < a.rows) exps[b * a.rows + gr] = e;
       // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
-      const int sh = 8 * S - 2 - e;
-      const int h1 = sh / 2;
-      rscale[threadIdx.x][0] = ldexp(1.0, h1);
-      rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
+      row_scale(S, e, rscale[threadIdx.x][0], rscale[threadIdx.x][1]);
     }
     __syncthreads();
     // pass 2: digits, transposed through smem, written as 16-byte vectors along K
@@ -224,7 +220,8 @@ __global__ void __launch_bounds__(NTH, 4) ozaki_slice_kernel(PlaneArgs a, int32_
       for (int e = 0; e < PER; ++e) {
         int r, kk;
         tile_coord(a.kcontig, e, r, kk);
-        const unsigned long long Y = slice_y(v[e], rscale[r][0], rscale[r][1], bias);
+        // a non-finite row (zero scale) has zero digits
+        const unsigned long long Y = slice_y(rscale[r][0] == 0.0 ? 0.0 : v[e], rscale[r][0], rscale[r][1], bias);
         const uint32_t lo = (uint32_t)Y, hi = (uint32_t)(Y >> 32);
 #pragma unroll
         for (int p = 0; p < S; ++p) {
@@ -256,7 +253,7 @@ __global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a0, int32_t
   const long b = blk / blocks_per_inst;
   const long row0 = (blk % blocks_per_inst) * RT;
   const double* X = (const double*)a.X[b];
-  double mx = 0.0;
+  unsigned long long mx = 0;
   if (a.kcontig) {
     const int r = threadIdx.x / 8, part = threadIdx.x % 8;
     const long gr = row0 + r;
@@ -268,13 +265,13 @@ __global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a0, int32_t
 #pragma unroll
         for (int j = 0; j < 16; ++j) t[j] = __ldg(row + k + 8 * j);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(t[j]));
+        for (int j = 0; j < 16; ++j) mx = max_u64(mx, abs_bits(t[j]));
       }
-      for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(row + k)));
+      for (; k < a.K; k += 8) mx = max_u64(mx, abs_bits(__ldg(row + k)));
     }
 #pragma unroll
-    for (int off = 4; off >= 1; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-    if (part == 0) red[0][r] = mx;
+    for (int off = 4; off >= 1; off >>= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (part == 0) red[0][r] = __longlong_as_double((long long)mx);
   } else {
     const int r = threadIdx.x % 32, part = threadIdx.x / 32;
     const long gr = row0 + r;
@@ -286,21 +283,19 @@ __global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a0, int32_t
 #pragma unroll
         for (int j = 0; j < 16; ++j) t[j] = __ldg(col + (k + 8 * j) * a.ld);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(t[j]));
+        for (int j = 0; j < 16; ++j) mx = max_u64(mx, abs_bits(t[j]));
       }
-      for (; k < a.K; k += 8) mx = fmax(mx, fabs(__ldg(col + k * a.ld)));
+      for (; k < a.K; k += 8) mx = max_u64(mx, abs_bits(__ldg(col + k * a.ld)));
     }
-    red[part][r] = mx;
+    red[part][r] = __longlong_as_double((long long)mx);
   }
   __syncthreads();
   if (threadIdx.x < RT) {
-    double m2 = red[0][threadIdx.x];
+    unsigned long long m2 = (unsigned long long)__double_as_longlong(red[0][threadIdx.x]);
     if (!a.kcontig)
-      for (int q = 1; q < 8; ++q) m2 = fmax(m2, red[q][threadIdx.x]);
-    int e = 0;
-    if (m2 > 0.0) frexp(m2, &e);
+      for (int q = 1; q < 8; ++q) m2 = max_u64(m2, (unsigned long long)__double_as_longlong(red[q][threadIdx.x]));
     const long gr = row0 + threadIdx.x;
-    if (gr < a.rows) exps[b * a.rows + gr] = e;
+    if (gr < a.rows) exps[b * a.rows + gr] = row_exponent(m2);
   }
 }
 
@@ -345,13 +340,14 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const i
   if (threadIdx.x < RT) {
     const long gr = row0 + threadIdx.x;
     const int e = gr < a.rows ? exps[b * a.rows + gr] : 0;
-    const int sh = 8 * S - 2 - e;
-    const int h1 = sh / 2;
-    rscale[threadIdx.x][0] = ldexp(1.0, h1);
-    rscale[threadIdx.x][1] = ldexp(1.0, sh - h1);
+    row_scale(S, e, rscale[threadIdx.x][0], rscale[threadIdx.x][1]);
   }
   __syncthreads();
   const double s0 = rscale[r][0], s1 = rscale[r][1];
+  if (s0 == 0.0) {   // a non-finite row has zero digits
+#pragma unroll
+    for (int e = 0; e < PER; ++e) v[e] = 0.0;
+  }
 #pragma unroll
   for (int g = 0; g < PER / 4; ++g) {
     uint32_t wd[S];
@@ -599,53 +595,52 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
         for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 4 * NC * j + i) * R + r];
     }
 
-    // partial row maxima of this CTA's K range
-    double mx = 0.0;
+    // partial row maxima of this CTA's K range (bit patterns of |x|; the shared-memory buffers
+    // hold them as doubles, bit for bit)
+    unsigned long long mx = 0;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) mx = fmax(mx, fabs(v[e]));
+    for (int e = 0; e < 16; ++e) mx = max_u64(mx, abs_bits(v[e]));
     double* pm = pmax + s * R;
+    auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
+    auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
     if (a.kcontig && NC <= 32) {
       // the NC threads of row r are consecutive lanes
 #pragma unroll
-      for (int off = 1; off < NC; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (c == 0) pm[r] = mx;
+      for (int off = 1; off < NC; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (c == 0) pm[r] = as_d(mx);
     } else if (a.kcontig) {
       // row r spans the NC / 32 warps r * NC / 32 ..
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (lane == 0) red[warp] = mx;
+      for (int off = 1; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane == 0) red[warp] = as_d(mx);
       __syncthreads();
       if (t < R) {
-        double m2 = red[t * (NC / 32)];
-        for (int w = 1; w < NC / 32; ++w) m2 = fmax(m2, red[t * (NC / 32) + w]);
-        pm[t] = m2;
+        unsigned long long m2 = as_u(red[t * (NC / 32)]);
+        for (int w = 1; w < NC / 32; ++w) m2 = max_u64(m2, as_u(red[t * (NC / 32) + w]));
+        pm[t] = as_d(m2);
       }
     } else {
       // row r: lanes with lane % LR == r % LR of the NW warps with w % RG == r / LR
 #pragma unroll
-      for (int off = LR; off < 32; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (lane < LR) red[(warp / RG) * 32 + r] = mx;
+      for (int off = LR; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane < LR) red[(warp / RG) * 32 + r] = as_d(mx);
       __syncthreads();
       if (t < R) {
-        double m2 = red[t];
+        unsigned long long m2 = as_u(red[t]);
 #pragma unroll
-        for (int w = 1; w < NW; ++w) m2 = fmax(m2, red[w * 32 + t]);
-        pm[t] = m2;
+        for (int w = 1; w < NW; ++w) m2 = max_u64(m2, as_u(red[w * 32 + t]));
+        pm[t] = as_d(m2);
       }
     }
     cluster_arrive();   // every CTA's pmax[s] is visible after the wait
     cluster_wait();
     if (t < R) {
-      double m2 = 0.0;
-      for (int q = 0; q < CS; ++q) m2 = fmax(m2, ld_cluster_f64(pm + t, (uint32_t)q));
-      int e = 0;
-      if (m2 > 0.0) frexp(m2, &e);
+      unsigned long long m2 = 0;
+      for (int q = 0; q < CS; ++q) m2 = max_u64(m2, as_u(ld_cluster_f64(pm + t, (uint32_t)q)));
+      const int e = row_exponent(m2);
       if (rank == 0 && ci.row0 + t < a.rows) exps[ci.b * a.rows + ci.row0 + t] = e;
       // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
-      const int sh = 8 * S - 2 - e;
-      const int h1 = sh / 2;
-      rscale[2 * t] = ldexp(1.0, h1);
-      rscale[2 * t + 1] = ldexp(1.0, sh - h1);
+      row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
     }
     __syncthreads();   // rscale visible; stage s fully read into registers
 
@@ -666,6 +661,10 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
 
     // digits: one 32-bit word per plane per run of 4 k, staged [p][r][k/4]
     const double s0 = rscale[2 * r], s1 = rscale[2 * r + 1];
+    if (s0 == 0.0) {   // a non-finite row has zero digits
+#pragma unroll
+      for (int e = 0; e < 16; ++e) v[e] = 0.0;
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       uint32_t wd[S];

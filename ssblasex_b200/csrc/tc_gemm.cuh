@@ -30,6 +30,9 @@ namespace ssb {
 namespace tc {
 
 constexpr int kThreads = 320;
+// exponent the slicing pre-passes give a row of op(A) / column of op(B) that holds an Inf or a NaN
+// (kNonFiniteExp of ozaki_digits.cuh)
+constexpr int kOzakiNonFiniteExp = 4096;
 
 enum Kind { KIND_I8 = 0, KIND_BF16 = 1 };
 enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2 };
@@ -360,13 +363,20 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               if (gj < n) {
                 // v * 2^E: one multiplication by the exact power of two when 2^E is a normal
                 // double (correctly rounded, so equal to scalbn), scalbn otherwise
-                const int E = ea + exb[gj] + prm.exp_shift;
-                const double w = (E >= -1022 && E <= 1023)
-                                     ? v[c][j] * __longlong_as_double((long long)(E + 1023) << 52)
-                                     : scalbn(v[c][j], E);
+                const int eb = exb[gj];
+                const int E = ea + eb + prm.exp_shift;
                 double* cp = Cd + gi + gj * ldc;
-                const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
-                *cp = fma(w, alpha_d, tb);
+                if (E >= -1022 && E <= 1023) {
+                  const double w = v[c][j] * __longlong_as_double((long long)(E + 1023) << 52);
+                  const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+                  *cp = fma(w, alpha_d, tb);
+                } else if (ea == kOzakiNonFiniteExp || eb == kOzakiNonFiniteExp) {
+                  // row i of op(A) or column j of op(B) holds an Inf or a NaN
+                  *cp = __longlong_as_double((long long)0x7FF8000000000000ull);
+                } else {
+                  const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+                  *cp = fma(scalbn(v[c][j], E), alpha_d, tb);
+                }
               }
             }
         }

@@ -119,3 +119,31 @@ def test_grouped_ozaki_tile_configurations(cfg):
     finally:
         S.set_kernel_config("grouped", -1)
         S.set_math_mode(0)
+
+
+def test_grouped_ozaki_nonfinite_inputs():
+    """The grouped Ozaki path follows the batched path's rule for Inf and NaN entries (zero
+    digits for the row / column, quiet NaN in every C(i, j) it touches), bit-exact against the
+    CPU restatement."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    probs = [W.make_problem("f64", ta, tb, 40 + 17 * i, 33 + 9 * i, 90 + 61 * i, 1, 1.0, 0.0, seed=700 + i,
+                            dist="expspread") for i, (ta, tb) in enumerate([(0, 0), (1, 1), (0, 1), (1, 0)])]
+    probs[0].op_a(0)[5, 2] = np.inf
+    probs[1].op_b(0)[7, 4] = np.nan
+    probs[2].op_a(0)[0, 0] = -np.inf
+    probs[2].op_b(0)[3, 30] = np.inf
+    S.set_math_mode(1)
+    try:
+        gd = runner.GroupedDevice(probs)
+        for rep in range(2):
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            for p, C in zip(probs, gd.results()):
+                _check(p, C, 1)
+        res = gd.results()
+        assert np.isnan(res[0][0][5 + 0 * probs[0].ldc]) and np.isnan(probs[0].c_view(res[0], 0)[5, :]).all()
+        assert np.isnan(probs[1].c_view(res[1], 0)[:, 4]).all()
+        assert not np.isnan(probs[3].c_view(res[3], 0)).any()
+    finally:
+        S.set_math_mode(0)

@@ -276,3 +276,34 @@ def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
     C = np.stack([flat[pad + b * per: pad + b * per + p.C[0].size] for b in range(batch)]).reshape(p.C.shape)
     assert O.normalized_error(p, C) <= 4 * k * 2.0 ** -24
     np.testing.assert_array_equal(C.reshape(batch, n, ldc)[:, :, m:], p.C.reshape(batch, n, ldc)[:, :, m:])
+
+
+# ------------------------------------------------------------------------- Ozaki: Inf / NaN ---
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("k", [300, 1030, 2500])
+def test_ozaki_nonfinite_inputs(S, ta, tb, k):
+    """Ozaki mode with Inf and NaN entries: rows of op(A) and columns of op(B) that hold one
+    get zero digits, and exactly the C(i, j) they touch become the quiet NaN; every other entry
+    is bit-exact against the CPU restatement (which follows the same rule), for the one-pass
+    (k <= 2048) and two-pass slicing forms."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    m, n, batch = 150, 70, 2
+    p = W.make_problem("f64", ta, tb, m, n, k, batch, 1.0, 0.5, seed=ta + 2 * tb + k, dist="expspread")
+    bad_rows, bad_cols = {0: [3, 97], 1: [0]}, {0: [5], 1: [40, 69]}
+    for b in range(batch):
+        opa, opb = p.op_a(b), p.op_b(b)
+        for i, val in zip(bad_rows[b], [np.inf, np.nan]):
+            opa[i, (7 * i) % k] = val
+        for j, val in zip(bad_cols[b], [-np.inf, np.nan]):
+            opb[(11 * j) % k, j] = val
+    C = run(p)
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+    for b in range(batch):
+        got = p.c_view(C, b)
+        want_nan = np.zeros((m, n), bool)
+        want_nan[bad_rows[b], :] = True
+        want_nan[:, bad_cols[b]] = True
+        np.testing.assert_array_equal(np.isnan(got), want_nan)

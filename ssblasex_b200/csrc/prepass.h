@@ -25,6 +25,8 @@ struct PlaneArgs {
 
 cudaError_t launch_pack_i8(const PlaneArgs& a, cudaStream_t st);
 cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st);
+// both operands of one call in one launch
+cudaError_t launch_split_bf16_pair(const PlaneArgs& a, const PlaneArgs& b, cudaStream_t st);
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st);
 // both operands of one call: two launches in all (exponents of both, then digits of both)
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* exps_a, const PlaneArgs& b, int32_t* exps_b,

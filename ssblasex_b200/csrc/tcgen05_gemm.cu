@@ -254,8 +254,7 @@ cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   if (!pb) return e;
   PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * 2};
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * 2};
-  if ((e = launch_split_bf16(a, st)) != cudaSuccess) return e;
-  if ((e = launch_split_bf16(b, st)) != cudaSuccess) return e;
+  if ((e = launch_split_bf16_pair(a, b, st)) != cudaSuccess) return e;
   const int BN = choose_config(SSBLAS_PATH_BF16X3_TCGEN05, d.m, d.n, d.k, d.batch, d.n <= 64 ? 0 : 1) == 0 ? 64 : 128;
   CUtensorMap ta, tb;
   if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.m, 2, d.batch, Kp * 2, sa, sa * 2, 64, 128, 2, 128) ||

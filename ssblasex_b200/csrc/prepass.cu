@@ -3,7 +3,8 @@
 // K-major "planes" [instance][plane][rows][Kp] that the GEMM kernel stages with TMA.
 //
 //   pack_i8      one plane: the int8 values themselves (int8 row, layouts other than TN)
-//   split_bf16   two planes: hi = bf16(x), lo = bf16(x - hi) of an fp32 value
+//   split_bf16   two planes: hi = bf16(x), lo = bf16(x - hi) of an fp32 value (both operands of a
+//                call in one launch)
 //   ozaki_slice  S planes of balanced int8 digits of an fp64 value under a per-row power-of-two
 //                exponent, plus that exponent (Ozaki scheme):
 //                  e   = exponent with max_k |x[r,k]| < 2^e  (0 for an all-zero row)
@@ -158,30 +159,6 @@ __global__ void __launch_bounds__(NTH) split_bf16_pair_kernel(PlaneArgs a0, long
     }
     __syncthreads();
     write_out<2, 2>(st, out, a.plane_stride, a.rows, a.Kp * 2, item_row0[q], item_k0[q] * 2);
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(NTH) split_bf16_kernel(PlaneArgs a) {
-  __shared__ __align__(16) uint8_t st[2 * RT * (2 * KT + 4)];
-  const long b = blockIdx.y;
-  const long row0 = (long)blockIdx.x * RT;
-  const float* X = (const float*)a.X[b];
-  uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
-  for (long k0 = 0; k0 < a.K; k0 += KT) {
-    float v[PER];
-    load_regs<float>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
-#pragma unroll
-    for (int e = 0; e < PER; ++e) {
-      int r, kk;
-      tile_coord(a.kcontig, e, r, kk);
-      const __nv_bfloat16 h = __float2bfloat16_rn(v[e]);
-      const __nv_bfloat16 l = __float2bfloat16_rn(v[e] - __bfloat162float(h));
-      *(__nv_bfloat16*)(st + (0 * RT + r) * (2 * KT + 4) + 2 * kk) = h;
-      *(__nv_bfloat16*)(st + (1 * RT + r) * (2 * KT + 4) + 2 * kk) = l;
-    }
-    __syncthreads();
-    write_out<2, 2>(st, out, a.plane_stride, a.rows, a.Kp * 2, row0, k0 * 2);
     __syncthreads();
   }
 }
@@ -875,12 +852,6 @@ cudaError_t launch_split_bf16_pair(const PlaneArgs& a, const PlaneArgs& b, cudaS
   return cudaGetLastError();
 }
 
-cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st) {
-  ProfScope prof("split_bf16", st);
-  split_bf16_kernel<<<grid_of(a), NTH, 0, st>>>(a);
-  note_launch();
-  return cudaGetLastError();
-}
 
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
                                     cudaStream_t st) {

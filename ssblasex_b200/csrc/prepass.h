@@ -24,7 +24,6 @@ struct PlaneArgs {
 };
 
 cudaError_t launch_pack_i8(const PlaneArgs& a, cudaStream_t st);
-cudaError_t launch_split_bf16(const PlaneArgs& a, cudaStream_t st);
 // both operands of one call in one launch
 cudaError_t launch_split_bf16_pair(const PlaneArgs& a, const PlaneArgs& b, cudaStream_t st);
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st);

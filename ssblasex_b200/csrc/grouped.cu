@@ -274,7 +274,7 @@ struct DevBuf {
 };
 
 struct KindDev {
-  DevBuf inst, tiles, prep, work, packA, packB, exps;
+  DevBuf inst, tiles, prep, work, packA, packB, exps, queue;
   long ninst = 0, ntiles = 0, nwork = 0;
 };
 
@@ -283,7 +283,7 @@ cudaError_t upload_kind(const KindPlan<Cfg>& kp, KindDev& kd, cudaStream_t st) {
   cudaError_t e;
   if ((e = kd.inst.alloc(sizeof(GInst) * kp.inst.size())) || (e = kd.tiles.alloc(sizeof(GTile) * kp.tiles.size())) ||
       (e = kd.prep.alloc(sizeof(GPrepInst) * kp.prep.size())) || (e = kd.work.alloc(sizeof(uint2) * kp.work.size())) ||
-      (e = kd.packA.alloc(kp.bytesA)) ||
+      (e = kd.packA.alloc(kp.bytesA)) || (e = kd.queue.alloc(sizeof(unsigned long long))) ||
       (e = kd.packB.alloc(kp.bytesB)) || (e = kd.exps.alloc(sizeof(int32_t) * (kp.nexp + 1))))
     return e;
   if ((e = cudaMemcpyAsync(kd.inst.p, kp.inst.data(), sizeof(GInst) * kp.inst.size(), cudaMemcpyHostToDevice, st)) ||
@@ -301,7 +301,7 @@ cudaError_t upload_kind(const KindPlan<Cfg>& kp, KindDev& kd, cudaStream_t st) {
 
 template <class Cfg, int MODE, int S>
 cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, const char* prep_name,
-                        const char* gemm_name) {
+                        const char* gemm_name, bool dynamic_order) {
   if (kd.ninst == 0) return cudaSuccess;
   {
     ProfScope prof(prep_name, st);
@@ -332,11 +332,17 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
   prm.gtiles = (const GTile*)kd.tiles.p;
   prm.packA = (const uint8_t*)kd.packA.p;
   prm.packB = (const uint8_t*)kd.packB.p;
+  prm.queue = dynamic_order ? (unsigned long long*)kd.queue.p : nullptr;
+  // the device-side tile queue starts at tile 0 on every launch (a memset node when captured)
+  if (dynamic_order) {
+    cudaError_t e = cudaMemsetAsync(kd.queue.p, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+  }
   CUtensorMap dummy;
   memset(&dummy, 0, sizeof(dummy));
   const long grid = kd.ntiles < num_sms() ? kd.ntiles : num_sms();
   ProfScope prof(gemm_name, st);
-  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(dummy, dummy, prm);
+  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, tc::kThreadsGrouped, Cfg::SMEM, st>>>(dummy, dummy, prm);
   note_launch();
   return cudaGetLastError();
 }
@@ -354,6 +360,7 @@ using GCfgI8 = tc::Config<tc::KIND_I8, 1, 1, 128, 128, 6, 1, 2, tc::EPI_I32, 0>;
 struct Plan {
   std::vector<uint64_t> key;
   int oz_cfg = 0;            // Ozaki tile configuration (0: 128 x 64, 1: 128 x 32)
+  bool dynamic = true;       // tiles from the device-side queue (else the static stride)
   KindDev oz, bf, i8;
   std::unique_ptr<GroupedSimt> simt;
   void* const* C = nullptr;
@@ -392,12 +399,12 @@ std::vector<uint64_t> signature(const GroupedDesc& g, int mode, int oz_cfg) {
 cudaError_t run_plan(Plan& pl, cudaStream_t st) {
   cudaError_t e;
   if (pl.oz_cfg == 1) {
-    if ((e = launch_kind<GCfgOz32, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm"))) return e;
+    if ((e = launch_kind<GCfgOz32, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic))) return e;
   } else {
-    if ((e = launch_kind<GCfgOz, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm"))) return e;
+    if ((e = launch_kind<GCfgOz, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic))) return e;
   }
-  if ((e = launch_kind<GCfgBf, 1, 1>(pl.bf, pl.C, st, "grouped_split_bf16", "grouped_bf16x3_gemm"))) return e;
-  if ((e = launch_kind<GCfgI8, 0, 1>(pl.i8, pl.C, st, "grouped_pack_i8", "grouped_i8_gemm"))) return e;
+  if ((e = launch_kind<GCfgBf, 1, 1>(pl.bf, pl.C, st, "grouped_split_bf16", "grouped_bf16x3_gemm", pl.dynamic))) return e;
+  if ((e = launch_kind<GCfgI8, 0, 1>(pl.i8, pl.C, st, "grouped_pack_i8", "grouped_i8_gemm", pl.dynamic))) return e;
   if (pl.simt && (e = launch_simt_grouped(*pl.simt, st))) return e;
   return cudaSuccess;
 }
@@ -409,10 +416,12 @@ cudaError_t grouped_run(const GroupedDesc& g, cudaStream_t st) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  // 128 x 32 tiles with two accumulators by default (2.62 ms against 3.16 ms for the
-  // 10,000-instance uneven batch)
-  const int oz_cfg = choose_config(SSBLAS_PATH_GROUPED, 0, 0, 0, 0, 1) == 0 ? 0 : 1;
-  std::vector<uint64_t> key = signature(g, mode, oz_cfg);
+  // configurations: 0 = 128 x 64 Ozaki tiles, dynamic tile queue; 1 (default) = 128 x 32 Ozaki
+  // tiles with two accumulators, dynamic tile queue; 2 = 128 x 32 tiles, static tile order
+  const int gcfg = choose_config(SSBLAS_PATH_GROUPED, 0, 0, 0, 0, 1);
+  const int oz_cfg = gcfg == 0 ? 0 : 1;
+  const bool dynamic_order = gcfg != 2;
+  std::vector<uint64_t> key = signature(g, mode, gcfg);
   auto it = g_plans.find(dev);
   if (it != g_plans.end() && it->second->key == key) {
     Plan& pl = *it->second;
@@ -447,6 +456,7 @@ cudaError_t grouped_run(const GroupedDesc& g, cudaStream_t st) {
   auto pl = std::make_unique<Plan>();
   pl->key = std::move(key);
   pl->oz_cfg = oz_cfg;
+  pl->dynamic = dynamic_order;
   pl->C = g.C;
   std::vector<int> oz, bf, i8, plain;
   for (int i = 0; i < (int)g.inst.size(); ++i) {

@@ -30,6 +30,10 @@ namespace ssb {
 namespace tc {
 
 constexpr int kThreads = 320;
+// grouped launches add a scheduler warp (warp 10) that feeds the device-side tile queue
+constexpr int kThreadsGrouped = 352;
+template <bool GROUPED>
+constexpr int threads_of() { return GROUPED ? kThreadsGrouped : kThreads; }
 // exponent the slicing pre-passes give a row of op(A) / column of op(B) that holds an Inf or a NaN
 // (kNonFiniteExp of ozaki_digits.cuh)
 constexpr int kOzakiNonFiniteExp = 4096;
@@ -77,7 +81,23 @@ struct Params {
   const GTile* gtiles;
   const uint8_t* packA;
   const uint8_t* packB;
+  unsigned long long* queue;   // grouped launches: tile counter (zero at launch) shared by all CTAs,
+                               // or nullptr for the static order (tile blockIdx.x + i * gridDim.x)
 };
+
+// Grouped launches take tiles from a device-side queue: a scheduler warp (warp 10) of each CTA
+// claims the next tile with an atomic increment of prm.queue, decodes its instance record once,
+// and passes it to the TMA, MMA and epilogue warps through a ring of kTQ shared-memory slots
+// (tq_full: record written; tq_empty: the TMA warp, the MMA warp and the 8 epilogue warps are done
+// with it). The scheduler runs up to kTQ records ahead, so the claim and the record loads are off
+// the other warps' paths. A record with valid == 0 ends the CTA's tile sequence.
+constexpr int kTQ = 8;
+struct TileDesc {
+  GInst g;
+  const void* cptr;         // the instance's C pointer
+  int mt, nt, valid, pad;
+};
+constexpr int kTileQueueBytes = 2048;   // 2 x kTQ barriers + kTQ records
 
 struct TileInfo {
   int b, mt, nt, nk;
@@ -122,7 +142,7 @@ struct Config {
   static constexpr int TMEM_COLS_USED = ACCB * NLEV * BN;
   static constexpr int TMEM_COLS = TMEM_COLS_USED <= 32 ? 32 : TMEM_COLS_USED <= 64 ? 64 : TMEM_COLS_USED <= 128 ? 128
                                    : TMEM_COLS_USED <= 256 ? 256 : 512;
-  static constexpr int SMEM = 1024 + STAGES * STAGE + 256;
+  static constexpr int SMEM = 1024 + STAGES * STAGE + 256 + kTileQueueBytes;
   static_assert(TMEM_COLS_USED <= 512, "tensor memory overflow");
   static_assert(A_STAGE % 1024 == 0 && B_STAGE % 1024 == 0, "stage alignment");
   static_assert(SMEM <= 232448, "shared memory overflow");
@@ -138,7 +158,7 @@ struct Config {
 };
 
 template <class Cfg, bool GROUPED>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(threads_of<GROUPED>(), 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -150,6 +170,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   uint64_t* tempty = tfull + 2;
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+  uint64_t* tq_full = (uint64_t*)(smem + Cfg::STAGES * Cfg::STAGE + 256);
+  uint64_t* tq_empty = tq_full + kTQ;
+  TileDesc* tq = (TileDesc*)(tq_empty + kTQ);
+  static_assert(2 * kTQ * 8 + kTQ * sizeof(TileDesc) <= kTileQueueBytes, "tile queue size");
 
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
@@ -165,6 +189,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       ptx::mbar_init(ptx::smem_u32(&tempty[a]), 8);
     }
     ptx::mbar_init(ptx::smem_u32(drain), 1);
+    if (GROUPED) {
+      for (int q = 0; q < kTQ; ++q) {
+        ptx::mbar_init(ptx::smem_u32(&tq_full[q]), 1);
+        ptx::mbar_init(ptx::smem_u32(&tq_empty[q]), 10);
+      }
+    }
     ptx::fence_mbar_init();
   }
   if (!GROUPED && warp == 0 && lane == 0) {
@@ -189,14 +219,23 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (lane == 0) {
       long it = 0;
       bool ok = true;
-      for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x) {
-        const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
+      for (long i = 0, t = blockIdx.x; ok; ++i, t += gridDim.x) {
+        TileInfo ti{};
         const uint8_t* srcA = nullptr;
         const uint8_t* srcB = nullptr;
         if constexpr (GROUPED) {
-          const GInst& gi = prm.ginst[ti.b];
-          srcA = prm.packA + gi.offA + (size_t)ti.mt * ti.nk * Cfg::A_STAGE;
-          srcB = prm.packB + gi.offB + (size_t)ti.nt * ti.nk * Cfg::B_STAGE;
+          // the next record of the tile queue
+          const int slot = (int)(i % kTQ);
+          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((i / kTQ) & 1), err, 13)) break;
+          const TileDesc& d = tq[slot];
+          if (!d.valid) break;
+          ti.mt = d.mt; ti.nt = d.nt; ti.nk = d.g.nk;
+          srcA = prm.packA + d.g.offA + (size_t)ti.mt * ti.nk * Cfg::A_STAGE;
+          srcB = prm.packB + d.g.offB + (size_t)ti.nt * ti.nk * Cfg::B_STAGE;
+          ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));
+        } else {
+          if (t >= prm.total_tiles) break;
+          ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
         }
         for (int kb = 0; kb < ti.nk; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
@@ -226,8 +265,19 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       long it = 0;
       int tcount = 0;
       bool ok = true;
-      for (long t = blockIdx.x; t < prm.total_tiles && ok; t += gridDim.x, ++tcount) {
-        const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
+      for (long t = blockIdx.x; ok; t += gridDim.x, ++tcount) {
+        TileInfo ti{};
+        int slot = 0;
+        if constexpr (GROUPED) {
+          slot = tcount % kTQ;
+          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 24)) break;
+          if (!tq[slot].valid) break;
+          ti.nk = tq[slot].g.nk;
+          ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));   // the MMA warp only needs nk
+        } else {
+          if (t >= prm.total_tiles) break;
+          ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
+        }
         const int acc = tcount % Cfg::ACCB;
         const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
         if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21)) { ok = false; break; }
@@ -287,6 +337,32 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       ptx::mma_commit(ptx::smem_u32(drain));
       ptx::mbar_wait(ptx::smem_u32(drain), 0, err, 23);
     }
+  } else if (GROUPED && warp == 10) {
+    // ------------------------------------------------------------------ scheduler ---------
+    if constexpr (GROUPED) {
+      if (lane == 0) {
+        for (long i = 0;; ++i) {
+          const int slot = (int)(i % kTQ);
+          const bool ok = ptx::mbar_wait(ptx::smem_u32(&tq_empty[slot]), (uint32_t)(((i / kTQ) & 1) ^ 1), err, 14);
+          TileDesc& d = tq[slot];
+          // dynamic order from the queue counter, or (without a counter) the static stride
+          const long q = !ok ? prm.total_tiles
+                             : prm.queue ? (long)atomicAdd(prm.queue, 1ull) : (long)blockIdx.x + i * (long)gridDim.x;
+          if (q >= prm.total_tiles) {
+            d.valid = 0;
+            ptx::mbar_arrive(ptx::smem_u32(&tq_full[slot]));
+            break;
+          }
+          const GTile gt = prm.gtiles[q];
+          d.g = prm.ginst[gt.inst];
+          d.cptr = prm.C[d.g.idx];
+          d.mt = gt.mt;
+          d.nt = gt.nt;
+          d.valid = 1;
+          ptx::mbar_arrive(ptx::smem_u32(&tq_full[slot]));
+        }
+      }
+    }
   } else {
     // ------------------------------------------------------------------ epilogue ----------
     // 8 warps: warp w reads TMEM lanes 32*(w%4) .. +31 (its rows) and half (w-2)/4 of the columns
@@ -295,8 +371,19 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int half = (warp - 2) / 4;
     const int row_in_tile = quarter * 32 + lane;
     int tcount = 0;
-    for (long t = blockIdx.x; t < prm.total_tiles; t += gridDim.x, ++tcount) {
-      const TileInfo ti = tile_info<GROUPED>(prm, t, tiles_mn, nk_uniform);
+    for (long t = blockIdx.x;; t += gridDim.x, ++tcount) {
+      TileInfo ti{};
+      int slot = 0;
+      if constexpr (GROUPED) {
+        slot = tcount % kTQ;
+        if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 32)) break;
+        if (!tq[slot].valid) break;
+        ti.mt = tq[slot].mt;
+        ti.nt = tq[slot].nt;
+      } else {
+        if (t >= prm.total_tiles) break;
+        ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
+      }
       long m = prm.m, n = prm.n, ldc = prm.ldc;
       double alpha_d = prm.alpha_d, beta_d = prm.beta_d;
       float alpha_f = prm.alpha_f, beta_f = prm.beta_f;
@@ -305,13 +392,16 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const int32_t* exb = prm.exp_b + (long)ti.b * prm.n;
       uint8_t* Cb;
       if constexpr (GROUPED) {
-        const GInst& g = prm.ginst[ti.b];
+        const GInst& g = tq[slot].g;
         m = g.m; n = g.n; ldc = g.ldc;
         alpha_d = g.alpha_d; beta_d = g.beta_d; alpha_f = g.alpha_f; beta_f = g.beta_f;
         alpha_i = g.alpha_i; beta_i = g.beta_i;
         exa = prm.exp_a + g.offEA;
         exb = prm.exp_a + g.offEB;
-        Cb = (uint8_t*)prm.C[g.idx];
+        Cb = (uint8_t*)tq[slot].cptr;
+        // the record is copied: release the slot
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));
       } else {
         Cb = (uint8_t*)prm.C[ti.b + prm.c_batch_offset];
       }

@@ -100,10 +100,11 @@ def test_grouped_long_k_instances():
         S.set_math_mode(0)
 
 
-@pytest.mark.parametrize("cfg", [0, 1])
+@pytest.mark.parametrize("cfg", [0, 1, 2])
 def test_grouped_ozaki_tile_configurations(cfg):
-    """Both Ozaki tile configurations of the grouped path (0: 128 x 64 tiles, one accumulator;
-    1: 128 x 32 tiles, two accumulators) give the bit-exact Ozaki result, fresh and replayed."""
+    """Every configuration of the grouped path (0: 128 x 64 Ozaki tiles, one accumulator, tiles
+    from the device-side queue; 1: 128 x 32 tiles, two accumulators, queue; 2: 128 x 32 tiles in
+    the static order) gives the bit-exact Ozaki result, fresh and replayed."""
     import ssblasex_b200 as S
     from ssblasex_b200 import runner
     S.set_math_mode(3)

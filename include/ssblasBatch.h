@@ -97,6 +97,8 @@ typedef struct {
   int kernel_launches;
   int device_error;  /* nonzero if a bounded device-side wait gave up (the call then returned
                         SSBLAS_STATUS_INTERNAL_ERROR) */
+  int split_k;       /* K pieces per output tile of a tcgen05 GEMM (1 = not split; 0 on the
+                        paths without split-K) */
 } ssblasRunInfo_t;
 
 typedef enum {
@@ -107,10 +109,18 @@ typedef enum {
   SSBLAS_PATH_BF16X3_TCGEN05 = 4,  /* fp32 via three BF16 split products, tcgen05 kind::f16 */
   SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch */
   SSBLAS_PATH_DMMA = 6,            /* plain fp64 on the FP64 tensor cores (mma.sync f64) */
-  SSBLAS_PATH_OZAKI_SLICER = 7     /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
+  SSBLAS_PATH_OZAKI_SLICER = 7,    /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
                                       pre-pass. 0 (default) and 3: one pass with thread-block
                                       clusters of 16 rows x 512 k per CTA when k <= 2048; 2: the
-                                      same with 32 rows x 256 k; 1: exponent pass then digit pass */
+                                      same with 32 rows x 256 k; 4: 8 rows x 1024 k; 1: exponent
+                                      pass then digit pass */
+  SSBLAS_PATH_SPLITK_I8 = 8,       /* not a path: ssblasSetKernelConfig keys of the split-K factor */
+  SSBLAS_PATH_SPLITK_OZAKI = 9     /* of the int8 and Ozaki tcgen05 GEMMs. config = number of K
+                                      pieces per output tile (1 = none, at most 64), 0 = automatic
+                                      (split only when the tiles fill less than half of the SMs).
+                                      Each piece's exact int32 sums are added in 64 bits, so the
+                                      result does not depend on the factor; the Ozaki GEMM always
+                                      splits k > 16384 into pieces of at most 16384. */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

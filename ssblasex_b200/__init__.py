@@ -51,7 +51,7 @@ class KernelProfile(ct.Structure):
 
 class RunInfo(ct.Structure):
     _fields_ = [("path", ct.c_int), ("slices", ct.c_int), ("kernel_launches", ct.c_int),
-                ("device_error", ct.c_int)]
+                ("device_error", ct.c_int), ("split_k", ct.c_int)]
 
 
 _lib = None
@@ -135,7 +135,8 @@ def last_run_info() -> dict:
     info = RunInfo()
     lib().ssblasGetLastRunInfo(ct.byref(info))
     return {"path": PATH_NAMES.get(info.path, str(info.path)), "slices": info.slices,
-            "kernel_launches": info.kernel_launches, "device_error": info.device_error}
+            "kernel_launches": info.kernel_launches, "device_error": info.device_error,
+            "split_k": info.split_k}
 
 
 def release_workspace() -> int:
@@ -156,7 +157,7 @@ def get_profile() -> dict:
 
 
 PATH_IDS = {"simt": 1, "i8_tcgen05": 2, "ozaki_tcgen05": 3, "bf16x3_tcgen05": 4, "grouped": 5, "dmma": 6,
-            "ozaki_slicer": 7}
+            "ozaki_slicer": 7, "splitk_i8": 8, "splitk_ozaki": 9}
 
 
 def set_kernel_config(path: str, config: int) -> int:

@@ -40,6 +40,19 @@ FAMILIES = {
         dict(row="f64", transa=1, transb=0, m=256, n=256, k=2048, batch=32, alpha=1.0, beta=0.0,
              dist="expspread"),
     ]),
+    # split-K factor (K pieces per output tile) of the Ozaki GEMM, on shapes with few tiles
+    "splitk_ozaki": (SSBLAS_MATH_FP64_OZAKI, [1, 2, 4, 8, 16], "(all)", [
+        dict(row="f64", transa=1, transb=0, m=256, n=256, k=8192, batch=2, alpha=1.0, beta=0.0,
+             dist="expspread"),
+        dict(row="f64", transa=0, transb=1, m=512, n=512, k=4096, batch=1, alpha=1.0, beta=0.0,
+             dist="expspread"),
+    ]),
+    "splitk_i8": (SSBLAS_MATH_PLAIN, [1, 2, 4, 8, 16], "i8_gemm", [
+        dict(row="i8", transa=1, transb=0, m=512, n=512, k=16384, batch=1, alpha=1, beta=0,
+             lda=16384, ldb=16384, ldc=512),
+        dict(row="i8", transa=1, transb=0, m=1024, n=1024, k=8192, batch=2, alpha=1, beta=0,
+             lda=8192, ldb=8192, ldc=1024),
+    ]),
     "i8_tcgen05": (SSBLAS_MATH_PLAIN, [0, 1], "i8_gemm", [
         dict(row="i8", transa=1, transb=0, m=512, n=512, k=512, batch=512, alpha=1, beta=1,
              lda=512, ldb=512, ldc=512),

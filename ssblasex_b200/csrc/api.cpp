@@ -103,6 +103,7 @@ static void prof_resolve() {
 }
 
 void note_launch(int count) { g_info.kernel_launches += count; }
+void note_splits(int splits) { g_info.split_k = splits; }
 void note_path(int path, int slices) {
   g_info.path = path;
   g_info.slices = slices;

@@ -328,6 +328,7 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
   prm.exp_b = (const int32_t*)kd.exps.p;
   prm.exp_shift = -12;
   prm.err = device_error_flag();
+  prm.splits = 1;
   prm.ginst = (const GInst*)kd.inst.p;
   prm.gtiles = (const GTile*)kd.tiles.p;
   prm.packA = (const uint8_t*)kd.packA.p;

@@ -42,12 +42,14 @@ struct Settings {
 Settings& settings();
 
 // Device workspace: a grow-only cached allocation per device and slot.
-enum WsSlot { WS_PTRS = 0, WS_PACK_A, WS_PACK_B, WS_EXP, WS_STAGE_A, WS_STAGE_B, WS_STAGE_C, WS_MISC, WS_NUM };
+enum WsSlot { WS_PTRS = 0, WS_PACK_A, WS_PACK_B, WS_EXP, WS_STAGE_A, WS_STAGE_B, WS_STAGE_C, WS_MISC, WS_SPLIT,
+               WS_SPLIT_CNT, WS_ROWMAX, WS_NUM };
 void* workspace(WsSlot slot, size_t bytes, cudaError_t* err);
 
 // Launch bookkeeping for ssblasGetLastRunInfo and the benchmark's launch count.
 void note_launch(int count = 1);
 void note_path(int path, int slices = 0);
+void note_splits(int splits);
 
 // Device-side error flag (set by kernels whose bounded waits give up).
 int* device_error_flag();

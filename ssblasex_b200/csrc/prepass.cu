@@ -322,18 +322,89 @@ __global__ void __launch_bounds__(NTH) ozaki_rowexp_kernel(PlaneArgs a0, int32_t
   }
 }
 
+// K-parallel form of the exponent pass: one CTA per (instance, 32 rows, MKT k) part; each row's
+// maximum of the |x| bit patterns over the part goes to bits[b * rows + r] by atomicMax (bits zero
+// at launch), so problems with few rows and long K still spread over all SMs.
+constexpr int MKT = 256;   // short parts: several CTAs per SM keep enough loads in flight
+__global__ void __launch_bounds__(NTH) ozaki_rowmax_kernel(PlaneArgs a0, unsigned long long* m0, long n0,
+                                                           PlaneArgs a1, unsigned long long* m1) {
+  __shared__ unsigned long long red[8][RT];
+  const bool second = blockIdx.x >= n0;
+  const PlaneArgs a = second ? a1 : a0;
+  unsigned long long* __restrict__ bits = second ? m1 : m0;
+  const long blk = second ? blockIdx.x - n0 : blockIdx.x;
+  const long blocks_per_inst = (a.rows + RT - 1) / RT;
+  const long kparts = (a.K + MKT - 1) / MKT;
+  const long item = blk / kparts;
+  const long klo = (blk % kparts) * MKT;
+  const long khi = klo + MKT < a.K ? klo + MKT : a.K;
+  const long b = item / blocks_per_inst;
+  const long row0 = (item % blocks_per_inst) * RT;
+  const double* X = (const double*)a.X[b];
+  unsigned long long mx = 0;
+  if (a.kcontig) {
+    // 8 threads per row, 16 loads in flight each
+    const int r = threadIdx.x / 8, part = threadIdx.x % 8;
+    const long gr = row0 + r;
+    if (gr < a.rows) {
+      const double* row = X + gr * a.ld;
+      long k = klo + part;
+      for (; k + 120 < khi; k += 128) {
+        double t[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) t[j] = __ldg(row + k + 8 * j);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) mx = max_u64(mx, abs_bits(t[j]));
+      }
+      for (; k < khi; k += 8) mx = max_u64(mx, abs_bits(__ldg(row + k)));
+    }
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (part == 0) red[0][r] = mx;
+  } else {
+    // a warp reads 32 adjacent rows of one k; 8 warps split the k range
+    const int r = threadIdx.x % 32, part = threadIdx.x / 32;
+    const long gr = row0 + r;
+    if (gr < a.rows) {
+      const double* col = X + gr;
+      long k = klo + part;
+      for (; k + 120 < khi; k += 128) {
+        double t[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) t[j] = __ldg(col + (k + 8 * j) * a.ld);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) mx = max_u64(mx, abs_bits(t[j]));
+      }
+      for (; k < khi; k += 8) mx = max_u64(mx, abs_bits(__ldg(col + k * a.ld)));
+    }
+    red[part][r] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < RT) {
+    unsigned long long m2 = red[0][threadIdx.x];
+    if (!a.kcontig)
+      for (int q = 1; q < 8; ++q) m2 = max_u64(m2, red[q][threadIdx.x]);
+    const long gr = row0 + threadIdx.x;
+    if (gr < a.rows && m2 != 0) atomicMax(bits + b * a.rows + gr, m2);
+  }
+}
+
 constexpr int DKT = 128;                // k per digits chunk
 constexpr int DPER = RT * DKT / NTH;     // 16 elements per thread
 constexpr int DPITCH = DKT + 4;          // 33 words per staged row: conflict-free
 
-template <int S>
-__global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const int32_t* e0, long n0, PlaneArgs a1,
-                                                           const int32_t* e1) {
+// FROM_BITS: the row maxima come as |x| bit patterns (ozaki_rowmax_kernel) in bits0/bits1; the
+// exponents are derived here and the chunks at k0 = 0 store them to e0/e1. Otherwise e0/e1 hold
+// the exponents already (ozaki_rowexp_kernel).
+template <int S, bool FROM_BITS>
+__global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t* e0, long n0, PlaneArgs a1,
+                                                           int32_t* e1, const unsigned long long* bits0,
+                                                           const unsigned long long* bits1) {
   __shared__ __align__(16) uint8_t st[S * RT * DPITCH];
   __shared__ double rscale[RT][2];
   const bool second = blockIdx.x >= n0;
   const PlaneArgs a = second ? a1 : a0;
-  const int32_t* __restrict__ exps = second ? e1 : e0;
+  int32_t* __restrict__ exps = second ? e1 : e0;
   const long blk = second ? blockIdx.x - n0 : blockIdx.x;
   const long blocks_per_inst = (a.rows + RT - 1) / RT;
   const long kchunks = (a.K + DKT - 1) / DKT;
@@ -362,7 +433,15 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, const i
   }
   if (threadIdx.x < RT) {
     const long gr = row0 + threadIdx.x;
-    const int e = gr < a.rows ? exps[b * a.rows + gr] : 0;
+    int e = 0;
+    if (gr < a.rows) {
+      if constexpr (FROM_BITS) {
+        e = row_exponent((second ? bits1 : bits0)[b * a.rows + gr]);
+        if (k0 == 0) exps[b * a.rows + gr] = e;
+      } else {
+        e = exps[b * a.rows + gr];
+      }
+    }
     row_scale(S, e, rscale[threadIdx.x][0], rscale[threadIdx.x][1]);
   }
   __syncthreads();
@@ -859,27 +938,35 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
   const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0);
   if (form != 1 && cluster_kernel_fits(a) && b.K == a.K)
     return launch_ozaki_cluster(a, ea, b, eb, true, slices, form, st);
+  // two passes over both operands: row maxima per (32 rows, 256 k) part, then digits per
+  // (32 rows, 128 k) chunk -- both spread over all SMs whatever the row count
   const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
+  const long parts_a = items_a * ((a.K + MKT - 1) / MKT), parts_b = items_b * ((b.K + MKT - 1) / MKT);
   const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);
-  if (items_a + items_b < 2L * num_sms() || chunks_a + chunks_b >= (1L << 31)) {
+  if (chunks_a + chunks_b >= (1L << 31)) {
     cudaError_t e = launch_ozaki_slice(a, slices, ea, st);
     return e != cudaSuccess ? e : launch_ozaki_slice(b, slices, eb, st);
   }
-  // enough rows to fill the GPU: exponents of both operands, then digits of both, per chunk
+  cudaError_t e;
+  const size_t nbits = (size_t)(a.rows * a.batch + b.rows * b.batch);
+  unsigned long long* bits = (unsigned long long*)workspace(WS_ROWMAX, sizeof(unsigned long long) * nbits, &e);
+  if (!bits) return e;
+  unsigned long long* bits_b = bits + a.rows * a.batch;
+  if ((e = cudaMemsetAsync(bits, 0, sizeof(unsigned long long) * nbits, st)) != cudaSuccess) return e;
   {
-    ProfScope prof("ozaki_rowexp", st);
-    ozaki_rowexp_kernel<<<(unsigned)(items_a + items_b), NTH, 0, st>>>(a, ea, items_a, b, eb);
+    ProfScope prof("ozaki_rowmax", st);
+    ozaki_rowmax_kernel<<<(unsigned)(parts_a + parts_b), NTH, 0, st>>>(a, bits, parts_a, b, bits_b);
     note_launch();
   }
   ProfScope prof("ozaki_slice", st);
   const unsigned g = (unsigned)(chunks_a + chunks_b);
   switch (slices) {
-    case 3: ozaki_digits_kernel<3><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
-    case 4: ozaki_digits_kernel<4><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
-    case 5: ozaki_digits_kernel<5><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
-    case 6: ozaki_digits_kernel<6><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
-    case 7: ozaki_digits_kernel<7><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
-    case 8: ozaki_digits_kernel<8><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb); break;
+    case 3: ozaki_digits_kernel<3, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
+    case 4: ozaki_digits_kernel<4, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
+    case 5: ozaki_digits_kernel<5, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
+    case 6: ozaki_digits_kernel<6, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
+    case 7: ozaki_digits_kernel<7, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
+    case 8: ozaki_digits_kernel<8, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;
     default: return cudaErrorInvalidValue;
   }
   note_launch();
@@ -900,12 +987,12 @@ cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cu
     }
     ProfScope prof("ozaki_slice", st);
     switch (slices) {
-      case 3: ozaki_digits_kernel<3><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
-      case 4: ozaki_digits_kernel<4><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
-      case 5: ozaki_digits_kernel<5><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
-      case 6: ozaki_digits_kernel<6><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
-      case 7: ozaki_digits_kernel<7><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
-      case 8: ozaki_digits_kernel<8><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps); break;
+      case 3: ozaki_digits_kernel<3, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
+      case 4: ozaki_digits_kernel<4, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
+      case 5: ozaki_digits_kernel<5, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
+      case 6: ozaki_digits_kernel<6, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
+      case 7: ozaki_digits_kernel<7, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
+      case 8: ozaki_digits_kernel<8, false><<<(unsigned)chunks, NTH, 0, st>>>(a, exps, chunks, a, exps, nullptr, nullptr); break;
       default: return cudaErrorInvalidValue;
     }
     note_launch();

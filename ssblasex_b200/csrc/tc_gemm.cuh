@@ -83,6 +83,15 @@ struct Params {
   const uint8_t* packB;
   unsigned long long* queue;   // grouped launches: tile counter (zero at launch) shared by all CTAs,
                                // or nullptr for the static order (tile blockIdx.x + i * gridDim.x)
+  // split-K (batched launches, integer and Ozaki epilogues): work unit u is split u % splits of
+  // tile u / splits and covers K blocks [split * kb_per_split, +kb_per_split) of it. Each unit
+  // stores its int32 level sums to split_ws ([tile][split][level][BN column][128 rows]); the
+  // epilogue warp that arrives last at its region of the tile (split_cnt[tile * 8 + warp - 2],
+  // zero at launch) adds the splits' sums in 64 bits and writes C.
+  int splits;
+  int kb_per_split;
+  int32_t* split_ws;
+  int* split_cnt;
 };
 
 // Grouped launches take tiles from a device-side queue: a scheduler warp (warp 10) of each CTA
@@ -100,25 +109,22 @@ struct TileDesc {
 constexpr int kTileQueueBytes = 2048;   // 2 x kTQ barriers + kTQ records
 
 struct TileInfo {
-  int b, mt, nt, nk;
+  int b, mt, nt;
+  int kb0, kb1;             // K blocks [kb0, kb1) of the tile
+  int sp;                   // split index
 };
 
-template <bool GROUPED>
+// work unit t of a batched launch -> instance, tile, K range
 __device__ __forceinline__ TileInfo tile_info(const Params& p, long t, long tiles_mn, int nk) {
   TileInfo ti;
-  if constexpr (GROUPED) {
-    const GTile g = p.gtiles[t];
-    ti.b = g.inst;
-    ti.mt = g.mt;
-    ti.nt = g.nt;
-    ti.nk = p.ginst[g.inst].nk;
-  } else {
-    ti.b = (int)(t / tiles_mn);
-    const long r = t % tiles_mn;
-    ti.mt = (int)(r / p.tiles_n);
-    ti.nt = (int)(r % p.tiles_n);
-    ti.nk = nk;
-  }
+  const long tile = p.splits > 1 ? t / p.splits : t;
+  ti.sp = (int)(t - tile * p.splits);
+  ti.b = (int)(tile / tiles_mn);
+  const long r = tile % tiles_mn;
+  ti.mt = (int)(r / p.tiles_n);
+  ti.nt = (int)(r % p.tiles_n);
+  ti.kb0 = ti.sp * p.kb_per_split;
+  ti.kb1 = min(nk, ti.kb0 + p.kb_per_split);
   return ti;
 }
 
@@ -156,6 +162,163 @@ struct Config {
     return PAIRS == 2 ? (p == 0) : (p == 0 && q == 0);
   }
 };
+
+// Ozaki epilogue of one thread's row gi: C(gi, j) = alpha * v_j * 2^(ea + eb_j + exp_shift) + beta * C
+// for the columns j = n0 + 16c + jj below n.
+template <int CH>
+__device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long ldc, int32_t ea,
+                                            const int32_t* exb, int exp_shift, double alpha_d, double beta_d,
+                                            const double (&v)[CH][16]) {
+#pragma unroll
+  for (int c = 0; c < CH; ++c)
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const long gj = n0 + c * 16 + j;
+      if (gj < n) {
+        // v * 2^E: one multiplication by the exact power of two when 2^E is a normal double
+        // (correctly rounded, so equal to scalbn), scalbn otherwise
+        const int eb = exb[gj];
+        const int E = ea + eb + exp_shift;
+        double* cp = Cd + gi + gj * ldc;
+        if (E >= -1022 && E <= 1023) {
+          const double w = v[c][j] * __longlong_as_double((long long)(E + 1023) << 52);
+          const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+          *cp = fma(w, alpha_d, tb);
+        } else if (ea == kOzakiNonFiniteExp || eb == kOzakiNonFiniteExp) {
+          // row i of op(A) or column j of op(B) holds an Inf or a NaN
+          *cp = __longlong_as_double((long long)0x7FF8000000000000ull);
+        } else {
+          const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+          *cp = fma(scalbn(v[c][j], E), alpha_d, tb);
+        }
+      }
+    }
+}
+
+// int32 epilogue of one thread's row (Ci = &C(gi, 0)): C(gi, j) = alpha * raw + beta * C with
+// wrapping int32 arithmetic, columns j = nb + 16c + jj below n. C is read (all reads first) only
+// when beta != 0.
+template <int GC>
+__device__ __forceinline__ void i32_store(int32_t* Ci, long nb, long n, long ldc, int32_t alpha_i, int32_t beta_i,
+                                          const uint32_t (&raw)[GC][16]) {
+  uint32_t cv[GC][16];
+  if (beta_i != 0) {
+#pragma unroll
+    for (int c = 0; c < GC; ++c)
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const long gj = nb + 16 * c + j;
+        cv[c][j] = (gj < n) ? (uint32_t)__ldcs(Ci + gj * ldc) : 0u;
+      }
+  }
+#pragma unroll
+  for (int c = 0; c < GC; ++c)
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const long gj = nb + 16 * c + j;
+      if (gj < n) {
+        const uint32_t t = (beta_i == 0) ? 0u : (uint32_t)beta_i * cv[c][j];
+        __stcs(Ci + gj * ldc, (int32_t)(t + raw[c][j] * (uint32_t)alpha_i));
+      }
+    }
+}
+
+// sum[j] += w[s * unit + j * pitch] over the pieces s < splits, four pieces' loads in flight at
+// once (the sums are read once, from L2).
+template <int PITCH>
+__device__ __forceinline__ void add_pieces(const int32_t* w, long unit, int splits, long long (&sum)[16]) {
+  int s = 0;
+#pragma unroll 1
+  for (; s + 4 <= splits; s += 4) {
+    int32_t x[4][16];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 16; ++j) x[u][j] = __ldcg(w + (s + u) * unit + j * PITCH);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 16; ++j) sum[j] += x[u][j];
+  }
+#pragma unroll 1
+  for (; s < splits; ++s) {
+    int32_t x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = __ldcg(w + s * unit + j * PITCH);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) sum[j] += x[j];
+  }
+}
+
+// Split-K epilogue of one epilogue warp's region of a tile (rows row_in_tile of the warp, columns
+// [half * HALF, +HALF) of the tile) for split `sp` of `splits`: store this split's level sums from
+// tensor memory to the workspace (the warp's 32 rows of one column are adjacent, so every store
+// is one 128-byte line), hand the accumulator back to the MMA warp, then count the arrival. The
+// warp that arrives last adds all splits' sums (64-bit, exact) and writes C. Not inlined, so its
+// registers do not add to the other epilogue paths'.
+template <class Cfg, int HALF>
+__device__ __noinline__ void split_k_region(uint32_t t_row, int32_t* split_ws, int* split_cnt, long tile, int splits,
+                                            int sp, int half, int region, int row_in_tile, int lane,
+                                            uint32_t tempty_bar, bool row_ok, uint8_t* Cb, long gi, long n0, long n,
+                                            long ldc, int32_t ea, const int32_t* exb, int exp_shift, double alpha_d,
+                                            double beta_d, int32_t alpha_i, int32_t beta_i) {
+  constexpr long UNIT = (long)Cfg::NLEV * Cfg::BN * Cfg::BM;   // int32 per (tile, split)
+  const long off = (long)half * HALF * Cfg::BM + row_in_tile;
+  const int32_t* wt = split_ws + tile * splits * UNIT + off;
+  {
+    int32_t* wm = split_ws + (tile * splits + sp) * UNIT + off;
+#pragma unroll 1
+    for (int l = 0; l < Cfg::NLEV; ++l) {
+#pragma unroll 1
+      for (int c = 0; c < HALF / 16; ++c) {
+        uint32_t raw[16];
+        ptx::tmem_ld16(t_row + (uint32_t)(l * Cfg::BN + c * 16), raw);
+        ptx::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) __stcg(wm + ((long)l * Cfg::BN + c * 16 + j) * Cfg::BM, (int)raw[j]);
+      }
+    }
+  }
+  ptx::tc_fence_before();
+  __syncwarp();
+  if (lane == 0) ptx::mbar_arrive(tempty_bar);
+  __threadfence();   // this lane's sums are visible before the arrival is counted
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) last = atomicAdd(split_cnt + tile * 8 + region, 1) == splits - 1;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __threadfence();   // the other splits' sums are read after their arrivals were seen
+#pragma unroll 1
+  for (int c = 0; c < HALF / 16; ++c) {
+    if (n0 + c * 16 >= n) break;   // columns outside C
+    if constexpr (Cfg::EPI == EPI_OZAKI) {
+      // Horner over the levels (l = NLEV-1 .. 0: v = v * 2^-8 + acc_l), acc_l summed over the splits
+      double v[1][16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[0][j] = 0.0;
+#pragma unroll 1
+      for (int l = Cfg::NLEV - 1; l >= 0; --l) {
+        long long sum[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) sum[j] = 0;
+        add_pieces<Cfg::BM>(wt + ((long)l * Cfg::BN + c * 16) * Cfg::BM, UNIT, splits, sum);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[0][j] = v[0][j] * 0x1p-8 + (double)sum[j];
+      }
+      if (row_ok) ozaki_store<1>((double*)Cb, gi, n0 + c * 16, n, ldc, ea, exb, exp_shift, alpha_d, beta_d, v);
+    } else {
+      long long sum[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) sum[j] = 0;
+      add_pieces<Cfg::BM>(wt + (long)c * 16 * Cfg::BM, UNIT, splits, sum);
+      uint32_t raw[1][16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) raw[0][j] = (uint32_t)sum[j];   // the int32 sum, wrapped
+      if (row_ok) i32_store<1>((int32_t*)Cb + gi, n0 + c * 16, n, ldc, alpha_i, beta_i, raw);
+    }
+  }
+}
 
 template <class Cfg, bool GROUPED>
 __global__ void __launch_bounds__(threads_of<GROUPED>(), 1)
@@ -229,15 +392,15 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((i / kTQ) & 1), err, 13)) break;
           const TileDesc& d = tq[slot];
           if (!d.valid) break;
-          ti.mt = d.mt; ti.nt = d.nt; ti.nk = d.g.nk;
-          srcA = prm.packA + d.g.offA + (size_t)ti.mt * ti.nk * Cfg::A_STAGE;
-          srcB = prm.packB + d.g.offB + (size_t)ti.nt * ti.nk * Cfg::B_STAGE;
+          ti.mt = d.mt; ti.nt = d.nt; ti.kb0 = 0; ti.kb1 = d.g.nk;
+          srcA = prm.packA + d.g.offA + (size_t)ti.mt * ti.kb1 * Cfg::A_STAGE;
+          srcB = prm.packB + d.g.offB + (size_t)ti.nt * ti.kb1 * Cfg::B_STAGE;
           ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));
         } else {
           if (t >= prm.total_tiles) break;
-          ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
+          ti = tile_info(prm, t, tiles_mn, nk_uniform);
         }
-        for (int kb = 0; kb < ti.nk; ++kb, ++it) {
+        for (int kb = ti.kb0; kb < ti.kb1; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
           if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11)) { ok = false; break; }
@@ -272,20 +435,22 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           slot = tcount % kTQ;
           if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 24)) break;
           if (!tq[slot].valid) break;
-          ti.nk = tq[slot].g.nk;
+          ti.kb0 = 0;
+          ti.kb1 = tq[slot].g.nk;
           ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));   // the MMA warp only needs nk
         } else {
           if (t >= prm.total_tiles) break;
-          ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
+          ti = tile_info(prm, t, tiles_mn, nk_uniform);
         }
         const int acc = tcount % Cfg::ACCB;
         const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
         if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21)) { ok = false; break; }
         ptx::tc_fence_after();
         const uint32_t d_base = tmem_base + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
-        for (int kb = 0; kb < ti.nk; ++kb, ++it) {
+        for (int kb = ti.kb0; kb < ti.kb1; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
+          const bool acc_k = kb > ti.kb0;   // this K block adds to the blocks before it
           if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), ph, err, 22)) { ok = false; break; }
           ptx::tc_fence_after();
           const uint32_t sa = ptx::smem_u32(stages + (size_t)s * Cfg::STAGE);
@@ -307,7 +472,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
                   const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
                   const uint64_t bd = ptx::smem_desc_kmajor(sb + q0 * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
-                  ptx::mma_i8(d, ad, bd, idesc, (kb > 0 || kk > 0 || p > 0) ? 1u : 0u);
+                  ptx::mma_i8(d, ad, bd, idesc, (acc_k || kk > 0 || p > 0) ? 1u : 0u);
                 }
               }
             }
@@ -322,7 +487,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
                 const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
                 const uint64_t bd = ptx::smem_desc_kmajor(sb + q * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
-                const uint32_t accum = (kb > 0 || kk > 0 || !Cfg::first_of_level(p, q)) ? 1u : 0u;
+                const uint32_t accum = (acc_k || kk > 0 || !Cfg::first_of_level(p, q)) ? 1u : 0u;
                 if (Cfg::KIND == KIND_I8) ptx::mma_i8(d, ad, bd, IDESC, accum);
                 else ptx::mma_f16(d, ad, bd, IDESC, accum);
               }
@@ -382,7 +547,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ti.nt = tq[slot].nt;
       } else {
         if (t >= prm.total_tiles) break;
-        ti = tile_info<false>(prm, t, tiles_mn, nk_uniform);
+        ti = tile_info(prm, t, tiles_mn, nk_uniform);
       }
       long m = prm.m, n = prm.n, ldc = prm.ldc;
       double alpha_d = prm.alpha_d, beta_d = prm.beta_d;
@@ -414,6 +579,15 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) +
                              (uint32_t)(acc * Cfg::NLEV * Cfg::BN + half * HALF);
       const bool row_ok = gi < m;
+      if constexpr (!GROUPED && Cfg::EPI != EPI_F32) {
+        if (prm.splits > 1) {
+          split_k_region<Cfg, HALF>(t_row, prm.split_ws, prm.split_cnt, t / prm.splits, prm.splits, ti.sp, half,
+                                    warp - 2, row_in_tile, lane, ptx::smem_u32(&tempty[acc]), row_ok, Cb, gi, n0, n,
+                                    ldc, (Cfg::EPI == EPI_OZAKI && row_ok) ? exa[gi] : 0, exb, prm.exp_shift, alpha_d, beta_d,
+                                    alpha_i, beta_i);
+          continue;
+        }
+      }
       if constexpr (Cfg::EPI == EPI_OZAKI) {
         // Horner over the levels (l = NLEV-1 .. 0: v = v * 2^-8 + acc_l) for this warp's columns,
         // four levels per batch of TMEM loads; then the accumulator is handed back to the MMA
@@ -442,34 +616,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ptx::tc_fence_before();
         __syncwarp();
         if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[acc]));
-        if (row_ok) {
-          const int32_t ea = exa[gi];
-          double* Cd = (double*)Cb;
-#pragma unroll
-          for (int c = 0; c < CH; ++c)
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const long gj = n0 + c * 16 + j;
-              if (gj < n) {
-                // v * 2^E: one multiplication by the exact power of two when 2^E is a normal
-                // double (correctly rounded, so equal to scalbn), scalbn otherwise
-                const int eb = exb[gj];
-                const int E = ea + eb + prm.exp_shift;
-                double* cp = Cd + gi + gj * ldc;
-                if (E >= -1022 && E <= 1023) {
-                  const double w = v[c][j] * __longlong_as_double((long long)(E + 1023) << 52);
-                  const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
-                  *cp = fma(w, alpha_d, tb);
-                } else if (ea == kOzakiNonFiniteExp || eb == kOzakiNonFiniteExp) {
-                  // row i of op(A) or column j of op(B) holds an Inf or a NaN
-                  *cp = __longlong_as_double((long long)0x7FF8000000000000ull);
-                } else {
-                  const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
-                  *cp = fma(scalbn(v[c][j], E), alpha_d, tb);
-                }
-              }
-            }
-        }
+        if (row_ok) ozaki_store<CH>((double*)Cb, gi, n0, n, ldc, exa[gi], exb, prm.exp_shift, alpha_d, beta_d, v);
         continue;
       }
       // Groups of up to 64 columns: all TMEM loads, then all C loads (when beta != 0) are issued
@@ -485,27 +632,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ptx::tmem_wait_ld();
         if (!row_ok) continue;
         if (Cfg::EPI == EPI_I32) {
-          int32_t* Ci = (int32_t*)Cb + gi;
-          uint32_t cv[GC][16];
-          if (beta_i != 0) {
-#pragma unroll
-            for (int c = 0; c < GC; ++c)
-#pragma unroll
-              for (int j = 0; j < 16; ++j) {
-                const long gj = n0 + g0 + 16 * c + j;
-                cv[c][j] = (gj < n) ? (uint32_t)__ldcs(Ci + gj * ldc) : 0u;
-              }
-          }
-#pragma unroll
-          for (int c = 0; c < GC; ++c)
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const long gj = n0 + g0 + 16 * c + j;
-              if (gj < n) {
-                const uint32_t t = (beta_i == 0) ? 0u : (uint32_t)beta_i * cv[c][j];
-                __stcs(Ci + gj * ldc, (int32_t)(t + raw[c][j] * (uint32_t)alpha_i));
-              }
-            }
+          i32_store<GC>((int32_t*)Cb + gi, n0 + g0, n, ldc, alpha_i, beta_i, raw);
         } else {
           float* Cf = (float*)Cb + gi;
           float cv[GC][16];

@@ -59,9 +59,39 @@ bool make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, long K
   return r == CUDA_SUCCESS;
 }
 
+// Split-K plan of one GEMM launch: how many K pieces per output tile.
+struct SplitPlan {
+  int key = -1;          // ssblasSetKernelConfig key (SSBLAS_PATH_SPLITK_*), -1 = never split
+  long min_kb = 1;       // automatic choice: K blocks a piece keeps at least
+  long max_kb = 0;       // K blocks a piece may hold at most (0 = no bound)
+};
+
+// Number of K pieces: forced or tuned (config = pieces, 0 = automatic), else automatic -- only
+// when the tiles fill less than half of the SMs, up to one wave of (tile, piece) units, each
+// piece keeping at least min_kb K blocks. A forced count is cut to four waves of units. Never
+// below what max_kb requires, never above nk.
+int choose_splits(const SplitPlan& sp, long m, long n, long k, long batch, long tiles, long nk) {
+  if (sp.key < 0) return 1;
+  const long need = sp.max_kb > 0 ? (nk + sp.max_kb - 1) / sp.max_kb : 1;
+  long s = choose_config(sp.key, m, n, k, batch, 0);
+  if (s > 1 && s * tiles > 4L * num_sms()) s = (4L * num_sms()) / tiles > 1 ? (4L * num_sms()) / tiles : 1;
+  if (s == 0) {
+    s = 1;
+    if (2 * tiles <= num_sms()) {
+      s = num_sms() / tiles;
+      const long by_k = nk / (sp.min_kb > 0 ? sp.min_kb : 1);
+      if (s > by_k) s = by_k;
+      if (s > 32) s = 32;
+    }
+  }
+  if (s < need) s = need;
+  if (s > nk) s = nk;
+  return s < 1 ? 1 : (int)s;
+}
+
 template <class Cfg>
 cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params prm, cudaStream_t st,
-                     const char* name) {
+                     const char* name, const SplitPlan& plan = SplitPlan()) {
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
@@ -70,7 +100,32 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   }
   prm.tiles_m = (int)((prm.m + Cfg::BM - 1) / Cfg::BM);
   prm.tiles_n = (int)((prm.n + Cfg::BN - 1) / Cfg::BN);
-  prm.total_tiles = (long)prm.tiles_m * prm.tiles_n * prm.batch;
+  const long tiles = (long)prm.tiles_m * prm.tiles_n * prm.batch;
+  constexpr long KE = Cfg::KB / Cfg::ELEM;
+  const long nk = (prm.k + KE - 1) / KE;
+  prm.splits = 1;
+  prm.kb_per_split = (int)nk;
+  if (Cfg::EPI != tc::EPI_F32) {
+    const int want = choose_splits(plan, prm.m, prm.n, prm.k, prm.batch, tiles, nk);
+    if (want > 1) {
+      // pieces of equal K-block count; the last may be shorter, none is empty
+      const long kps = (nk + want - 1) / want;
+      const int splits = (int)((nk + kps - 1) / kps);
+      cudaError_t e;
+      const size_t unit = (size_t)Cfg::NLEV * Cfg::BN * Cfg::BM * sizeof(int32_t);
+      void* ws = workspace(WS_SPLIT, unit * (size_t)tiles * splits, &e);
+      if (!ws) return e;
+      void* cnt = workspace(WS_SPLIT_CNT, sizeof(int) * 8 * (size_t)tiles, &e);
+      if (!cnt) return e;
+      if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * 8 * (size_t)tiles, st)) != cudaSuccess) return e;
+      prm.splits = splits;
+      prm.kb_per_split = (int)kps;
+      prm.split_ws = (int32_t*)ws;
+      prm.split_cnt = (int*)cnt;
+    }
+  }
+  prm.total_tiles = tiles * prm.splits;
+  note_splits(prm.splits);
   long grid = prm.total_tiles < num_sms() ? prm.total_tiles : num_sms();
   ProfScope prof(name, st);
   tc::tc_gemm_kernel<Cfg, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
@@ -87,6 +142,7 @@ tc::Params base_params(const BatchDesc& d) {
   p.alpha_f = d.alpha_f; p.beta_f = d.beta_f;
   p.alpha_i = d.alpha_i; p.beta_i = d.beta_i;
   p.err = device_error_flag();
+  p.splits = 1;
   return p;
 }
 
@@ -125,9 +181,23 @@ template <> struct OzCfg<8> { using T = tc::Config<tc::KIND_I8, 8, 8, 64, 32, 4,
 using OzCfg7KB64 = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2>;
 using OzCfg7N32 = tc::Config<tc::KIND_I8, 7, 7, 32, 32, 6, 7, 2, tc::EPI_OZAKI, 2>;
 
+// Ozaki split-K: a piece holds at most 16384 k (its int32 level sums stay exact); automatic
+// pieces keep at least 512 k.
+constexpr long kOzakiMaxPieceK = 16384;
+template <class Cfg>
+SplitPlan ozaki_split_plan(bool allow_split) {
+  SplitPlan p;
+  if (!allow_split) return p;
+  constexpr long KE = Cfg::KB / Cfg::ELEM;
+  p.key = SSBLAS_PATH_SPLITK_OZAKI;
+  p.min_kb = 512 / KE;
+  p.max_kb = kOzakiMaxPieceK / KE;
+  return p;
+}
+
 template <class Cfg>
 cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
-                           long Kp, cudaStream_t st) {
+                           long Kp, bool allow_split, cudaStream_t st) {
   const long sa = d.m * Kp, sb = d.n * Kp;
   CUtensorMap ta, tb;
   if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, Cfg::KB, 128, S,
@@ -140,24 +210,24 @@ cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const in
   prm.exp_b = ex + d.m * d.batch;
   prm.exp_shift = -12;
   note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
-  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm");
+  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split));
 }
 
 cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex, long Kp,
-                       cudaStream_t st) {
+                       bool allow_split, cudaStream_t st) {
   switch (S) {
-    case 3: return ozaki_gemm_cfg<OzCfg<3>::T>(d, S, pa, pb, ex, Kp, st);
-    case 4: return ozaki_gemm_cfg<OzCfg<4>::T>(d, S, pa, pb, ex, Kp, st);
-    case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, ex, Kp, st);
-    case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, ex, Kp, st);
+    case 3: return ozaki_gemm_cfg<OzCfg<3>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+    case 4: return ozaki_gemm_cfg<OzCfg<4>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+    case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+    case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
     case 7: {
       // 64-byte K stages won every bucket the autotuner measured, so they are the default
       const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 1);
-      if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, ex, Kp, st);
-      if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, ex, Kp, st);
-      return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, ex, Kp, st);
+      if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, ex, Kp, allow_split, st);
+      if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, ex, Kp, allow_split, st);
+      return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
     }
-    default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, ex, Kp, st);
+    default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
   }
 }
 
@@ -209,13 +279,19 @@ cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t st) {
   if (!ok) return cudaErrorNotSupported;
   tc::Params prm = base_params(d);
   note_path(SSBLAS_PATH_I8_TCGEN05);
-  return BN == 128 ? run_gemm<CfgI8N128>(ta, tb, prm, st, "i8_gemm") : run_gemm<CfgI8N256>(ta, tb, prm, st, "i8_gemm");
+  // split-K: int32 sums wrap identically in any order; automatic pieces keep at least 2048 k
+  SplitPlan plan;
+  plan.key = SSBLAS_PATH_SPLITK_I8;
+  plan.min_kb = 2048 / 128;
+  return BN == 128 ? run_gemm<CfgI8N128>(ta, tb, prm, st, "i8_gemm", plan)
+                   : run_gemm<CfgI8N256>(ta, tb, prm, st, "i8_gemm", plan);
 }
 
 cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
-  // int32 accumulation stays exact while (pairs per level) * k * 2^14 < 2^31
-  if (d.k > 16384 || d.m > (1L << 31) || d.n > (1L << 31)) return cudaErrorNotSupported;
+  // int32 accumulation stays exact while (pairs per level) * k * 2^14 < 2^31: longer k is cut into
+  // split-K pieces of at most 16384, whose sums are added in 64 bits
+  if (d.k > (1L << 30) || d.m > (1L << 31) || d.n > (1L << 31)) return cudaErrorNotSupported;
   const int S = slices == 0 ? 7 : slices;
   if (S < 3 || S > 8) return cudaErrorInvalidValue;
   cudaError_t e;
@@ -232,14 +308,15 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   if (d.A0 && (d.batch == 1 || d.strideA > 0)) { a.X0 = d.A0; a.xstride = d.batch == 1 ? 16 : d.strideA; }
   if (d.B0 && (d.batch == 1 || d.strideB > 0)) { b.X0 = d.B0; b.xstride = d.batch == 1 ? 16 : d.strideB; }
   if ((e = launch_ozaki_slice_pair(a, ex, b, ex + d.m * d.batch, S, st)) != cudaSuccess) return e;
-  return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
+  return ozaki_gemm(d, S, pa, pb, ex, Kp, true, st);
 }
 
 cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
                                  long Kp, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (S < 3 || S > 8) return cudaErrorInvalidValue;
-  return ozaki_gemm(d, S, pa, pb, ex, Kp, st);
+  if (d.k > kOzakiMaxPieceK) return cudaErrorNotSupported;   // splitting would need workspace
+  return ozaki_gemm(d, S, pa, pb, ex, Kp, false, st);
 }
 
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {

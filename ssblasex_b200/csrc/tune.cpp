@@ -22,7 +22,8 @@ namespace {
 std::mutex g_tune_mutex;
 bool g_loaded = false;
 std::map<std::pair<int, std::string>, int> g_table;
-int g_forced[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+constexpr int kKeys = 16;
+int g_forced[kKeys] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
 
 int clog2(long x) {
   int r = 0;
@@ -68,7 +69,7 @@ std::string size_bucket(long m, long n, long k, long batch) {
 
 int choose_config(int path, long m, long n, long k, long batch, int fallback) {
   std::lock_guard<std::mutex> lock(g_tune_mutex);
-  if (path >= 0 && path < 8 && g_forced[path] >= 0) return g_forced[path];
+  if (path >= 0 && path < kKeys && g_forced[path] >= 0) return g_forced[path];
   if (!g_loaded) load_table();
   auto it = g_table.find({path, size_bucket(m, n, k, batch)});
   return it != g_table.end() ? it->second : fallback;
@@ -77,7 +78,7 @@ int choose_config(int path, long m, long n, long k, long batch, int fallback) {
 }  // namespace ssb
 
 extern "C" ssblasStatus_t ssblasSetKernelConfig(int path, int config) {
-  if (path < 0 || path >= 8 || config < -1 || config > 15) return SSBLAS_STATUS_INVALID_VALUE;
+  if (path < 0 || path >= ssb::kKeys || config < -1 || config > 64) return SSBLAS_STATUS_INVALID_VALUE;
   std::lock_guard<std::mutex> lock(ssb::g_tune_mutex);
   ssb::g_forced[path] = config;
   return SSBLAS_STATUS_SUCCESS;

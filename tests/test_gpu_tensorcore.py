@@ -102,18 +102,21 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
-@pytest.mark.parametrize("form", [2, 3, 4])
+@pytest.mark.parametrize("form", [1, 2, 3, 4])
 @pytest.mark.parametrize("ta,tb,m,n,k,batch", [
     (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 (4) CTAs, K contiguous, 16-byte loads
     (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2 (1), odd ld (8-byte loads)
     (0, 1, 300, 33, 1030, 2),     # single pass, rows contiguous, ragged last row block
-    (0, 1, 64, 48, 2500, 2),      # K > 2048 with few rows: one-kernel slicer
-    (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows: exponent pass, then digit chunks
+    (0, 1, 64, 48, 2500, 2),      # K > 2048 with few rows: K-parallel row maxima, digit chunks
+    (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows
+    (1, 1, 40, 200, 9000, 1),     # K > 2048, several row-maximum parts per row, ragged last part
 ])
 def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
-    """Every slicing kernel (and both item shapes of the one-pass kernel: form 2 = 32 rows x 256 k
-    per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k) produces the planes the CPU restatement produces: the product
-    is bit-exact against oracle.ozaki_f64 whichever kernel sliced the operands."""
+    """Every slicing kernel (the two-pass form 1 -- row maxima per (32 rows, 256 k) part, then
+    digits per (32 rows, 128 k) chunk -- and the one-pass item shapes: form 2 = 32 rows x 256 k
+    per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k) produces the planes the CPU restatement
+    produces: the product is bit-exact against oracle.ozaki_f64 whichever kernel sliced the
+    operands."""
     from ssblasex_b200 import workloads as W
     if k > 2048 and form in (2, 4):
         pytest.skip("the one-pass forms apply to k <= 2048")
@@ -307,3 +310,90 @@ def test_ozaki_nonfinite_inputs(S, ta, tb, k):
         want_nan[bad_rows[b], :] = True
         want_nan[:, bad_cols[b]] = True
         np.testing.assert_array_equal(np.isnan(got), want_nan)
+
+
+# ------------------------------------------------------------------------- split-K ---------
+def pieces(k, k_block, want):
+    """K pieces the library makes of `want`: equal K-block counts, none empty."""
+    nk = -(-k // k_block)
+    per = -(-nk // min(want, nk))
+    return -(-nk // per)
+
+
+@pytest.mark.parametrize("splits", [0, 1, 2, 3, 7, 16])
+@pytest.mark.parametrize("ta,tb,m,n,k,batch,alpha,beta", [
+    (1, 0, 200, 300, 5000, 2, 2, -1),    # direct TMA path (op(A) = T, op(B) = N), ragged tiles
+    (0, 0, 70, 90, 3000, 3, -3, 2),      # pack pre-pass, one tile per instance
+])
+def test_split_k_i8(S, splits, ta, tb, m, n, k, batch, alpha, beta):
+    """int8 split-K: every K-piece count (0 = automatic) gives the unsplit result bit for bit --
+    the pieces' int32 sums wrap the same way in any order."""
+    from ssblasex_b200 import workloads as W
+    lda = -(-k // 16) * 16 if ta == 1 else m
+    ldb = -(-k // 16) * 16 if tb == 0 else n
+    p = W.make_problem("i8", ta, tb, m, n, k, batch, alpha, beta, lda=lda, ldb=ldb, seed=k + splits)
+    S.set_kernel_config("splitk_i8", splits)
+    try:
+        C = run(p)
+        info = S.last_run_info()
+    finally:
+        S.set_kernel_config("splitk_i8", -1)
+    assert info["path"] == "i8_tcgen05"
+    if splits > 1:
+        assert info["split_k"] == pieces(k, 128, splits)
+    np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+
+
+@pytest.mark.parametrize("splits", [0, 1, 2, 5, 9])
+@pytest.mark.parametrize("ta,tb", [(0, 1), (1, 0)])
+def test_split_k_ozaki(S, splits, ta, tb):
+    """Ozaki split-K: the level sums of the pieces are added exactly, so the result is bit-exact
+    against the CPU restatement whatever the piece count."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", ta, tb, 130, 70, 4100, 2, 0.75, -0.5, seed=splits + 3 * ta, dist="expspread")
+    S.set_kernel_config("splitk_ozaki", splits)
+    try:
+        C = run(p)
+        info = S.last_run_info()
+    finally:
+        S.set_kernel_config("splitk_ozaki", -1)
+    assert info["path"] == "ozaki_tcgen05"
+    if splits > 1:
+        assert info["split_k"] == pieces(p.k, 64, splits)
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+
+
+def test_ozaki_long_k_is_split(S):
+    """k > 16384 stays on the Ozaki path: the GEMM is cut into K pieces of at most 16384, each
+    exact in int32, added in 64 bits."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", 1, 0, 40, 33, 40000, 2, 1.0, 0.25, seed=5, dist="expspread")
+    C = run(p)
+    info = S.last_run_info()
+    assert info["path"] == "ozaki_tcgen05" and info["split_k"] >= 3
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+    assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
+
+
+def test_ozaki_level_sum_beyond_int32(S):
+    """Constant operands make every product of leading digits equal, so the leading level's sum
+    over k = 600000 exceeds the int32 range (the CPU restatement reports that with status -1);
+    the split pieces are added in 64 bits and the result is still bit-exact."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", 1, 0, 3, 2, 600000, 1, 1.0, 0.0, seed=1)
+    for b in range(p.batch):
+        p.op_a(b)[:] = 0.99
+        p.op_b(b)[:] = -0.97
+    C = run(p)
+    assert S.last_run_info()["path"] == "ozaki_tcgen05"
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == -1
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+    np.testing.assert_allclose(p.c_view(C, 0), 600000 * 0.99 * -0.97, rtol=1e-12)

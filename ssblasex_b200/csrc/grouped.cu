@@ -68,10 +68,16 @@ constexpr int GNT = 256;
 // (conflict-free word stores) and leave as 16-byte vectors into the pre-swizzled tile layout the
 // grouped GEMM stages with bulk copies: for each (row tile, K block) of the instance, P planes of
 // [RTILE rows][KB bytes], 16-byte chunks permuted by the hardware swizzle of a KB-byte span.
+template <int MODE> struct GElem;
+template <> struct GElem<0> { using T = int8_t; };
+template <> struct GElem<1> { using T = float; };
+template <> struct GElem<2> { using T = double; };
+
 template <int MODE, int S, int KB, int RTILE_A, int RTILE_B>
-__global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
+__global__ void __launch_bounds__(GNT, MODE == 2 ? 4 : MODE == 0 ? 6 : 8) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
                                                     uint8_t* __restrict__ outA, uint8_t* __restrict__ outB,
                                                     int32_t* __restrict__ exps) {
+  using T = typename GElem<MODE>::T;
   constexpr int P = MODE == 0 ? 1 : MODE == 1 ? 2 : S;
   constexpr int OB = MODE == 1 ? 2 : 1;                     // output bytes per element and plane
   constexpr int KE = KB / OB;                               // K elements per block
@@ -80,8 +86,12 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
   constexpr int RPR = KC / 4;                               // runs of 4 k per row and chunk
   constexpr int PER = GRT * RPR / GNT;                      // runs per thread and chunk
   constexpr int PB = KB + 4;                                // staged row pitch (bytes)
-  static_assert(NKB >= 1 && PER >= 1 && RPR >= 8, "chunk shape");
-  __shared__ __align__(16) uint8_t stage[NKB * P * GRT * PB];
+  constexpr int CPR = KB / 16;                              // 16-byte chunks per staged row
+  constexpr int CHT = GRT * CPR;                            // 16-byte chunks per (K block, plane)
+  constexpr int BPP = GNT / CHT;                            // (K block, plane) pairs per write pass
+  constexpr int NBP = NKB * P;                              // (K block, plane) pairs per chunk
+  static_assert(NKB >= 1 && PER >= 1 && RPR >= 8 && RPR <= 32 && GNT % RPR == 0 && GNT % CHT == 0, "chunk shape");
+  __shared__ __align__(16) uint8_t stage[NBP * GRT * PB];
   __shared__ double red[8][GRT];
   __shared__ double rscale[GRT][2];
 
@@ -90,54 +100,87 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
   const bool is_b = (wk.x & 1) != 0;
   const int RTILE = is_b ? RTILE_B : RTILE_A;
   uint8_t* out = (is_b ? outB : outA) + it.off;
-  const uint8_t* X = (const uint8_t*)it.X[it.idx];
+  const T* X = (const T*)it.X[it.idx];
   const long gr0 = (long)wk.y * GRT;                        // first row (of the padded range)
   const int rt = (int)(gr0 / RTILE), rr0 = (int)(gr0 % RTILE);
-  const long kpad = (long)it.nk * KE;
+  const long K = it.K, ld = it.ld;
+  const bool kc = it.kcontig != 0;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
 
-  // (row, first k) of this thread's q-th run in a chunk
-  auto run_of = [&](int q, int& r, int& kl) {
-    if (it.kcontig) {
-      const int idx = t + q * GNT;
-      r = idx / RPR;
-      kl = 4 * (idx % RPR);
+  // This thread's runs: row r[q] of the item and first k kq[q] within a chunk. K contiguous: the
+  // RPR threads of a row are consecutive lanes; rows contiguous: lane = row (coalesced loads).
+  // Element (r, k) is at pq[q][(k - kq[q]) * estep]; rows past the matrix are never read.
+  int rq[PER], kq[PER];
+  const T* pq[PER];
+  bool rv[PER];
+  const long estep = kc ? 1 : ld;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    rq[q] = kc ? t / RPR + q * (GNT / RPR) : lane;
+    kq[q] = kc ? 4 * (t % RPR) : 4 * (warp + 8 * q);
+    const long gr = gr0 + rq[q];
+    rv[q] = gr < it.rows;
+    pq[q] = rv[q] ? X + (kc ? gr * ld + kq[q] : gr + kq[q] * ld) : X;
+  }
+  // 4 consecutive k of a row in one vector load when the row starts are aligned for it
+  const bool vec = kc && ((uintptr_t)X % (sizeof(T) == 1 ? 4 : 16)) == 0 && ld % (sizeof(T) == 8 ? 2 : 4) == 0;
+  auto load4 = [&](int q, long k0, T (&x)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x[i] = T(0);
+    if (!rv[q]) return;
+    const T* p = pq[q] + k0 * estep;
+    const long kk = k0 + kq[q];
+    if (kk + 4 <= K) {
+      if (vec) {
+        if constexpr (sizeof(T) == 8) {
+          const double2 a = __ldg((const double2*)p), b = __ldg((const double2*)p + 1);
+          x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+        } else if constexpr (sizeof(T) == 4) {
+          const float4 a = __ldg((const float4*)p);
+          x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        } else {
+          const char4 a = __ldg((const char4*)p);
+          x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = __ldg(p + i * estep);
+      }
     } else {
-      r = lane;
-      kl = 4 * (warp + 8 * q);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (kk + i < K) x[i] = __ldg(p + i * estep);
     }
-  };
-  auto load = [&](long gr, long k) -> double {
-    if (gr >= it.rows || k >= it.K) return 0.0;
-    const long off = it.kcontig ? gr * it.ld + k : gr + k * it.ld;
-    if (MODE == 0) return (double)((const int8_t*)X)[off];
-    if (MODE == 1) return (double)((const float*)X)[off];
-    return ((const double*)X)[off];
   };
 
-  if (MODE == 2) {
-    // row maxima over all of K (bit patterns of |x|, stored in the double buffers bit for bit)
+  // Ozaki: row maxima over all of K (bit patterns of |x|, stored in the double buffers bit for
+  // bit); the first chunk's values stay in registers for the digits
+  T v0[PER][4];
+  if constexpr (MODE == 2) {
     unsigned long long mx[PER];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) mx[q] = 0;
-    for (long k0 = 0; k0 < it.K; k0 += KC) {
+    for (int q = 0; q < PER; ++q) {
+      load4(q, 0, v0[q]);
+      mx[q] = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(v0[q][i]));
+    }
+    for (long k0 = KC; k0 < K; k0 += KC) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
-        int r, kl;
-        run_of(q, r, kl);
+        T x[4];
+        load4(q, k0, x);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(load(gr0 + r, k0 + kl + i)));
+        for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(x[i]));
       }
     }
-    if (it.kcontig) {
+    if (kc) {
       // the RPR threads of a row are consecutive lanes
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
 #pragma unroll
-        for (int off = 1; off < RPR && off < 32; off <<= 1) mx[q] = max_u64(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
-        int r, kl;
-        run_of(q, r, kl);
-        if (kl == 0) red[0][r] = __longlong_as_double((long long)mx[q]);
+        for (int off = 1; off < RPR; off <<= 1) mx[q] = max_u64(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], off));
+        if (kq[q] == 0) red[0][rq[q]] = __longlong_as_double((long long)mx[q]);
       }
     } else {
       unsigned long long m = mx[0];
@@ -148,7 +191,7 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
     __syncthreads();
     if (t < GRT) {
       unsigned long long m2 = (unsigned long long)__double_as_longlong(red[0][t]);
-      if (!it.kcontig)
+      if (!kc)
         for (int w = 1; w < 8; ++w) m2 = max_u64(m2, (unsigned long long)__double_as_longlong(red[w][t]));
       const int e = row_exponent(m2);
       if (gr0 + t < it.rows) exps[it.eoff + gr0 + t] = e;
@@ -157,29 +200,39 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
     __syncthreads();
   }
 
-  for (long k0 = 0; k0 < kpad; k0 += KC) {
-    // convert PER runs per thread into the staging buffer
+  // write-out mapping: this thread's row and 16-byte chunk of a staged (K block, plane) block,
+  // and that chunk's place in the hardware-swizzled tile
+  const int wr = (t % CHT) / CPR, wc = t % CPR;
+  const bool wrow = gr0 + wr < it.rows;
+  const uint32_t soff = (uint32_t)(wr * PB + 16 * wc);
+  const uint32_t doff = swz(rr0 + wr, 16 * wc, KB);
+  const long tile_bytes = (long)P * RTILE * KB;             // one (row tile, K block) chunk, all planes
+
+  // K blocks at or past K are padding, zero since the plan was created: chunks start below K
+  for (long k0 = 0; k0 < K; k0 += KC) {
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-      int r, kl;
-      run_of(q, r, kl);
-      double x[4];
+      T x[4];
+      if (MODE == 2 && k0 == 0) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) x[i] = load(gr0 + r, k0 + kl + i);
+        for (int i = 0; i < 4; ++i) x[i] = v0[q][i];
+      } else {
+        load4(q, k0, x);
+      }
+      const int r = rq[q], kl = kq[q];
       const int kb = kl / KE, cbyte = (kl % KE) * OB;
       uint8_t* row = stage + (kb * P) * GRT * PB + r * PB + cbyte;
-      if (MODE == 0) {
+      if constexpr (MODE == 0) {
         uint32_t w = 0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) w |= ((uint32_t)(uint8_t)(int8_t)x[i]) << (8 * i);
+        for (int i = 0; i < 4; ++i) w |= ((uint32_t)(uint8_t)x[i]) << (8 * i);
         *(uint32_t*)row = w;
-      } else if (MODE == 1) {
+      } else if constexpr (MODE == 1) {
         __nv_bfloat16 h[4], l[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const float f = (float)x[i];
-          h[i] = __float2bfloat16_rn(f);
-          l[i] = __float2bfloat16_rn(f - __bfloat162float(h[i]));
+          h[i] = __float2bfloat16_rn(x[i]);
+          l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
         }
         __nv_bfloat162 h01, h23, l01, l23;
         h01.x = h[0]; h01.y = h[1]; h23.x = h[2]; h23.y = h[3];
@@ -189,29 +242,28 @@ __global__ void __launch_bounds__(GNT, 8) gprep_kernel(const GPrepInst* __restri
         *(__nv_bfloat162*)(row + GRT * PB) = l01;
         *(__nv_bfloat162*)(row + GRT * PB + 4) = l23;
       } else {
-        // rows beyond the matrix are zero digits (a zero value gives Y = bias), and so are rows
-        // holding an Inf or a NaN (zero scale)
-        if (rscale[r][0] == 0.0) x[0] = x[1] = x[2] = x[3] = 0.0;
+        // rows beyond the matrix are never written out; rows holding an Inf or a NaN (zero
+        // scale) have zero digits
+        double xd[4] = {x[0], x[1], x[2], x[3]};
+        if (rscale[r][0] == 0.0) xd[0] = xd[1] = xd[2] = xd[3] = 0.0;
         uint32_t wd[S];
-        digit_words<S>(x, rscale[r][0], rscale[r][1], wd);
+        digit_words<S>(xd, rscale[r][0], rscale[r][1], wd);
 #pragma unroll
         for (int p = 0; p < P; ++p) *(uint32_t*)(row + p * GRT * PB) = wd[p];
       }
     }
     __syncthreads();
     // write-out: per (K block, plane), 32 rows x KB bytes of the tile, 16-byte chunks swizzled
-    constexpr int CPR = KB / 16;                       // 16-byte chunks per row
-    constexpr int NCH = NKB * P * GRT * CPR;
-    for (int ch = t; ch < NCH; ch += GNT) {
-      const int c = ch % CPR, r = (ch / CPR) % GRT, bp = ch / (CPR * GRT);
-      const int kb = bp / P, pl = bp % P;
-      const long kbg = k0 / KE + kb;
-      // K blocks past K and rows past the matrix are padding, zero since the plan was created
-      if (kbg >= it.nk || kbg * KE >= it.K || gr0 + r >= it.rows) continue;
-      const uint32_t* src = (const uint32_t*)(stage + bp * GRT * PB + r * PB + 16 * c);
-      const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
-      uint8_t* chunk = out + ((long)rt * it.nk + kbg) * (long)P * RTILE * KB + (long)pl * RTILE * KB;
-      *(uint4*)(chunk + swz(rr0 + r, 16 * c, KB)) = w;
+    if (wrow) {
+#pragma unroll
+      for (int bp = t / CHT; bp < NBP; bp += BPP) {
+        const int kb = bp / P, pl = bp - kb * P;
+        const long kbg = k0 / KE + kb;
+        if (kbg * KE >= K) continue;
+        const uint32_t* src = (const uint32_t*)(stage + bp * GRT * PB + soff);
+        const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+        *(uint4*)(out + ((long)rt * it.nk + kbg) * tile_bytes + (long)pl * RTILE * KB + doff) = w;
+      }
     }
     __syncthreads();
   }
@@ -236,13 +288,27 @@ void plan_kind(const GroupedDesc& g, const std::vector<int>& members, KindPlan<C
     gi.m = in.m; gi.n = in.n; gi.k = in.k; gi.ldc = in.ldc; gi.idx = in.idx;
     gi.alpha_d = in.alpha_d; gi.beta_d = in.beta_d; gi.alpha_f = in.alpha_f; gi.beta_f = in.beta_f;
     gi.alpha_i = in.alpha_i; gi.beta_i = in.beta_i;
-    const int tm = (int)((in.m + Cfg::BM - 1) / Cfg::BM), tn = (int)((in.n + Cfg::BN - 1) / Cfg::BN);
+    // Ozaki tiles are BM = 128 rows by BN (< BM) columns: when the transposed product C^T =
+    // op(B)^T op(A)^T wastes less of its tiles (n on the 128-row side, m on the narrow side), the
+    // instance is computed that way -- its rows are then n, its columns m, and the epilogue writes
+    // element (i, j) of C^T to C(j, i). (The FP32 and int32 kinds keep the direct orientation: their
+    // tiles hold less work per output element, and the transposed stores cost them more than the
+    // padding they save.)
+    auto padded = [&](long rows, long cols) {
+      return ((rows + Cfg::BM - 1) / Cfg::BM) * Cfg::BM * (((cols + Cfg::BN - 1) / Cfg::BN) * Cfg::BN);
+    };
+    const bool swap = Cfg::EPI == tc::EPI_OZAKI && padded(in.n, in.m) < padded(in.m, in.n);
+    const long rows = swap ? in.n : in.m, cols = swap ? in.m : in.n;
+    gi.m = rows;
+    gi.n = cols;
+    gi.swap = swap ? 1 : 0;
+    const int tm = (int)((rows + Cfg::BM - 1) / Cfg::BM), tn = (int)((cols + Cfg::BN - 1) / Cfg::BN);
     gi.nk = (int)((in.k + KE - 1) / KE);
     gi.tiles_n = tn;
     gi.offA = kp.bytesA;
     gi.offB = kp.bytesB;
     gi.offEA = kp.nexp;
-    gi.offEB = kp.nexp + in.m;
+    gi.offEB = kp.nexp + rows;
     kp.bytesA += (long)tm * gi.nk * Cfg::A_STAGE;
     kp.bytesB += (long)tn * gi.nk * Cfg::B_STAGE;
     kp.nexp += in.m + in.n;
@@ -250,13 +316,17 @@ void plan_kind(const GroupedDesc& g, const std::vector<int>& members, KindPlan<C
     kp.inst.push_back(gi);
     for (int a = 0; a < tm; ++a)
       for (int b = 0; b < tn; ++b) kp.tiles.push_back(GTile{li, a, b});
-    GPrepInst pa{g.A, in.idx, in.m, in.k, in.lda, in.transa == SSBLAS_OP_T, tm, gi.nk, gi.offA, gi.offEA};
-    GPrepInst pb{(const void* const*)g.B, in.idx, in.n, in.k, in.ldb, in.transb == SSBLAS_OP_N, tn, gi.nk, gi.offB, gi.offEB};
+    // op(A) as rows x K (K contiguous when A is transposed), op(B)^T likewise
+    const GPrepInst opa{g.A, in.idx, in.m, in.k, in.lda, in.transa == SSBLAS_OP_T, 0, gi.nk, 0, 0};
+    const GPrepInst opb{(const void* const*)g.B, in.idx, in.n, in.k, in.ldb, in.transb == SSBLAS_OP_N, 0, gi.nk, 0, 0};
+    GPrepInst pa = swap ? opb : opa, pb = swap ? opa : opb;   // tile rows, tile columns
+    pa.tiles = tm; pa.off = gi.offA; pa.eoff = gi.offEA;
+    pb.tiles = tn; pb.off = gi.offB; pb.eoff = gi.offEB;
     // only row blocks that hold rows of the matrix: the padding of the tiles is zeroed once, when
     // the plan's buffers are created, and no call writes it again
-    for (long rb = 0; rb < (in.m + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
+    for (long rb = 0; rb < (pa.rows + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pa);
-    for (long rb = 0; rb < (in.n + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
+    for (long rb = 0; rb < (pb.rows + GRT - 1) / GRT; ++rb) kp.work.push_back(make_uint2((unsigned)kp.prep.size(), (unsigned)rb));
     kp.prep.push_back(pb);
   }
   // longest K first: the persistent CTAs then finish close together

@@ -50,6 +50,9 @@ struct GInst {
   long offEA, offEB;        // element offsets of its Ozaki exponents
   int nk;                   // K blocks (stages) per tile
   int tiles_n;
+  int swap;                 // 1: the tiles compute C^T = op(B)^T op(A)^T (m and n, the exponents and
+                            // the operand packs are those of the transposed product)
+  int pad_;
   double alpha_d, beta_d;
   float alpha_f, beta_f;
   int32_t alpha_i, beta_i;
@@ -95,18 +98,20 @@ struct Params {
 };
 
 // Grouped launches take tiles from a device-side queue: a scheduler warp (warp 10) of each CTA
-// claims the next tile with an atomic increment of prm.queue, decodes its instance record once,
-// and passes it to the TMA, MMA and epilogue warps through a ring of kTQ shared-memory slots
+// claims kSB tiles at a time with one atomic add to prm.queue, decodes their instance records
+// (lane j fills record j of the batch, so the batch costs one chain of dependent loads, not kSB),
+// and passes them to the TMA, MMA and epilogue warps through a ring of kTQ shared-memory slots
 // (tq_full: record written; tq_empty: the TMA warp, the MMA warp and the 8 epilogue warps are done
-// with it). The scheduler runs up to kTQ records ahead, so the claim and the record loads are off
+// with it). The scheduler runs up to kTQ records ahead, so the claims and the record loads are off
 // the other warps' paths. A record with valid == 0 ends the CTA's tile sequence.
-constexpr int kTQ = 8;
+constexpr int kTQ = 16;
+constexpr int kSB = kTQ / 2;
 struct TileDesc {
   GInst g;
   const void* cptr;         // the instance's C pointer
   int mt, nt, valid, pad;
 };
-constexpr int kTileQueueBytes = 2048;   // 2 x kTQ barriers + kTQ records
+constexpr int kTileQueueBytes = 4096;   // 2 x kTQ barriers + kTQ records
 
 struct TileInfo {
   int b, mt, nt;
@@ -164,11 +169,12 @@ struct Config {
 };
 
 // Ozaki epilogue of one thread's row gi: C(gi, j) = alpha * v_j * 2^(ea + eb_j + exp_shift) + beta * C
-// for the columns j = n0 + 16c + jj below n.
-template <int CH>
-__device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long ldc, int32_t ea,
+// for the columns j = n0 + 16c + jj below n; element (i, j) of C is at Cd[i * rs + j * cs]. The
+// column exponents come from exb, or (PRE) from registers loaded before the accumulator was ready.
+template <int CH, bool PRE = false>
+__device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long rs, long cs, int32_t ea,
                                             const int32_t* exb, int exp_shift, double alpha_d, double beta_d,
-                                            const double (&v)[CH][16]) {
+                                            const double (&v)[CH][16], const int32_t (*ebp)[16] = nullptr) {
 #pragma unroll
   for (int c = 0; c < CH; ++c)
 #pragma unroll
@@ -177,9 +183,9 @@ __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n
       if (gj < n) {
         // v * 2^E: one multiplication by the exact power of two when 2^E is a normal double
         // (correctly rounded, so equal to scalbn), scalbn otherwise
-        const int eb = exb[gj];
+        const int eb = PRE ? ebp[c][j] : exb[gj];
         const int E = ea + eb + exp_shift;
-        double* cp = Cd + gi + gj * ldc;
+        double* cp = Cd + gi * rs + gj * cs;
         if (E >= -1022 && E <= 1023) {
           const double w = v[c][j] * __longlong_as_double((long long)(E + 1023) << 52);
           const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
@@ -306,7 +312,7 @@ __device__ __noinline__ void split_k_region(uint32_t t_row, int32_t* split_ws, i
 #pragma unroll
         for (int j = 0; j < 16; ++j) v[0][j] = v[0][j] * 0x1p-8 + (double)sum[j];
       }
-      if (row_ok) ozaki_store<1>((double*)Cb, gi, n0 + c * 16, n, ldc, ea, exb, exp_shift, alpha_d, beta_d, v);
+      if (row_ok) ozaki_store<1>((double*)Cb, gi, n0 + c * 16, n, 1, ldc, ea, exb, exp_shift, alpha_d, beta_d, v);
     } else {
       long long sum[16];
 #pragma unroll
@@ -320,7 +326,9 @@ __device__ __noinline__ void split_k_region(uint32_t t_row, int32_t* split_ws, i
   }
 }
 
-template <class Cfg, bool GROUPED>
+// SPLIT: the split-K form (batched launches with prm.splits > 1); a separate instantiation, so the
+// unsplit kernels carry no trace of the split epilogue.
+template <class Cfg, bool GROUPED, bool SPLIT = false>
 __global__ void __launch_bounds__(threads_of<GROUPED>(), 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
   extern __shared__ uint8_t smem_raw[];
@@ -505,27 +513,34 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   } else if (GROUPED && warp == 10) {
     // ------------------------------------------------------------------ scheduler ---------
     if constexpr (GROUPED) {
-      if (lane == 0) {
-        for (long i = 0;; ++i) {
-          const int slot = (int)(i % kTQ);
-          const bool ok = ptx::mbar_wait(ptx::smem_u32(&tq_empty[slot]), (uint32_t)(((i / kTQ) & 1) ^ 1), err, 14);
+      // batches of kSB records: lane j < kSB fills record i + j (slot (i + j) % kTQ)
+      for (long i = 0;; i += kSB) {
+        const long rec = i + lane;
+        const int slot = (int)(rec % kTQ);
+        bool ok = true;
+        if (lane < kSB) ok = ptx::mbar_wait(ptx::smem_u32(&tq_empty[slot]), (uint32_t)(((rec / kTQ) & 1) ^ 1), err, 14);
+        // dynamic order: kSB consecutive tiles per claim; static order: the CTA's stride
+        unsigned long long base = 0;
+        if (prm.queue && lane == 0) base = atomicAdd(prm.queue, (unsigned long long)kSB);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const long q = !ok ? prm.total_tiles
+                           : prm.queue ? (long)base + lane : (long)blockIdx.x + rec * (long)gridDim.x;
+        const bool last = __any_sync(0xffffffffu, lane < kSB && q >= prm.total_tiles);
+        if (lane < kSB) {
           TileDesc& d = tq[slot];
-          // dynamic order from the queue counter, or (without a counter) the static stride
-          const long q = !ok ? prm.total_tiles
-                             : prm.queue ? (long)atomicAdd(prm.queue, 1ull) : (long)blockIdx.x + i * (long)gridDim.x;
           if (q >= prm.total_tiles) {
             d.valid = 0;
-            ptx::mbar_arrive(ptx::smem_u32(&tq_full[slot]));
-            break;
+          } else {
+            const GTile gt = prm.gtiles[q];
+            d.g = prm.ginst[gt.inst];
+            d.cptr = prm.C[d.g.idx];
+            d.mt = gt.mt;
+            d.nt = gt.nt;
+            d.valid = 1;
           }
-          const GTile gt = prm.gtiles[q];
-          d.g = prm.ginst[gt.inst];
-          d.cptr = prm.C[d.g.idx];
-          d.mt = gt.mt;
-          d.nt = gt.nt;
-          d.valid = 1;
           ptx::mbar_arrive(ptx::smem_u32(&tq_full[slot]));
         }
+        if (last) break;
       }
     }
   } else {
@@ -550,6 +565,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ti = tile_info(prm, t, tiles_mn, nk_uniform);
       }
       long m = prm.m, n = prm.n, ldc = prm.ldc;
+      long rs = 1;   // C(i, j) at C[i * rs + j * cs]
       double alpha_d = prm.alpha_d, beta_d = prm.beta_d;
       float alpha_f = prm.alpha_f, beta_f = prm.beta_f;
       int32_t alpha_i = prm.alpha_i, beta_i = prm.beta_i;
@@ -563,12 +579,24 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         alpha_i = g.alpha_i; beta_i = g.beta_i;
         exa = prm.exp_a + g.offEA;
         exb = prm.exp_a + g.offEB;
+        if (g.swap) { rs = ldc; ldc = 1; }
         Cb = (uint8_t*)tq[slot].cptr;
         // the record is copied: release the slot
         __syncwarp();
         if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tq_empty[slot]));
       } else {
         Cb = (uint8_t*)prm.C[ti.b + prm.c_batch_offset];
+      }
+      // grouped Ozaki tiles are short: the exponents of a 16-column region are loaded while the
+      // MMAs still run
+      constexpr bool PRE = GROUPED && Cfg::EPI == EPI_OZAKI && HALF == 16;
+      int32_t pre_ea = 0;
+      int32_t pre_eb[1][16];
+      if constexpr (PRE) {
+        const long pi = (long)ti.mt * Cfg::BM + row_in_tile, pn0 = (long)ti.nt * Cfg::BN + half * HALF;
+        if (pi < m) pre_ea = exa[pi];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) pre_eb[0][j] = pn0 + j < n ? exb[pn0 + j] : 0;
       }
       const int acc = tcount % Cfg::ACCB;
       const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
@@ -579,8 +607,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) +
                              (uint32_t)(acc * Cfg::NLEV * Cfg::BN + half * HALF);
       const bool row_ok = gi < m;
-      if constexpr (!GROUPED && Cfg::EPI != EPI_F32) {
-        if (prm.splits > 1) {
+      if constexpr (SPLIT && !GROUPED && Cfg::EPI != EPI_F32) {
+        {
           split_k_region<Cfg, HALF>(t_row, prm.split_ws, prm.split_cnt, t / prm.splits, prm.splits, ti.sp, half,
                                     warp - 2, row_in_tile, lane, ptx::smem_u32(&tempty[acc]), row_ok, Cb, gi, n0, n,
                                     ldc, (Cfg::EPI == EPI_OZAKI && row_ok) ? exa[gi] : 0, exb, prm.exp_shift, alpha_d, beta_d,
@@ -616,7 +644,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ptx::tc_fence_before();
         __syncwarp();
         if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[acc]));
-        if (row_ok) ozaki_store<CH>((double*)Cb, gi, n0, n, ldc, exa[gi], exb, prm.exp_shift, alpha_d, beta_d, v);
+        if constexpr (PRE) {
+          if (row_ok) ozaki_store<1, true>((double*)Cb, gi, n0, n, rs, ldc, pre_ea, exb, prm.exp_shift, alpha_d, beta_d, v, pre_eb);
+        } else {
+          if (row_ok) ozaki_store<CH>((double*)Cb, gi, n0, n, rs, ldc, exa[gi], exb, prm.exp_shift, alpha_d, beta_d, v);
+        }
         continue;
       }
       // Groups of up to 64 columns: all TMEM loads, then all C loads (when beta != 0) are issued
@@ -632,9 +664,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ptx::tmem_wait_ld();
         if (!row_ok) continue;
         if (Cfg::EPI == EPI_I32) {
-          i32_store<GC>((int32_t*)Cb + gi, n0 + g0, n, ldc, alpha_i, beta_i, raw);
+          i32_store<GC>((int32_t*)Cb + gi * rs, n0 + g0, n, ldc, alpha_i, beta_i, raw);
         } else {
-          float* Cf = (float*)Cb + gi;
+          float* Cf = (float*)Cb + gi * rs;
           float cv[GC][16];
           if (beta_f != 0.0f) {
 #pragma unroll

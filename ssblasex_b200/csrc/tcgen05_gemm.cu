@@ -94,7 +94,12 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
                      const char* name, const SplitPlan& plan = SplitPlan()) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, false, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    if constexpr (Cfg::EPI != tc::EPI_F32)
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg::SMEM);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
@@ -128,7 +133,12 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   note_splits(prm.splits);
   long grid = prm.total_tiles < num_sms() ? prm.total_tiles : num_sms();
   ProfScope prof(name, st);
-  tc::tc_gemm_kernel<Cfg, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
+  if (prm.splits > 1) {
+    if constexpr (Cfg::EPI != tc::EPI_F32)
+      tc::tc_gemm_kernel<Cfg, false, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
+  } else {
+    tc::tc_gemm_kernel<Cfg, false, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
+  }
   note_launch();
   return cudaGetLastError();
 }

@@ -148,3 +148,34 @@ def test_grouped_ozaki_nonfinite_inputs():
         assert not np.isnan(probs[3].c_view(res[3], 0)).any()
     finally:
         S.set_math_mode(0)
+
+
+@pytest.mark.parametrize("mode", [0, 3])
+def test_grouped_transposed_orientation(mode):
+    """Ozaki instances whose transposed product fills the 128-row tiles better (m small, n large)
+    are computed as C^T = op(B)^T op(A)^T and written back transposed; the other kinds keep the
+    direct orientation. Every kind, every op(A)/op(B) combination, beta != 0 and C with a padded
+    leading dimension."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    S.set_math_mode(mode)
+    try:
+        probs, seed = [], 300
+        for row in ("f64", "f32", "i8"):
+            al, be = (2, -1) if row == "i8" else (0.75, 0.5)
+            for ta in (0, 1):
+                for tb in (0, 1):
+                    for m, n, k in ((20, 300, 70), (300, 20, 70), (5, 129, 33), (129, 5, 33), (1, 200, 9)):
+                        seed += 1
+                        probs.append(W.make_problem(row, ta, tb, m, n, k, 1, al, be, ldc=m + 3, seed=seed,
+                                                    dist="expspread" if row == "f64" else "uniform"))
+        gd = runner.GroupedDevice(probs)
+        for rep in range(3):
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            for p, C in zip(probs, gd.results()):
+                _check(p, C, mode)
+                # the padding rows of C (m <= i < ldc) are untouched
+                np.testing.assert_array_equal(C.reshape(p.n, p.ldc)[:, p.m:], p.C.reshape(p.n, p.ldc)[:, p.m:])
+    finally:
+        S.set_math_mode(0)

@@ -74,7 +74,7 @@ template <> struct GElem<1> { using T = float; };
 template <> struct GElem<2> { using T = double; };
 
 template <int MODE, int S, int KB, int RTILE_A, int RTILE_B>
-__global__ void __launch_bounds__(GNT, MODE == 2 ? 4 : MODE == 0 ? 6 : 8) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
+__global__ void __launch_bounds__(GNT, MODE == 2 ? 6 : MODE == 0 ? 6 : 8) gprep_kernel(const GPrepInst* __restrict__ items, const uint2* __restrict__ work,
                                                     uint8_t* __restrict__ outA, uint8_t* __restrict__ outB,
                                                     int32_t* __restrict__ exps) {
   using T = typename GElem<MODE>::T;
@@ -154,18 +154,12 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 4 : MODE == 0 ? 6 : 8) gprep_
   };
 
   // Ozaki: row maxima over all of K (bit patterns of |x|, stored in the double buffers bit for
-  // bit); the first chunk's values stay in registers for the digits
-  T v0[PER][4];
+  // bit); the digit pass reads the values again, mostly from L1/L2
   if constexpr (MODE == 2) {
     unsigned long long mx[PER];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      load4(q, 0, v0[q]);
-      mx[q] = 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(v0[q][i]));
-    }
-    for (long k0 = KC; k0 < K; k0 += KC) {
+    for (int q = 0; q < PER; ++q) mx[q] = 0;
+    for (long k0 = 0; k0 < K; k0 += KC) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
         T x[4];
@@ -212,16 +206,21 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 4 : MODE == 0 ? 6 : 8) gprep_
   for (long k0 = 0; k0 < K; k0 += KC) {
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-      T x[4];
-      if (MODE == 2 && k0 == 0) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = v0[q][i];
-      } else {
-        load4(q, k0, x);
-      }
       const int r = rq[q], kl = kq[q];
       const int kb = kl / KE, cbyte = (kl % KE) * OB;
       uint8_t* row = stage + (kb * P) * GRT * PB + r * PB + cbyte;
+      // rows past the matrix are never written out; a run past K is zero in every plane (the
+      // digits, BF16 parts and int8 copy of 0 are all zero bytes)
+      if (!rv[q]) continue;
+      if (k0 + kl >= K) {
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int w = 0; w < OB; ++w) *(uint32_t*)(row + p * GRT * PB + 4 * w) = 0u;
+        continue;
+      }
+      T x[4];
+      load4(q, k0, x);
       if constexpr (MODE == 0) {
         uint32_t w = 0;
 #pragma unroll
@@ -242,8 +241,7 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 4 : MODE == 0 ? 6 : 8) gprep_
         *(__nv_bfloat162*)(row + GRT * PB) = l01;
         *(__nv_bfloat162*)(row + GRT * PB + 4) = l23;
       } else {
-        // rows beyond the matrix are never written out; rows holding an Inf or a NaN (zero
-        // scale) have zero digits
+        // rows holding an Inf or a NaN (zero scale) have zero digits
         double xd[4] = {x[0], x[1], x[2], x[3]};
         if (rscale[r][0] == 0.0) xd[0] = xd[1] = xd[2] = xd[3] = 0.0;
         uint32_t wd[S];

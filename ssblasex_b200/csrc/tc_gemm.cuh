@@ -168,6 +168,18 @@ struct Config {
   }
 };
 
+// Exact integer -> double conversions on the FP64 pipe (the magic-number method: an integer
+// placed in the low mantissa bits of a large power of two, which is then subtracted), instead of
+// the conversion instructions, which run on the narrow XU pipe and bounded the Horner epilogue.
+//   int32 x:  2^52 + (x + 2^31) has x + 2^31 (as an unsigned word) in its low 32 mantissa bits;
+//   int64 s, |s| < 2^51:  1.5 * 2^52 + s has s in its low 51 mantissa bits (two's complement).
+__device__ __forceinline__ double i32_to_f64(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 0x1.000008p52;
+}
+__device__ __forceinline__ double i64_to_f64(long long s) {
+  return __longlong_as_double(s + 0x4338000000000000ll) - 0x1.8p52;
+}
+
 // Ozaki epilogue of one thread's row gi: C(gi, j) = alpha * v_j * 2^(ea + eb_j + exp_shift) + beta * C
 // for the columns j = n0 + 16c + jj below n; element (i, j) of C is at Cd[i * rs + j * cs]. The
 // column exponents come from exb, or (PRE) from registers loaded before the accumulator was ready.
@@ -310,7 +322,7 @@ __device__ __noinline__ void split_k_region(uint32_t t_row, int32_t* split_ws, i
         for (int j = 0; j < 16; ++j) sum[j] = 0;
         add_pieces<Cfg::BM>(wt + ((long)l * Cfg::BN + c * 16) * Cfg::BM, UNIT, splits, sum);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[0][j] = v[0][j] * 0x1p-8 + (double)sum[j];
+        for (int j = 0; j < 16; ++j) v[0][j] = fma(v[0][j], 0x1p-8, i64_to_f64(sum[j]));
       }
       if (row_ok) ozaki_store<1>((double*)Cb, gi, n0 + c * 16, n, 1, ldc, ea, exb, exp_shift, alpha_d, beta_d, v);
     } else {
@@ -637,7 +649,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             for (int q = 0; q < 4; ++q)
               if (l0 - q >= 0) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) v[c][j] = v[c][j] * 0x1p-8 + (double)(int32_t)raw[q][j];
+                for (int j = 0; j < 16; ++j) v[c][j] = fma(v[c][j], 0x1p-8, i32_to_f64(raw[q][j]));
               }
           }
         }

@@ -180,35 +180,52 @@ __device__ __forceinline__ double i64_to_f64(long long s) {
   return __longlong_as_double(s + 0x4338000000000000ll) - 0x1.8p52;
 }
 
+// C value of one Ozaki output: alpha * v * 2^(ea + eb + exp_shift) + beta * old (old is only used,
+// and must only be read, when beta != 0); the quiet NaN when the row or column held an Inf or NaN.
+__device__ __forceinline__ double ozaki_value(double v, int ea, int eb, int exp_shift, double alpha_d, double beta_d,
+                                              double old) {
+  const int E = ea + eb + exp_shift;
+  const double tb = (beta_d == 0.0) ? 0.0 : beta_d * old;
+  // v * 2^E: one multiplication by the exact power of two when 2^E is a normal double (correctly
+  // rounded, so equal to scalbn), scalbn otherwise
+  if (E >= -1022 && E <= 1023) return fma(v * __longlong_as_double((long long)(E + 1023) << 52), alpha_d, tb);
+  // row i of op(A) or column j of op(B) holds an Inf or a NaN
+  if (ea == kOzakiNonFiniteExp || eb == kOzakiNonFiniteExp) return __longlong_as_double((long long)0x7FF8000000000000ull);
+  return fma(scalbn(v, E), alpha_d, tb);
+}
+
 // Ozaki epilogue of one thread's row gi: C(gi, j) = alpha * v_j * 2^(ea + eb_j + exp_shift) + beta * C
 // for the columns j = n0 + 16c + jj below n; element (i, j) of C is at Cd[i * rs + j * cs]. The
 // column exponents come from exb, or (PRE) from registers loaded before the accumulator was ready.
+// When a thread's 16 outputs are adjacent in memory (cs = 1: a transposed grouped tile) and
+// 16-byte aligned, they are read and written as 8 two-double vectors.
 template <int CH, bool PRE = false>
 __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long rs, long cs, int32_t ea,
                                             const int32_t* exb, int exp_shift, double alpha_d, double beta_d,
                                             const double (&v)[CH][16], const int32_t (*ebp)[16] = nullptr) {
+  if constexpr (PRE && CH == 1) {
+    double* row = Cd + gi * rs + n0;
+    if (cs == 1 && n0 + 16 <= n && ((uintptr_t)row & 15) == 0) {
+      double2* p2 = (double2*)row;
+      double2 old[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) old[h] = (beta_d == 0.0) ? make_double2(0.0, 0.0) : p2[h];
+#pragma unroll
+      for (int h = 0; h < 8; ++h)
+        p2[h] = make_double2(ozaki_value(v[0][2 * h], ea, ebp[0][2 * h], exp_shift, alpha_d, beta_d, old[h].x),
+                             ozaki_value(v[0][2 * h + 1], ea, ebp[0][2 * h + 1], exp_shift, alpha_d, beta_d, old[h].y));
+      return;
+    }
+  }
 #pragma unroll
   for (int c = 0; c < CH; ++c)
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const long gj = n0 + c * 16 + j;
       if (gj < n) {
-        // v * 2^E: one multiplication by the exact power of two when 2^E is a normal double
-        // (correctly rounded, so equal to scalbn), scalbn otherwise
         const int eb = PRE ? ebp[c][j] : exb[gj];
-        const int E = ea + eb + exp_shift;
         double* cp = Cd + gi * rs + gj * cs;
-        if (E >= -1022 && E <= 1023) {
-          const double w = v[c][j] * __longlong_as_double((long long)(E + 1023) << 52);
-          const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
-          *cp = fma(w, alpha_d, tb);
-        } else if (ea == kOzakiNonFiniteExp || eb == kOzakiNonFiniteExp) {
-          // row i of op(A) or column j of op(B) holds an Inf or a NaN
-          *cp = __longlong_as_double((long long)0x7FF8000000000000ull);
-        } else {
-          const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
-          *cp = fma(scalbn(v[c][j], E), alpha_d, tb);
-        }
+        *cp = ozaki_value(v[c][j], ea, eb, exp_shift, alpha_d, beta_d, (beta_d == 0.0) ? 0.0 : *cp);
       }
     }
 }

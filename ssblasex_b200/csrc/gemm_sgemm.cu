@@ -194,6 +194,147 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_async_kerne
   }
 }
 
+// Persistent form for K <= KS * BK (the whole K of a work item fits the KS stages of one buffer):
+// work item w = (instance w / tiles, tile w % tiles), CTA c takes items c, c + G, c + 2G, ... and
+// double-buffers them -- the next item's operands are in flight while the current one is computed
+// and written -- so a batch of thousands of small instances keeps HBM busy instead of paying one
+// load latency per CTA. C of the item (when beta != 0) is read into registers before the
+// products, so that read overlaps them too.
+template <int BM, int BN, int BK, int TM, int TN, int KS, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kernel(SgemmArgs args, long tiles_m,
+                                                                                   long tiles, long total) {
+  constexpr int TX = BM / TM, TY = BN / TN, NT = TX * TY;
+  constexpr int PA = BM + 4, PB = BN + 4;
+  constexpr int STAGE = BK * (PA + PB);
+  constexpr int BUF = KS * STAGE;
+  extern __shared__ __align__(16) float sm[];
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  constexpr int WX = TX / 4;   // warps along m (a warp = 4 (m) x 8 (n) threads)
+  const int tx = (warp % WX) * 4 + lane % 4;
+  const int ty = (warp / WX) * 8 + lane / 4;
+  const long ktiles = (args.k + BK - 1) / BK;   // <= KS (checked by the launcher)
+  const bool read_c = args.beta != 0.0f;
+
+  auto issue = [&](long w, int buf) {
+    const long b = w / tiles, t = w - b * tiles;
+    const long m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+    const float* __restrict__ A = args.A[b];
+    const float* __restrict__ B = args.B[b];
+    const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
+    const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 4 == 0);
+#pragma unroll
+    for (int kt = 0; kt < KS; ++kt) {
+      if (kt >= ktiles) break;
+      float* sa = sm + buf * BUF + kt * STAGE;
+      sload<BM, BK, NT, A_MN>(sa, A, args.m, args.k, args.lda, m0, kt * BK, vecA);
+      sload<BN, BK, NT, B_MN>(sa + BK * PA, B, args.n, args.k, args.ldb, n0, kt * BK, vecB);
+    }
+  };
+
+  long w = blockIdx.x;
+  if (w < total) issue(w, 0);
+  commit_s();
+  for (int buf = 0; w < total; w += gridDim.x, buf ^= 1) {
+    // the next item's operands go into the other buffer (free since the previous iteration's
+    // closing barrier)
+    if (w + gridDim.x < total) issue(w + gridDim.x, buf ^ 1);
+    commit_s();
+    const long b = w / tiles, t = w - b * tiles;
+    const long m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+    float* __restrict__ C = args.C[b];
+    const long gi0 = m0 + tx * TM;
+    const bool cvec = (((uintptr_t)C) % 16 == 0) && (args.ldc % 4 == 0) && gi0 + TM <= args.m;
+    float cv[TN][TM];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + ty * TN + j;
+      const float* cp = C + gi0 + gj * args.ldc;
+#pragma unroll
+      for (int i = 0; i < TM; i += 4) {
+        if (read_c && gj < args.n && cvec) {
+          const float4 x = *(const float4*)(cp + i);
+          cv[j][i] = x.x; cv[j][i + 1] = x.y; cv[j][i + 2] = x.z; cv[j][i + 3] = x.w;
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) cv[j][i + q] = (read_c && gj < args.n && gi0 + i + q < args.m) ? cp[i + q] : 0.0f;
+        }
+      }
+    }
+    wait_s<1>();   // this item's group has landed (the next item's may still be in flight)
+    __syncthreads();
+    float acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
+    for (int kt = 0; kt < ktiles; ++kt) {
+      const float* sa = sm + buf * BUF + kt * STAGE;
+      const float* sb = sa + BK * PA;
+#pragma unroll 4
+      for (int kk = 0; kk < BK; ++kk) {
+        float av[TM], bv[TN];
+#pragma unroll
+        for (int i = 0; i < TM; i += 4) {
+          const float4 x = *(const float4*)(sa + kk * PA + tx * TM + i);
+          av[i] = x.x; av[i + 1] = x.y; av[i + 2] = x.z; av[i + 3] = x.w;
+        }
+#pragma unroll
+        for (int j = 0; j < TN; j += 4) {
+          const float4 x = *(const float4*)(sb + kk * PB + ty * TN + j);
+          bv[j] = x.x; bv[j + 1] = x.y; bv[j + 2] = x.z; bv[j + 3] = x.w;
+        }
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + ty * TN + j;
+      if (gj >= args.n) continue;
+      float* cp = C + gi0 + gj * args.ldc;
+      if (cvec) {
+#pragma unroll
+        for (int i = 0; i < TM; i += 4) {
+          float4 o;
+          o.x = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[j][i] : 0.0f);
+          o.y = fmaf(acc[i + 1][j], args.alpha, read_c ? args.beta * cv[j][i + 1] : 0.0f);
+          o.z = fmaf(acc[i + 2][j], args.alpha, read_c ? args.beta * cv[j][i + 2] : 0.0f);
+          o.w = fmaf(acc[i + 3][j], args.alpha, read_c ? args.beta * cv[j][i + 3] : 0.0f);
+          *(float4*)(cp + i) = o;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+          if (gi0 + i < args.m) cp[i] = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[j][i] : 0.0f);
+      }
+    }
+    __syncthreads();   // this buffer is refilled by the next iteration's copies
+  }
+  wait_s<0>();
+}
+
+template <int BM, int BN, int BK, int TM, int TN, int KS, int MINB, bool A_MN, bool B_MN>
+cudaError_t launch_small(const SgemmArgs& a, cudaStream_t st) {
+  constexpr int NT = (BM / TM) * (BN / TN);
+  constexpr int SMEM = 2 * KS * BK * (BM + 4 + BN + 4) * 4;
+  auto kern = sgemm_small_kernel<BM, BN, BK, TM, TN, KS, MINB, A_MN, B_MN>;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, SMEM);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+  }
+  const long tiles_m = (a.m + BM - 1) / BM;
+  const long tiles = tiles_m * ((a.n + BN - 1) / BN);
+  const long total = tiles * a.batch;
+  const long cap = (long)per_sm * num_sms();
+  kern<<<(unsigned)(total < cap ? total : cap), NT, SMEM, st>>>(a, tiles_m, tiles, total);
+  return cudaGetLastError();
+}
+
 template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB, bool A_MN, bool B_MN>
 cudaError_t launch_s(const SgemmArgs& a, cudaStream_t st) {
   constexpr int NT = (BM / TM) * (BN / TN);
@@ -236,8 +377,17 @@ cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t st) 
   cudaError_t e;
   // 3: 64 x 64 tiles, 256 threads of 4 x 4, 32-deep K stages x 2 (k <= 64 entirely in flight)
   // 4: 128 x 128 tiles, 256 threads of 8 x 8, 16-deep K stages x 3
-  if (config == 4) e = launch_sl<128, 128, 16, 8, 8, 3, 1>(a, a_mn, b_mn, st);
-  else e = launch_sl<64, 64, 32, 4, 4, 2, 3>(a, a_mn, b_mn, st);
+  // 5 (k <= 64): 64 x 64 tiles, persistent CTAs that double-buffer their work items
+  if (config == 5 && d.k <= 64) {
+    if (a_mn && b_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, true, true>(a, st);
+    else if (a_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, true, false>(a, st);
+    else if (b_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, false, true>(a, st);
+    else e = launch_small<64, 64, 32, 4, 4, 2, 3, false, false>(a, st);
+  } else if (config == 4) {
+    e = launch_sl<128, 128, 16, 8, 8, 3, 1>(a, a_mn, b_mn, st);
+  } else {
+    e = launch_sl<64, 64, 32, 4, 4, 2, 3>(a, a_mn, b_mn, st);
+  }
   note_launch();
   return e;
 }

@@ -243,8 +243,8 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
   const long big_tiles = ((d.m + 127) / 128) * ((d.n + 127) / 128) * d.batch;
   const bool big_default = d.m >= 128 && d.n >= 128 && big_tiles >= 2L * num_sms();
   const int cfg = choose_config(SSBLAS_PATH_SIMT, d.m, d.n, d.k, d.batch,
-                                d.row == ROW_F32 ? (big_default ? 4 : 3) : (big_default ? 1 : 0));
-  // fp32: configurations 3 and 4 are the cp.async-pipelined kernel (gemm_sgemm.cu)
+                                d.row == ROW_F32 ? (big_default ? 4 : d.k <= 64 ? 5 : 3) : (big_default ? 1 : 0));
+  // fp32: configurations 3, 4 and 5 are the cp.async-pipelined kernels (gemm_sgemm.cu)
   if (d.row == ROW_F32 && cfg >= 3) return launch_sgemm_async(d, cfg, stream);
   const bool big = cfg == 1;
   switch (d.row) {

@@ -240,17 +240,19 @@ def test_dmma_layouts_and_alignment(S, transa, transb, aligned):
 
 
 # ------------------------------------------------------------------------- plain fp32 (cp.async)
-@pytest.mark.parametrize("cfg", [3, 4])
+@pytest.mark.parametrize("cfg", [3, 4, 5])
 @pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("aligned", [True, False])
 def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
-    """Plain fp32 on the cp.async-pipelined kernel (configuration 3: 64 x 64 tiles, 4: 128 x 128)
-    for every op(A)/op(B) pair, with 16-byte aligned instances and leading dimensions that are
-    multiples of 4 (16-byte copies) or instances at odd 4-byte offsets with odd leading dimensions
-    (4-byte copies), ragged edges in m, n and k, beta != 0."""
+    """Plain fp32 on the cp.async-pipelined kernels (configuration 3: 64 x 64 tiles, 4: 128 x 128,
+    5: persistent 64 x 64 CTAs that double-buffer their (tile, instance) items, for k <= 64 -- run
+    with 300 instances, so every CTA walks several items) for every op(A)/op(B) pair, with 16-byte
+    aligned instances and leading dimensions that are multiples of 4 (16-byte copies) or instances
+    at odd 4-byte offsets with odd leading dimensions (4-byte copies), ragged edges in m, n and k,
+    beta != 0."""
     import torch
     from ssblasex_b200 import workloads as W
-    m, n, k, batch = 141, 77, 203, 3
+    m, n, k, batch = (141, 77, 203, 3) if cfg != 5 else (141, 77, 61, 300)
     arows, brows = (m if transa == 0 else k), (k if transb == 0 else n)
     pad = 0 if aligned else 1
     lda, ldb, ldc = arows + (3 if aligned else 2), brows + (1 if aligned else 2), m + (3 if aligned else 2)

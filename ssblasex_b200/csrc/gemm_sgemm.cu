@@ -45,6 +45,9 @@ __device__ __forceinline__ void wait_s() { asm volatile("cp.async.wait_group %0;
 
 // Copies the (ROWS x BK) slab of one operand at (r0, k0) into a stage buffer staged [k][r]
 // (pitch ROWS + 4 floats). MN: element (r, k) at X[r + k*ld]; otherwise at X[r*ld + k].
+// Each thread's chunks keep one position along the contiguous dimension and step a fixed number
+// of rows (or k) per iteration, so the source pointer advances by a constant: no per-element
+// index arithmetic.
 template <int ROWS, int BK, int NT, bool MN>
 __device__ __forceinline__ void sload(float* dst, const float* __restrict__ X, long nrows, long K, long ld, long r0,
                                       long k0, bool vec) {
@@ -52,40 +55,45 @@ __device__ __forceinline__ void sload(float* dst, const float* __restrict__ X, l
   const int t = threadIdx.x;
   if (MN) {
     if (vec) {
-      constexpr int CH = ROWS * BK / 4;   // 16-byte chunks along r
+      // 16-byte chunks along r: thread t takes r = 4 (t % (ROWS/4)), k = t / (ROWS/4) + q KSTEP
+      constexpr int CPR = ROWS / 4, KSTEP = NT / CPR, NQ = BK / KSTEP;
+      static_assert(NT % CPR == 0 && BK % KSTEP == 0, "copy shape");
+      const int rr = 4 * (t % CPR), kk0 = t / CPR;
+      const long gr = r0 + rr;
+      long nv = nrows - gr;
+      nv = nv < 0 ? 0 : (nv > 4 ? 4 : nv);
+      const float* src = X + gr + (k0 + kk0) * ld;
+      const uint32_t d0 = saddr(dst + kk0 * P + rr);
 #pragma unroll
-      for (int q = 0; q < (CH + NT - 1) / NT; ++q) {
-        const int idx = t + q * NT;
-        if (CH % NT != 0 && idx >= CH) break;
-        const int kk = idx / (ROWS / 4), rr = 4 * (idx % (ROWS / 4));
-        const long gr = r0 + rr, gk = k0 + kk;
-        long nv = (gk < K) ? nrows - gr : 0;
-        nv = nv < 0 ? 0 : (nv > 4 ? 4 : nv);
-        cp16s(saddr(dst + kk * P + rr), nv > 0 ? X + gr + gk * ld : X, (int)(4 * nv));
+      for (int q = 0; q < NQ; ++q) {
+        const bool ok = nv > 0 && k0 + kk0 + q * KSTEP < K;
+        cp16s(d0 + 4u * (uint32_t)(q * KSTEP * P), ok ? src + (long)q * KSTEP * ld : X, ok ? (int)(4 * nv) : 0);
       }
     } else {
-      constexpr int EL = ROWS * BK;
+      constexpr int KSTEP = NT / ROWS, NQ = BK / KSTEP;
+      static_assert(NT % ROWS == 0 && BK % KSTEP == 0, "copy shape");
+      const int rr = t % ROWS, kk0 = t / ROWS;
+      const bool rok = r0 + rr < nrows;
+      const float* src = X + (r0 + rr) + (k0 + kk0) * ld;
+      const uint32_t d0 = saddr(dst + kk0 * P + rr);
 #pragma unroll
-      for (int q = 0; q < (EL + NT - 1) / NT; ++q) {
-        const int idx = t + q * NT;
-        if (EL % NT != 0 && idx >= EL) break;
-        const int kk = idx / ROWS, rr = idx % ROWS;
-        const long gr = r0 + rr, gk = k0 + kk;
-        const bool ok = gr < nrows && gk < K;
-        cp4s(saddr(dst + kk * P + rr), ok ? X + gr + gk * ld : X, ok ? 4 : 0);
+      for (int q = 0; q < NQ; ++q) {
+        const bool ok = rok && k0 + kk0 + q * KSTEP < K;
+        cp4s(d0 + 4u * (uint32_t)(q * KSTEP * P), ok ? src + (long)q * KSTEP * ld : X, ok ? 4 : 0);
       }
     }
   } else {
     // transpose by the copy: consecutive threads take consecutive k of one row
-    constexpr int EL = ROWS * BK;
+    constexpr int RSTEP = NT / BK, NQ = ROWS / RSTEP;
+    static_assert(NT % BK == 0 && ROWS % RSTEP == 0, "copy shape");
+    const int kk = t % BK, rr0 = t / BK;
+    const bool kok = k0 + kk < K;
+    const float* src = X + (r0 + rr0) * ld + (k0 + kk);
+    const uint32_t d0 = saddr(dst + kk * P + rr0);
 #pragma unroll
-    for (int q = 0; q < (EL + NT - 1) / NT; ++q) {
-      const int idx = t + q * NT;
-      if (EL % NT != 0 && idx >= EL) break;
-      const int rr = idx / BK, kk = idx % BK;
-      const long gr = r0 + rr, gk = k0 + kk;
-      const bool ok = gr < nrows && gk < K;
-      cp4s(saddr(dst + kk * P + rr), ok ? X + gr * ld + gk : X, ok ? 4 : 0);
+    for (int q = 0; q < NQ; ++q) {
+      const bool ok = kok && r0 + rr0 + q * RSTEP < nrows;
+      cp4s(d0 + 4u * (uint32_t)(q * RSTEP), ok ? src + (long)q * RSTEP * ld : X, ok ? 4 : 0);
     }
   }
 }

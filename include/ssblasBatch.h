@@ -112,7 +112,8 @@ typedef enum {
   SSBLAS_PATH_OZAKI_SLICER = 7,    /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
                                       pre-pass. 0 (default) and 3: one pass with thread-block
                                       clusters of 16 rows x 512 k per CTA when k <= 2048; 2: the
-                                      same with 32 rows x 256 k; 4: 8 rows x 1024 k; 1: exponent
+                                      same with 32 rows x 256 k; 4: 8 rows x 1024 k; 5: 16 rows x
+                                      256 k per 256-thread CTA, two CTAs per SM; 1: exponent
                                       pass then digit pass */
   SSBLAS_PATH_SPLITK_I8 = 8,       /* not a path: ssblasSetKernelConfig keys of the split-K factor */
   SSBLAS_PATH_SPLITK_OZAKI = 9     /* of the int8 and Ozaki tcgen05 GEMMs. config = number of K

@@ -488,17 +488,19 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
 //     [k / 256][R rows][256 k] (one TMA box per 256 k).
 constexpr int CL_NTH = 512;
 
-template <int R, int KC>
+template <int R, int KC, int NTH>
 struct ClShape {
-  static constexpr int TILE = R * KC;                // fp64 values per stage (8192)
+  static constexpr int TILE = R * KC;                // fp64 values per stage (16 per thread)
+  static constexpr int W = NTH / 32;                 // warps
   static constexpr int NC = KC / 16;                 // runs of 4 k per row (per thread group)
   static constexpr int LR = R < 16 ? R : 16;         // rows per half-warp (rows contiguous)
   static constexpr int RG = R / LR;                  // row groups
-  static constexpr int NW = 16 / RG;                 // warps sharing a row (rows contiguous)
+  static constexpr int NW = W / RG;                  // warps sharing a row (rows contiguous)
   static constexpr int PW = KC / 4 + 4;              // staged digit words per row (16-byte aligned)
-  static_assert(TILE == 8192 && TILE / CL_NTH == 16, "tile shape");
+  static_assert(TILE / NTH == 16 && TILE % NTH == 0, "tile shape");
+  static_assert(W % RG == 0 && (32 / LR) * NW == NC && NTH % NC == 0, "thread mapping");
   template <int S>
-  static constexpr int smem_bytes() { return 2 * TILE * 8 + S * R * PW * 4 + 16 * 32 * 8 + 2 * R * 8 + R * 16 + 16; }
+  static constexpr int smem_bytes() { return 2 * TILE * 8 + S * R * PW * 4 + W * 32 * 8 + 2 * R * 8 + R * 16 + 16; }
   // position of element (r, k) of a tile staged with K contiguous
   static __device__ __forceinline__ int kc_index(int r, int k) { return (k / 256) * R * 256 + r * 256 + (k % 256); }
 };
@@ -546,17 +548,17 @@ __device__ __forceinline__ ClusterItem cluster_item(long item, long n0, uint32_t
 }
 
 // cp.async: this CTA's R x KC slab of an item into a stage (zero outside the matrix).
-template <int R, int KC>
+template <int R, int KC, int NTH>
 __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, const ClusterItem& ci, long kbase) {
-  using Sh = ClShape<R, KC>;
+  using Sh = ClShape<R, KC, NTH>;
   const double* X = (const double*)a.X[ci.b];
   const int t = threadIdx.x;
   const bool vec = (((uintptr_t)X) % 16 == 0) && (a.ld % 2 == 0);
   if (!a.kcontig) {
     // [k][R rows]: chunk = 2 rows at one k
 #pragma unroll 4
-    for (int q = 0; q < Sh::TILE / 2 / CL_NTH; ++q) {
-      const int ch = t + q * CL_NTH, kl = ch / (R / 2), rp = 2 * (ch % (R / 2));
+    for (int q = 0; q < Sh::TILE / 2 / NTH; ++q) {
+      const int ch = t + q * NTH, kl = ch / (R / 2), rp = 2 * (ch % (R / 2));
       const long gr = ci.row0 + rp, gk = kbase + kl;
       const long nr = (gk < a.K) ? (a.rows - gr >= 2 ? 2 : (a.rows - gr > 0 ? a.rows - gr : 0)) : 0;
       const double* src = nr > 0 ? X + gr + gk * a.ld : X;
@@ -571,8 +573,8 @@ __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, c
   } else {
     // [k / 256][R rows][256 k]: chunk = 2 consecutive k of one row
 #pragma unroll 4
-    for (int q = 0; q < Sh::TILE / 2 / CL_NTH; ++q) {
-      const int ch = t + q * CL_NTH, rl = ch / (KC / 2), kp = 2 * (ch % (KC / 2));
+    for (int q = 0; q < Sh::TILE / 2 / NTH; ++q) {
+      const int ch = t + q * NTH, rl = ch / (KC / 2), kp = 2 * (ch % (KC / 2));
       const long gr = ci.row0 + rl, gk = kbase + kp;
       const long nk = (gr < a.rows) ? (a.K - gk >= 2 ? 2 : (a.K - gk > 0 ? a.K - gk : 0)) : 0;
       const double* src = nk > 0 ? X + gr * a.ld + gk : X;
@@ -606,11 +608,11 @@ __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_
 
 // TMA: the item's R x KC tile of one operand through its 3-D tensor map (box: R rows x 256 k,
 // zero outside), one box per 256 k.
-template <int R, int KC>
+template <int R, int KC, int NTH>
 __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const CUtensorMap* tm, bool kcontig,
                                             const ClusterItem& ci, long kbase) {
   const uint32_t b = ptx::smem_u32(bar);
-  ptx::mbar_arrive_expect_tx(b, ClShape<R, KC>::TILE * 8);
+  ptx::mbar_arrive_expect_tx(b, ClShape<R, KC, NTH>::TILE * 8);
 #pragma unroll
   for (int h = 0; h < KC / 256; ++h) {
     const uint32_t dst = ptx::smem_u32(stage + h * R * 256);
@@ -619,18 +621,18 @@ __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const 
   }
 }
 
-template <int S, bool TMA, int R, int KC>
-__global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
+template <int S, bool TMA, int R, int KC, int NTH>
+__global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
                                                                   const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
                                                                   int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
                                                                   long n_items, int CS, int* err) {
-  using Sh = ClShape<R, KC>;
+  using Sh = ClShape<R, KC, NTH>;
   constexpr int NC = Sh::NC, LR = Sh::LR, RG = Sh::RG, NW = Sh::NW, PW = Sh::PW, TILE = Sh::TILE;
   extern __shared__ __align__(16) uint8_t dyn[];
   double* stages = (double*)dyn;                                                   // [2][TILE]
   uint32_t* st = (uint32_t*)(dyn + 2 * TILE * 8);                                  // [S][R][PW]
-  double* red = (double*)(dyn + 2 * TILE * 8 + S * R * PW * 4);                    // [16][32]
-  double* pmax = red + 16 * 32;                                                    // [2][R]
+  double* red = (double*)(dyn + 2 * TILE * 8 + S * R * PW * 4);                    // [W][32]
+  double* pmax = red + Sh::W * 32;                                                    // [2][R]
   double* rscale = pmax + 2 * R;                                                   // [R][2]
   uint64_t* full = (uint64_t*)(rscale + 2 * R);                                    // [2] (TMA)
 
@@ -654,10 +656,10 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
     if (item < n_items) {
       const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
       if (TMA) {
-        if (t == 0) cluster_tma<R, KC>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
+        if (t == 0) cluster_tma<R, KC, NTH>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
                                        ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
       } else {
-        cluster_load<R, KC>(stages + s * TILE, ci.second ? a1 : a0, ci, kbase);
+        cluster_load<R, KC, NTH>(stages + s * TILE, ci.second ? a1 : a0, ci, kbase);
       }
     }
     if (!TMA) cpa_commit();
@@ -752,10 +754,10 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
       if (nxt < n_items) {
         const ClusterItem cn = cluster_item<R>(nxt, n0, bpi0, bpi1);
         if (TMA) {
-          if (t == 0) cluster_tma<R, KC>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
+          if (t == 0) cluster_tma<R, KC, NTH>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
                                          cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
         } else {
-          cluster_load<R, KC>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
+          cluster_load<R, KC, NTH>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
         }
       }
       if (!TMA) cpa_commit();
@@ -805,11 +807,11 @@ __global__ void __launch_bounds__(CL_NTH, 1) ozaki_cluster_kernel(const __grid_c
   cluster_wait();
 }
 
-template <int S, bool TMA, int R, int KC>
+template <int S, bool TMA, int R, int KC, int NTH>
 cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, const PlaneArgs& a0, int32_t* e0,
                               long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st) {
-  constexpr int SMEM = ClShape<R, KC>::template smem_bytes<S>();
-  auto kern = ozaki_cluster_kernel<S, TMA, R, KC>;
+  constexpr int SMEM = ClShape<R, KC, NTH>::template smem_bytes<S>();
+  auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
@@ -817,7 +819,7 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
     attr = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.blockDim = dim3(CL_NTH, 1, 1);
+  cfg.blockDim = dim3(NTH, 1, 1);
   cfg.dynamicSmemBytes = SMEM;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -827,15 +829,15 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  // persistent clusters: as many as fit at once (one CTA per SM), at most one per item
+  // persistent clusters: as many as fit at once (CL_NTH / NTH CTAs per SM), at most one per item
   static int max_clusters[9] = {0};
   if (max_clusters[CS] == 0) {
-    cfg.gridDim = dim3((unsigned)(CS * num_sms()), 1, 1);
+    cfg.gridDim = dim3((unsigned)(CS * num_sms() * (CL_NTH / NTH)), 1, 1);
     int nc = 0;
     cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, kern, &cfg);
     if (e != cudaSuccess || nc <= 0) {
       cudaGetLastError();
-      nc = num_sms() / CS;
+      nc = num_sms() * (CL_NTH / NTH) / CS;
     }
     max_clusters[CS] = nc > 0 ? nc : 1;
   }
@@ -863,7 +865,7 @@ bool slicer_map(CUtensorMap* m, const PlaneArgs& a, int R) {
   return make_tiled_map(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, a.X0, dims, strides, box, 0);
 }
 
-template <int S, int R, int KC>
+template <int S, int R, int KC, int NTH = CL_NTH>
 cudaError_t launch_cluster_shape(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
                                  cudaStream_t st) {
   const int CS = (int)((a0.Kp + KC - 1) / KC);
@@ -873,14 +875,17 @@ cudaError_t launch_cluster_shape(const PlaneArgs& a0, int32_t* e0, const PlaneAr
   CUtensorMap tm0, tm1;
   const bool tma = slicer_map(&tm0, a0, R) && (!two || slicer_map(&tm1, a1, R));
   if (!two) tm1 = tm0;
-  if (tma) return launch_cluster_st<S, true, R, KC>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
-  return launch_cluster_st<S, false, R, KC>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  if (tma) return launch_cluster_st<S, true, R, KC, NTH>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  return launch_cluster_st<S, false, R, KC, NTH>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
 }
 
-// Item shape: 16 x 512 (configuration 3, the default), 32 x 256 (2) or 8 x 1024 (4).
+// Item shape: 16 x 512 (configuration 3, the default), 32 x 256 (2) or 8 x 1024 (4), all with
+// 512-thread CTAs (one per SM); or 16 x 256 with 256-thread CTAs, two per SM (5), so that one
+// CTA converts while the other waits at its cluster barrier.
 template <int S>
 cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two, int shape,
                              cudaStream_t st) {
+  if (shape == 5) return launch_cluster_shape<S, 16, 256, 256>(a0, e0, a1, e1, two, st);
   if (shape == 2) return launch_cluster_shape<S, 32, 256>(a0, e0, a1, e1, two, st);
   if (shape == 4) return launch_cluster_shape<S, 8, 1024>(a0, e0, a1, e1, two, st);
   return launch_cluster_shape<S, 16, 512>(a0, e0, a1, e1, two, st);

@@ -102,7 +102,7 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
-@pytest.mark.parametrize("form", [1, 2, 3, 4])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5])
 @pytest.mark.parametrize("ta,tb,m,n,k,batch", [
     (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 (4) CTAs, K contiguous, 16-byte loads
     (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2 (1), odd ld (8-byte loads)
@@ -114,11 +114,11 @@ def test_ozaki_layouts_and_error(S, ta, tb):
 def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
     """Every slicing kernel (the two-pass form 1 -- row maxima per (32 rows, 256 k) part, then
     digits per (32 rows, 128 k) chunk -- and the one-pass item shapes: form 2 = 32 rows x 256 k
-    per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k) produces the planes the CPU restatement
-    produces: the product is bit-exact against oracle.ozaki_f64 whichever kernel sliced the
-    operands."""
+    per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k, 5 = 16 rows x 256 k with two 256-thread
+    CTAs per SM) produces the planes the CPU restatement produces: the product is bit-exact
+    against oracle.ozaki_f64 whichever kernel sliced the operands."""
     from ssblasex_b200 import workloads as W
-    if k > 2048 and form in (2, 4):
+    if k > 2048 and form in (2, 4, 5):
         pytest.skip("the one-pass forms apply to k <= 2048")
     S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
     S.set_kernel_config("ozaki_slicer", form)

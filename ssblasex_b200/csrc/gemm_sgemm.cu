@@ -83,10 +83,15 @@ __device__ __forceinline__ void sload(float* dst, const float* __restrict__ X, l
       }
     }
   } else {
-    // transpose by the copy: consecutive threads take consecutive k of one row
-    constexpr int RSTEP = NT / BK, NQ = ROWS / RSTEP;
-    static_assert(NT % BK == 0 && ROWS % RSTEP == 0, "copy shape");
-    const int kk = t % BK, rr0 = t / BK;
+    // Transpose by the copy. A warp instruction covers 8 consecutive k of 4 consecutive rows
+    // (lane = 4 * (k % 8) + r % 4): the reads are whole 32-byte sectors, and the [k][r] stores
+    // land in banks (4 k + r) mod 32 (pitch = 4 mod 32), all 32 distinct. Instruction u = warp + W q
+    // of the stage takes k group u % KG and row group u / KG, so each thread keeps its k and
+    // steps RSTEP rows per iteration.
+    constexpr int W = NT / 32, KG = BK / 8, RSTEP = 4 * (W / KG), NQ = ROWS / RSTEP;
+    static_assert(BK % 8 == 0 && W % KG == 0 && ROWS % RSTEP == 0 && P % 32 == 4, "copy shape");
+    const int lane = t % 32, warp = t / 32;
+    const int kk = 8 * (warp % KG) + lane / 4, rr0 = 4 * (warp / KG) + lane % 4;
     const bool kok = k0 + kk < K;
     const float* src = X + (r0 + rr0) * ld + (k0 + kk);
     const uint32_t d0 = saddr(dst + kk * P + rr0);

@@ -198,7 +198,8 @@ __device__ __forceinline__ double ozaki_value(double v, int ea, int eb, int exp_
 // for the columns j = n0 + 16c + jj below n; element (i, j) of C is at Cd[i * rs + j * cs]. The
 // column exponents come from exb, or (PRE) from registers loaded before the accumulator was ready.
 // When a thread's 16 outputs are adjacent in memory (cs = 1: a transposed grouped tile) and
-// 16-byte aligned, they are read and written as 8 two-double vectors.
+// 16-byte aligned, they are read and written as 8 two-double vectors. C is written with
+// evict-first (streaming) stores: nothing here reads it again, and the operand tiles keep L2.
 template <int CH, bool PRE = false>
 __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long rs, long cs, int32_t ea,
                                             const int32_t* exb, int exp_shift, double alpha_d, double beta_d,
@@ -212,8 +213,9 @@ __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n
       for (int h = 0; h < 8; ++h) old[h] = (beta_d == 0.0) ? make_double2(0.0, 0.0) : p2[h];
 #pragma unroll
       for (int h = 0; h < 8; ++h)
-        p2[h] = make_double2(ozaki_value(v[0][2 * h], ea, ebp[0][2 * h], exp_shift, alpha_d, beta_d, old[h].x),
-                             ozaki_value(v[0][2 * h + 1], ea, ebp[0][2 * h + 1], exp_shift, alpha_d, beta_d, old[h].y));
+        __stcs(p2 + h, make_double2(ozaki_value(v[0][2 * h], ea, ebp[0][2 * h], exp_shift, alpha_d, beta_d, old[h].x),
+                                    ozaki_value(v[0][2 * h + 1], ea, ebp[0][2 * h + 1], exp_shift, alpha_d, beta_d,
+                                                old[h].y)));
       return;
     }
   }
@@ -225,7 +227,7 @@ __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n
       if (gj < n) {
         const int eb = PRE ? ebp[c][j] : exb[gj];
         double* cp = Cd + gi * rs + gj * cs;
-        *cp = ozaki_value(v[c][j], ea, eb, exp_shift, alpha_d, beta_d, (beta_d == 0.0) ? 0.0 : *cp);
+        __stcs(cp, ozaki_value(v[c][j], ea, eb, exp_shift, alpha_d, beta_d, (beta_d == 0.0) ? 0.0 : *cp));
       }
     }
 }

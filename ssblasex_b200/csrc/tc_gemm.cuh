@@ -197,39 +197,67 @@ __device__ __forceinline__ double ozaki_value(double v, int ea, int eb, int exp_
 // Ozaki epilogue of one thread's row gi: C(gi, j) = alpha * v_j * 2^(ea + eb_j + exp_shift) + beta * C
 // for the columns j = n0 + 16c + jj below n; element (i, j) of C is at Cd[i * rs + j * cs]. The
 // column exponents come from exb, or (PRE) from registers loaded before the accumulator was ready.
-// When a thread's 16 outputs are adjacent in memory (cs = 1: a transposed grouped tile) and
-// 16-byte aligned, they are read and written as 8 two-double vectors. C is written with
-// evict-first (streaming) stores: nothing here reads it again, and the operand tiles keep L2.
+// Each output is computed and stored with 2^E built as a normal double when E is in [-1022, 1023];
+// the others (huge or tiny scale factors, and the sentinel exponent of rows/columns holding Inf or
+// NaN) are only flagged, then redone through ozaki_value in a block entered only when a flag is
+// set -- so the common path carries no trace of scalbn and the NaN case, and every result equals
+// ozaki_value's bit for bit. When a thread's 16 outputs are adjacent in memory (cs = 1: a
+// transposed grouped tile) and 16-byte aligned, they are written as 8 two-double vectors. C is
+// written with evict-first (streaming) stores: nothing here reads it again, and the operand tiles
+// keep L2.
 template <int CH, bool PRE = false>
 __device__ __forceinline__ void ozaki_store(double* Cd, long gi, long n0, long n, long rs, long cs, int32_t ea,
                                             const int32_t* exb, int exp_shift, double alpha_d, double beta_d,
                                             const double (&v)[CH][16], const int32_t (*ebp)[16] = nullptr) {
+  static_assert(CH <= 2, "flag bits");
   if constexpr (PRE && CH == 1) {
     double* row = Cd + gi * rs + n0;
     if (cs == 1 && n0 + 16 <= n && ((uintptr_t)row & 15) == 0) {
-      double2* p2 = (double2*)row;
-      double2 old[8];
+      double w[16];
+      bool rare = false;
 #pragma unroll
-      for (int h = 0; h < 8; ++h) old[h] = (beta_d == 0.0) ? make_double2(0.0, 0.0) : p2[h];
+      for (int j = 0; j < 16; ++j) {
+        const int E = ea + ebp[0][j] + exp_shift;
+        rare |= (unsigned)(E + 1022) > 2045u;
+        const double tb = (beta_d == 0.0) ? 0.0 : beta_d * row[j];
+        w[j] = fma(v[0][j] * __longlong_as_double((long long)(E + 1023) << 52), alpha_d, tb);
+      }
+      if (!rare) {
 #pragma unroll
-      for (int h = 0; h < 8; ++h)
-        __stcs(p2 + h, make_double2(ozaki_value(v[0][2 * h], ea, ebp[0][2 * h], exp_shift, alpha_d, beta_d, old[h].x),
-                                    ozaki_value(v[0][2 * h + 1], ea, ebp[0][2 * h + 1], exp_shift, alpha_d, beta_d,
-                                                old[h].y)));
-      return;
+        for (int h = 0; h < 8; ++h) __stcs((double2*)row + h, make_double2(w[2 * h], w[2 * h + 1]));
+        return;
+      }
     }
   }
+  uint32_t slow = 0u;   // bit 16c + j: output (c, j) needs ozaki_value
 #pragma unroll
   for (int c = 0; c < CH; ++c)
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const long gj = n0 + c * 16 + j;
       if (gj < n) {
-        const int eb = PRE ? ebp[c][j] : exb[gj];
+        const int E = ea + (PRE ? ebp[c][j] : exb[gj]) + exp_shift;
         double* cp = Cd + gi * rs + gj * cs;
-        __stcs(cp, ozaki_value(v[c][j], ea, eb, exp_shift, alpha_d, beta_d, (beta_d == 0.0) ? 0.0 : *cp));
+        if ((unsigned)(E + 1022) <= 2045u) {
+          const double tb = (beta_d == 0.0) ? 0.0 : beta_d * (*cp);
+          __stcs(cp, fma(v[c][j] * __longlong_as_double((long long)(E + 1023) << 52), alpha_d, tb));
+        } else {
+          slow |= 1u << (16 * c + j);
+        }
       }
     }
+  if (slow) {
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if ((slow >> (16 * c + j)) & 1u) {
+          const long gj = n0 + c * 16 + j;
+          double* cp = Cd + gi * rs + gj * cs;
+          __stcs(cp, ozaki_value(v[c][j], ea, PRE ? ebp[c][j] : exb[gj], exp_shift, alpha_d, beta_d,
+                                 (beta_d == 0.0) ? 0.0 : *cp));
+        }
+  }
 }
 
 // int32 epilogue of one thread's row (Ci = &C(gi, 0)): C(gi, j) = alpha * raw + beta * C with

@@ -116,12 +116,16 @@ typedef enum {
                                       256 k per 256-thread CTA, two CTAs per SM; 1: exponent
                                       pass then digit pass */
   SSBLAS_PATH_SPLITK_I8 = 8,       /* not a path: ssblasSetKernelConfig keys of the split-K factor */
-  SSBLAS_PATH_SPLITK_OZAKI = 9     /* of the int8 and Ozaki tcgen05 GEMMs. config = number of K
+  SSBLAS_PATH_SPLITK_OZAKI = 9,    /* of the int8 and Ozaki tcgen05 GEMMs. config = number of K
                                       pieces per output tile (1 = none, at most 64), 0 = automatic
                                       (split only when the tiles fill less than half of the SMs).
                                       Each piece's exact int32 sums are added in 64 bits, so the
                                       result does not depend on the factor; the Ozaki GEMM always
                                       splits k > 16384 into pieces of at most 16384. */
+  SSBLAS_PATH_OZAKI_PIPELINE = 10  /* not a path: ssblasSetKernelConfig key of the Ozaki slicing /
+                                      GEMM pipeline: config = chunks of the batch (1 = none, at most
+                                      8), 0 = automatic (none); the slicing of chunk c + 1 runs
+                                      beside the GEMM of chunk c. */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

@@ -488,16 +488,16 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
 //     [k / 256][R rows][256 k] (one TMA box per 256 k).
 constexpr int CL_NTH = 512;
 
-template <int R, int KC, int NTH>
+template <int R, int KC, int NTH, int RUNS = 4>
 struct ClShape {
-  static constexpr int TILE = R * KC;                // fp64 values per stage (16 per thread)
+  static constexpr int TILE = R * KC;                // fp64 values per stage (4 RUNS per thread)
   static constexpr int W = NTH / 32;                 // warps
-  static constexpr int NC = KC / 16;                 // runs of 4 k per row (per thread group)
+  static constexpr int NC = KC / (4 * RUNS);         // run positions per row (threads sharing a row)
   static constexpr int LR = R < 16 ? R : 16;         // rows per half-warp (rows contiguous)
   static constexpr int RG = R / LR;                  // row groups
   static constexpr int NW = W / RG;                  // warps sharing a row (rows contiguous)
   static constexpr int PW = KC / 4 + 4;              // staged digit words per row (16-byte aligned)
-  static_assert(TILE / NTH == 16 && TILE % NTH == 0, "tile shape");
+  static_assert(TILE / NTH == 4 * RUNS && TILE % NTH == 0, "tile shape");
   static_assert(W % RG == 0 && (32 / LR) * NW == NC && NTH % NC == 0, "thread mapping");
   template <int S>
   static constexpr int smem_bytes() { return 2 * TILE * 8 + S * R * PW * 4 + W * 32 * 8 + 2 * R * 8 + R * 16 + 16; }
@@ -548,9 +548,9 @@ __device__ __forceinline__ ClusterItem cluster_item(long item, long n0, uint32_t
 }
 
 // cp.async: this CTA's R x KC slab of an item into a stage (zero outside the matrix).
-template <int R, int KC, int NTH>
+template <int R, int KC, int NTH, int RUNS>
 __device__ __forceinline__ void cluster_load(double* stage, const PlaneArgs a, const ClusterItem& ci, long kbase) {
-  using Sh = ClShape<R, KC, NTH>;
+  using Sh = ClShape<R, KC, NTH, RUNS>;
   const double* X = (const double*)a.X[ci.b];
   const int t = threadIdx.x;
   const bool vec = (((uintptr_t)X) % 16 == 0) && (a.ld % 2 == 0);
@@ -608,11 +608,11 @@ __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_
 
 // TMA: the item's R x KC tile of one operand through its 3-D tensor map (box: R rows x 256 k,
 // zero outside), one box per 256 k.
-template <int R, int KC, int NTH>
+template <int R, int KC, int NTH, int RUNS>
 __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const CUtensorMap* tm, bool kcontig,
                                             const ClusterItem& ci, long kbase) {
   const uint32_t b = ptx::smem_u32(bar);
-  ptx::mbar_arrive_expect_tx(b, ClShape<R, KC, NTH>::TILE * 8);
+  ptx::mbar_arrive_expect_tx(b, ClShape<R, KC, NTH, RUNS>::TILE * 8);
 #pragma unroll
   for (int h = 0; h < KC / 256; ++h) {
     const uint32_t dst = ptx::smem_u32(stage + h * R * 256);
@@ -621,12 +621,12 @@ __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const 
   }
 }
 
-template <int S, bool TMA, int R, int KC, int NTH>
-__global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
+template <int S, bool TMA, int R, int KC, int NTH, int RUNS>
+__global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
                                                                   const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
                                                                   int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
                                                                   long n_items, int CS, int* err) {
-  using Sh = ClShape<R, KC, NTH>;
+  using Sh = ClShape<R, KC, NTH, RUNS>;
   constexpr int NC = Sh::NC, LR = Sh::LR, RG = Sh::RG, NW = Sh::NW, PW = Sh::PW, TILE = Sh::TILE;
   extern __shared__ __align__(16) uint8_t dyn[];
   double* stages = (double*)dyn;                                                   // [2][TILE]
@@ -656,10 +656,10 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
     if (item < n_items) {
       const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
       if (TMA) {
-        if (t == 0) cluster_tma<R, KC, NTH>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
+        if (t == 0) cluster_tma<R, KC, NTH, RUNS>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
                                        ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
       } else {
-        cluster_load<R, KC, NTH>(stages + s * TILE, ci.second ? a1 : a0, ci, kbase);
+        cluster_load<R, KC, NTH, RUNS>(stages + s * TILE, ci.second ? a1 : a0, ci, kbase);
       }
     }
     if (!TMA) cpa_commit();
@@ -683,10 +683,10 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
     if (t < S * R) bulk_wait_read0();   // the previous item's digit rows have left st
     __syncthreads();
     const double* tile = stages + s * TILE;
-    double v[16];
+    double v[4 * RUNS];
     if (a.kcontig) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < RUNS; ++j) {
         const int k = 4 * c + 4 * NC * j;
         const double2 x0 = *(const double2*)(tile + Sh::kc_index(r, k));
         const double2 x1 = *(const double2*)(tile + Sh::kc_index(r, k) + 2);
@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < RUNS; ++j)
 #pragma unroll
         for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 4 * NC * j + i) * R + r];
     }
@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
     // hold them as doubles, bit for bit)
     unsigned long long mx = 0;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) mx = max_u64(mx, abs_bits(v[e]));
+    for (int e = 0; e < 4 * RUNS; ++e) mx = max_u64(mx, abs_bits(v[e]));
     double* pm = pmax + s * R;
     auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
     auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
@@ -754,10 +754,10 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
       if (nxt < n_items) {
         const ClusterItem cn = cluster_item<R>(nxt, n0, bpi0, bpi1);
         if (TMA) {
-          if (t == 0) cluster_tma<R, KC, NTH>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
+          if (t == 0) cluster_tma<R, KC, NTH, RUNS>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
                                          cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
         } else {
-          cluster_load<R, KC, NTH>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
+          cluster_load<R, KC, NTH, RUNS>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
         }
       }
       if (!TMA) cpa_commit();
@@ -767,10 +767,10 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
     const double s0 = rscale[2 * r], s1 = rscale[2 * r + 1];
     if (s0 == 0.0) {   // a non-finite row has zero digits
 #pragma unroll
-      for (int e = 0; e < 16; ++e) v[e] = 0.0;
+      for (int e = 0; e < 4 * RUNS; ++e) v[e] = 0.0;
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < RUNS; ++j) {
       uint32_t wd[S];
       const double x[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
       digit_words<S>(x, s0, s1, wd);
@@ -807,11 +807,11 @@ __global__ void __launch_bounds__(NTH, CL_NTH / NTH) ozaki_cluster_kernel(const 
   cluster_wait();
 }
 
-template <int S, bool TMA, int R, int KC, int NTH>
+template <int S, bool TMA, int R, int KC, int NTH, int RUNS>
 cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, const PlaneArgs& a0, int32_t* e0,
                               long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st) {
-  constexpr int SMEM = ClShape<R, KC, NTH>::template smem_bytes<S>();
-  auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH>;
+  constexpr int SMEM = ClShape<R, KC, NTH, RUNS>::template smem_bytes<S>();
+  auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH, RUNS>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
@@ -865,7 +865,7 @@ bool slicer_map(CUtensorMap* m, const PlaneArgs& a, int R) {
   return make_tiled_map(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, a.X0, dims, strides, box, 0);
 }
 
-template <int S, int R, int KC, int NTH = CL_NTH>
+template <int S, int R, int KC, int NTH = CL_NTH, int RUNS = 4>
 cudaError_t launch_cluster_shape(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
                                  cudaStream_t st) {
   const int CS = (int)((a0.Kp + KC - 1) / KC);
@@ -875,8 +875,8 @@ cudaError_t launch_cluster_shape(const PlaneArgs& a0, int32_t* e0, const PlaneAr
   CUtensorMap tm0, tm1;
   const bool tma = slicer_map(&tm0, a0, R) && (!two || slicer_map(&tm1, a1, R));
   if (!two) tm1 = tm0;
-  if (tma) return launch_cluster_st<S, true, R, KC, NTH>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
-  return launch_cluster_st<S, false, R, KC, NTH>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  if (tma) return launch_cluster_st<S, true, R, KC, NTH, RUNS>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
+  return launch_cluster_st<S, false, R, KC, NTH, RUNS>(tm0, tm1, a0, e0, n0, a1, e1, n1, CS, st);
 }
 
 // Item shape: 16 x 512 (configuration 3, the default), 32 x 256 (2) or 8 x 1024 (4), all with
@@ -886,10 +886,13 @@ template <int S>
 cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two, int shape,
                              cudaStream_t st) {
   if (shape == 5) return launch_cluster_shape<S, 16, 256, 256>(a0, e0, a1, e1, two, st);
+  if (shape == 6) return launch_cluster_shape<S, 4, 256, 128, 2>(a0, e0, a1, e1, two, st);
   if (shape == 2) return launch_cluster_shape<S, 32, 256>(a0, e0, a1, e1, two, st);
   if (shape == 4) return launch_cluster_shape<S, 8, 1024>(a0, e0, a1, e1, two, st);
   return launch_cluster_shape<S, 16, 512>(a0, e0, a1, e1, two, st);
 }
+
+}  // namespace
 
 // K up to 2048 with clusters of at most 8 CTAs of 256 k (at most 4 of 512 k)
 bool cluster_kernel_fits(const PlaneArgs& a) { return a.K <= 2048 && a.Kp <= 2048; }
@@ -911,6 +914,8 @@ cudaError_t launch_ozaki_cluster(const PlaneArgs& a0, int32_t* e0, const PlaneAr
   note_launch();
   return e;
 }
+
+namespace {
 
 dim3 grid_of(const PlaneArgs& a) {
   return dim3((unsigned)((a.rows + RT - 1) / RT), (unsigned)a.batch);

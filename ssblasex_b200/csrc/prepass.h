@@ -30,5 +30,10 @@ cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cu
 // both operands of one call: two launches in all (exponents of both, then digits of both)
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* exps_a, const PlaneArgs& b, int32_t* exps_b,
                                     int slices, cudaStream_t st);
+// the one-pass cluster slicer with a given item shape (the SSBLAS_PATH_OZAKI_SLICER configurations
+// 2-6) for one or two operands, k <= 2048
+cudaError_t launch_ozaki_cluster(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& a1, int32_t* e1, bool two,
+                                 int slices, int shape, cudaStream_t st);
+bool cluster_kernel_fits(const PlaneArgs& a);
 
 }  // namespace ssb

@@ -206,8 +206,8 @@ SplitPlan ozaki_split_plan(bool allow_split) {
 }
 
 template <class Cfg>
-cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
-                           long Kp, bool allow_split, cudaStream_t st) {
+cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* exa,
+                           const int32_t* exb, long Kp, bool allow_split, cudaStream_t st) {
   const long sa = d.m * Kp, sb = d.n * Kp;
   CUtensorMap ta, tb;
   if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, Cfg::KB, 128, S,
@@ -216,28 +216,29 @@ cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const in
                 Cfg::KB))
     return cudaErrorNotSupported;
   tc::Params prm = base_params(d);
-  prm.exp_a = ex;
-  prm.exp_b = ex + d.m * d.batch;
+  prm.exp_a = exa;
+  prm.exp_b = exb;
   prm.exp_shift = -12;
   note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
   return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split));
 }
 
-cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex, long Kp,
-                       bool allow_split, cudaStream_t st) {
+// exa: exponents of the rows of op(A), [batch][m]; exb: of the columns of op(B), [batch][n]
+cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* exa,
+                       const int32_t* exb, long Kp, bool allow_split, cudaStream_t st) {
   switch (S) {
-    case 3: return ozaki_gemm_cfg<OzCfg<3>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
-    case 4: return ozaki_gemm_cfg<OzCfg<4>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
-    case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
-    case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+    case 3: return ozaki_gemm_cfg<OzCfg<3>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+    case 4: return ozaki_gemm_cfg<OzCfg<4>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+    case 5: return ozaki_gemm_cfg<OzCfg<5>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+    case 6: return ozaki_gemm_cfg<OzCfg<6>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
     case 7: {
       // 64-byte K stages won every bucket the autotuner measured, so they are the default
       const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 1);
-      if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, ex, Kp, allow_split, st);
-      if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, ex, Kp, allow_split, st);
-      return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+      if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
     }
-    default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, ex, Kp, allow_split, st);
+    default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
   }
 }
 
@@ -297,6 +298,99 @@ cudaError_t launch_i8_tcgen05(const BatchDesc& d, cudaStream_t st) {
                    : run_gemm<CfgI8N256>(ta, tb, prm, st, "i8_gemm", plan);
 }
 
+namespace {
+
+// The instances [b0, b0 + nb) of an operand's slicing arguments.
+PlaneArgs plane_chunk(const PlaneArgs& x, long b0, long nb) {
+  PlaneArgs c = x;
+  c.X = x.X + b0;
+  c.batch = nb;
+  c.out = (int8_t*)x.out + b0 * x.batch_stride;
+  if (x.X0) c.X0 = (const uint8_t*)x.X0 + b0 * x.xstride;
+  return c;
+}
+
+// Chunks of the slicing / GEMM pipeline (1 = none): a tuned or forced count
+// (SSBLAS_PATH_OZAKI_PIPELINE); automatic means none. Measured on 32 x 1024^3: the slim slicer
+// beside the GEMM slows the GEMM by a third (0.65 -> 0.87 ms for the batch) -- the GEMM streams its
+// operands through shared memory near that memory's bandwidth, and the slicer needs the same --
+// so the 4-chunk pipeline took 1.15 ms against 0.89 ms for slicing then multiplying.
+int ozaki_pipeline_chunks(const BatchDesc& d, const PlaneArgs& a) {
+  if (!cluster_kernel_fits(a) || d.batch < 2) return 1;
+  int c = choose_config(SSBLAS_PATH_OZAKI_PIPELINE, d.m, d.n, d.k, d.batch, 0);
+  if (c == 0) c = 1;
+  if (c > d.batch) c = (int)d.batch;
+  if (c > 8) c = 8;
+  return c < 1 ? 1 : c;
+}
+
+// Side stream and events of the pipeline, one set per device, created on first use.
+struct PipeRes {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t ready[8] = {};
+};
+cudaError_t pipe_res(PipeRes** out) {
+  static PipeRes res[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  PipeRes& r = res[dev];
+  if (!r.side) {
+    if ((e = cudaStreamCreateWithFlags(&r.side, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+    for (auto& ev : r.ready)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  *out = &r;
+  return cudaSuccess;
+}
+
+// Slicing of chunk c + 1 overlaps the GEMM of chunk c: chunk 0 is sliced on the caller's stream by
+// the full-size one-pass kernel; then a side stream slices chunks 1.. with the slim kernel (4 rows
+// x 256 k per 128-thread CTA, 80 registers, 25 KB of shared memory), which fits on an SM beside a
+// GEMM CTA, so it uses the issue slots and memory bandwidth the tensor-bound GEMM leaves free.
+// GEMM chunk c waits for its chunk's event; the last wait joins the side stream back into the
+// caller's.
+cudaError_t ozaki_pipelined(const BatchDesc& d, int S, const PlaneArgs& a, const PlaneArgs& b, int8_t* pa,
+                            int8_t* pb, int32_t* ex, long Kp, int chunks, cudaStream_t st) {
+  PipeRes* r = nullptr;
+  cudaError_t e = pipe_res(&r);
+  if (e != cudaSuccess) return e;
+  int32_t* exa = ex;
+  int32_t* exb = ex + d.m * d.batch;
+  auto lo = [&](int c) { return d.batch * c / chunks; };
+  {
+    const long b0 = lo(0), nb = lo(1) - b0;
+    if ((e = launch_ozaki_slice_pair(plane_chunk(a, b0, nb), exa + b0 * d.m, plane_chunk(b, b0, nb),
+                                     exb + b0 * d.n, S, st)) != cudaSuccess)
+      return e;
+  }
+  if ((e = cudaEventRecord(r->fork, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(r->side, r->fork, 0)) != cudaSuccess) return e;
+  for (int c = 1; c < chunks; ++c) {
+    const long b0 = lo(c), nb = lo(c + 1) - b0;
+    if ((e = launch_ozaki_cluster(plane_chunk(a, b0, nb), exa + b0 * d.m, plane_chunk(b, b0, nb), exb + b0 * d.n,
+                                  true, S, 6, r->side)) != cudaSuccess)
+      return e;
+    if ((e = cudaEventRecord(r->ready[c], r->side)) != cudaSuccess) return e;
+  }
+  for (int c = 0; c < chunks; ++c) {
+    const long b0 = lo(c), nb = lo(c + 1) - b0;
+    if (c > 0 && (e = cudaStreamWaitEvent(st, r->ready[c], 0)) != cudaSuccess) return e;
+    BatchDesc dc = d;
+    dc.batch = nb;
+    dc.C = d.C + b0;
+    if ((e = ozaki_gemm(dc, S, pa + b0 * a.batch_stride, pb + b0 * b.batch_stride, exa + b0 * d.m,
+                        exb + b0 * d.n, Kp, false, st)) != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
 cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   // int32 accumulation stays exact while (pairs per level) * k * 2^14 < 2^31: longer k is cut into
@@ -317,8 +411,12 @@ cudaError_t launch_ozaki_f64(const BatchDesc& d, int slices, cudaStream_t st) {
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * S};
   if (d.A0 && (d.batch == 1 || d.strideA > 0)) { a.X0 = d.A0; a.xstride = d.batch == 1 ? 16 : d.strideA; }
   if (d.B0 && (d.batch == 1 || d.strideB > 0)) { b.X0 = d.B0; b.xstride = d.batch == 1 ? 16 : d.strideB; }
-  if ((e = launch_ozaki_slice_pair(a, ex, b, ex + d.m * d.batch, S, st)) != cudaSuccess) return e;
-  return ozaki_gemm(d, S, pa, pb, ex, Kp, true, st);
+  const int chunks = ozaki_pipeline_chunks(d, a);
+  if (chunks <= 1) {
+    if ((e = launch_ozaki_slice_pair(a, ex, b, ex + d.m * d.batch, S, st)) != cudaSuccess) return e;
+    return ozaki_gemm(d, S, pa, pb, ex, ex + d.m * d.batch, Kp, true, st);
+  }
+  return ozaki_pipelined(d, S, a, b, pa, pb, ex, Kp, chunks, st);
 }
 
 cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, const int8_t* pb, const int32_t* ex,
@@ -326,7 +424,7 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, co
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (S < 3 || S > 8) return cudaErrorInvalidValue;
   if (d.k > kOzakiMaxPieceK) return cudaErrorNotSupported;   // splitting would need workspace
-  return ozaki_gemm(d, S, pa, pb, ex, Kp, false, st);
+  return ozaki_gemm(d, S, pa, pb, ex, ex + d.m * d.batch, Kp, false, st);
 }
 
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {

@@ -102,7 +102,7 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
-@pytest.mark.parametrize("form", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("ta,tb,m,n,k,batch", [
     (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 (4) CTAs, K contiguous, 16-byte loads
     (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2 (1), odd ld (8-byte loads)
@@ -115,10 +115,11 @@ def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
     """Every slicing kernel (the two-pass form 1 -- row maxima per (32 rows, 256 k) part, then
     digits per (32 rows, 128 k) chunk -- and the one-pass item shapes: form 2 = 32 rows x 256 k
     per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k, 5 = 16 rows x 256 k with two 256-thread
-    CTAs per SM) produces the planes the CPU restatement produces: the product is bit-exact
-    against oracle.ozaki_f64 whichever kernel sliced the operands."""
+    CTAs per SM, 6 = 4 rows x 256 k per 128-thread CTA, the slim form that runs beside the GEMM)
+    produces the planes the CPU restatement produces: the product is bit-exact against
+    oracle.ozaki_f64 whichever kernel sliced the operands."""
     from ssblasex_b200 import workloads as W
-    if k > 2048 and form in (2, 4, 5):
+    if k > 2048 and form in (2, 4, 5, 6):
         pytest.skip("the one-pass forms apply to k <= 2048")
     S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
     S.set_kernel_config("ozaki_slicer", form)
@@ -399,3 +400,31 @@ def test_ozaki_level_sum_beyond_int32(S):
     assert st == -1
     np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
     np.testing.assert_allclose(p.c_view(C, 0), 600000 * 0.99 * -0.97, rtol=1e-12)
+
+
+# ------------------------------------------------------------------------- slicing / GEMM pipeline
+@pytest.mark.parametrize("chunks", [2, 3, 4])
+@pytest.mark.parametrize("ta,tb,m,n,k,batch", [
+    (0, 1, 300, 200, 1030, 7),    # uneven chunks, rows contiguous, ragged tiles
+    (1, 0, 256, 130, 512, 9),     # k contiguous (TMA boxes along k)
+])
+def test_ozaki_pipeline(S, chunks, ta, tb, m, n, k, batch):
+    """The batch cut into chunks, the slicing of chunk c + 1 (slim kernel, side stream) beside the
+    GEMM of chunk c: bit-exact against the CPU restatement, and equal to the unpipelined result."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    p = W.make_problem("f64", ta, tb, m, n, k, batch, 0.5, -1.5, seed=chunks + m, dist="expspread")
+    S.set_kernel_config("ozaki_pipeline", chunks)
+    try:
+        C = run(p)
+        C_again = run(p)
+        S.set_kernel_config("ozaki_pipeline", 1)
+        C_plain = run(p)
+    finally:
+        S.set_kernel_config("ozaki_pipeline", -1)
+    assert S.last_run_info()["path"] == "ozaki_tcgen05"
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+    np.testing.assert_array_equal(C_again.view(np.uint64), C_o.view(np.uint64))
+    np.testing.assert_array_equal(C_plain.view(np.uint64), C_o.view(np.uint64))

@@ -132,8 +132,8 @@ def peaks():
 
 # DRAM traffic per launch of the dominant kernel (dram__bytes_read.sum + dram__bytes_write.sum from
 # one ncu capture). The 32-instance launch is too large to capture under ncu, so an 8-instance
-# launch of the same kernel was captured (156 MB) and scaled by the instances it processes.
-NCU_TRAFFIC = {("f64_batch32_1024", "ozaki"): 156.0e6 * 4}
+# launch of the same kernel was captured (153 MB) and scaled by the instances it processes.
+NCU_TRAFFIC = {("f64_batch32_1024", "ozaki"): 153.1e6 * 4}
 
 
 def cpu_threads():

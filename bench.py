@@ -193,7 +193,8 @@ def run_reference_arm(args):
     os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
     p = W.workload(args.workload)
     sample = {"f64_batch32_1024": 2, "i8_batch512_512": 4, "fp32_batch64_128": 64,
-              "fp32_batch4096_64": 512, "i8_batch8_4096": 1}[args.workload]
+              "fp32_batch4096_64": 512, "i8_batch8_4096": 1, "f64_batch2_256_8192": 1,
+              "i8_batch64_512_nn": 4}[args.workload]
     ts, kind = reference_timing(p, args.steps, args.warmup, sample)
     flops = 2.0 * p.m * p.n * p.k * sample
     t = float(np.mean(ts))
@@ -461,7 +462,7 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         sample = {"f64_batch32_1024": 2, "i8_batch512_512": 4, "fp32_batch64_128": 64, "fp32_batch4096_64": 512,
-                  "i8_batch8_4096": 1}[args.workload]
+                  "i8_batch8_4096": 1, "f64_batch2_256_8192": 1, "i8_batch64_512_nn": 4}[args.workload]
         ts, kind = reference_timing(p, 3, 1, sample)
         fl = 2.0 * p.m * p.n * p.k * sample
         cpu = {"value": fl / min(ts) / 1e12, "unit": "TFLOP/s", "cores": int(os.environ["OMP_NUM_THREADS"]),

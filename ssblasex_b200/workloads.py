@@ -174,6 +174,13 @@ WORKLOADS = {
     # (the 512^3 beta=1 batch is bound by HBM bandwidth)
     "i8_batch8_4096": dict(row="i8", transa=OP_T, transb=OP_N, m=4096, n=4096, k=4096, batch=8,
                            alpha=1, beta=0, lda=4096, ldb=4096, ldc=4096, seed=4),
+    # not configurations of the task either: few output tiles and a long k (two-pass slicing and
+    # split-K of the Ozaki path), and int8 in the N/N layout (the pack pre-pass ahead of the
+    # tensor-core kernel)
+    "f64_batch2_256_8192": dict(row="f64", transa=OP_T, transb=OP_N, m=256, n=256, k=8192, batch=2,
+                                alpha=1.0, beta=0.0, seed=5, dist="expspread"),
+    "i8_batch64_512_nn": dict(row="i8", transa=OP_N, transb=OP_N, m=512, n=512, k=512, batch=64,
+                              alpha=1, beta=1, seed=6),
 }
 
 

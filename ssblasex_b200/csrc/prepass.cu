@@ -37,6 +37,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstring>
+
 #include "internal.h"
 #include "ozaki_digits.cuh"
 #include "prepass.h"
@@ -96,24 +98,78 @@ __device__ __forceinline__ void write_out(const uint8_t* st, uint8_t* out, long 
   write_rows<P, KT * BPE>(st, out, plane_stride, rows, Kp_bytes, row0, kbyte0);
 }
 
-__global__ void __launch_bounds__(NTH) pack_i8_kernel(PlaneArgs a) {
-  __shared__ __align__(16) uint8_t st[RT * (KT + 4)];
-  const long b = blockIdx.y;
-  const long row0 = (long)blockIdx.x * RT;
+// int8 -> K-major plane. A CTA takes 128 rows x 128 k of one instance (blocks: k tile fastest,
+// then row tile, then instance). K contiguous: already K-major, each thread copies 16-byte row
+// segments to the plane's pitch. Rows contiguous (element (r, k) at X[r + k*ld]): each thread
+// loads four 4 x 4 byte blocks as 32-bit words -- lane l of a warp takes rows 4l .. 4l+3, so one
+// load instruction reads 128 contiguous bytes -- transposes them in registers (byte permutes),
+// stages the 4-byte k runs of its rows in shared memory, and the CTA writes 16-byte row segments.
+// Positions past K (up to Kp) get zero bytes.
+constexpr int PKR = 128, PKK = 128;          // rows and k per CTA
+constexpr int PKP = PKK + 4;                 // staged row pitch (bytes)
+__global__ void __launch_bounds__(NTH) pack_i8_kernel(PlaneArgs a, long ktiles, long rtiles) {
+  __shared__ __align__(16) uint8_t st[PKR * PKP];
+  const long blk = blockIdx.x;
+  const long kt = blk % ktiles, rt = (blk / ktiles) % rtiles, b = blk / (ktiles * rtiles);
+  const long r0 = rt * PKR, k0 = kt * PKK;
   const int8_t* X = (const int8_t*)a.X[b];
   uint8_t* out = (uint8_t*)a.out + b * a.batch_stride;
-  for (long k0 = 0; k0 < a.K; k0 += KT) {
-    int8_t v[PER];
-    load_regs<int8_t>(v, X, a.rows, a.K, a.ld, a.kcontig, row0, k0);
+  const int t = threadIdx.x;
+  if (a.kcontig) {
+    const bool vec = ((uintptr_t)X % 16) == 0 && a.ld % 16 == 0;
 #pragma unroll
-    for (int e = 0; e < PER; ++e) {
-      int r, kk;
-      tile_coord(a.kcontig, e, r, kk);
-      st[r * (KT + 4) + kk] = (uint8_t)v[e];
+    for (int q = 0; q < PKR * PKK / 16 / NTH; ++q) {
+      const int id = t + q * NTH, r = id / (PKK / 16), c = id % (PKK / 16);
+      const long gr = r0 + r, gk = k0 + 16 * c;
+      if (gr >= a.rows || gk >= a.Kp) continue;
+      uint4 w = make_uint4(0u, 0u, 0u, 0u);
+      const int8_t* src = X + gr * a.ld + gk;
+      if (vec && gk + 16 <= a.K) {
+        w = __ldg((const uint4*)src);
+      } else {
+        uint8_t by[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) by[i] = gk + i < a.K ? (uint8_t)__ldg(src + i) : 0;
+        memcpy(&w, by, 16);
+      }
+      *(uint4*)(out + gr * a.Kp + gk) = w;
     }
-    __syncthreads();
-    write_out<1, 1>(st, out, a.plane_stride, a.rows, a.Kp, row0, k0);
-    __syncthreads();
+    return;
+  }
+  const bool vec = ((uintptr_t)X % 4) == 0 && a.ld % 4 == 0;
+  const int rg = t % 32;                       // rows 4 rg .. 4 rg + 3 of the tile
+  const long gr = r0 + 4 * rg;
+#pragma unroll
+  for (int q = 0; q < PKK / 4 / (NTH / 32); ++q) {
+    const int kg = t / 32 + (NTH / 32) * q;    // k 4 kg .. 4 kg + 3 of the tile
+    uint32_t w[4], o[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const long gk = k0 + 4 * kg + i;
+      const int8_t* src = X + gr + gk * a.ld;
+      w[i] = 0u;
+      if (gk < a.K) {
+        if (vec && gr + 4 <= a.rows) {
+          w[i] = __ldg((const uint32_t*)src);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (gr + j < a.rows) w[i] |= (uint32_t)(uint8_t)__ldg(src + j) << (8 * j);
+        }
+      }
+    }
+    byte_transpose4(w, o);                     // o[j]: k 4 kg .. 4 kg + 3 of row 4 rg + j
+#pragma unroll
+    for (int j = 0; j < 4; ++j) *(uint32_t*)(st + (4 * rg + j) * PKP + 4 * kg) = o[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PKR * PKK / 16 / NTH; ++q) {
+    const int id = t + q * NTH, r = id / (PKK / 16), c = id % (PKK / 16);
+    const long gr2 = r0 + r, gk = k0 + 16 * c;
+    if (gr2 >= a.rows || gk >= a.Kp) continue;
+    const uint32_t* src = (const uint32_t*)(st + r * PKP + 16 * c);
+    *(uint4*)(out + gr2 * a.Kp + gk) = make_uint4(src[0], src[1], src[2], src[3]);
   }
 }
 
@@ -915,17 +971,13 @@ cudaError_t launch_ozaki_cluster(const PlaneArgs& a0, int32_t* e0, const PlaneAr
   return e;
 }
 
-namespace {
-
-dim3 grid_of(const PlaneArgs& a) {
-  return dim3((unsigned)((a.rows + RT - 1) / RT), (unsigned)a.batch);
-}
-
-}  // namespace
 
 cudaError_t launch_pack_i8(const PlaneArgs& a, cudaStream_t st) {
+  const long ktiles = (a.Kp + PKK - 1) / PKK, rtiles = (a.rows + PKR - 1) / PKR;
+  const long blocks = ktiles * rtiles * a.batch;
+  if (blocks >= (1L << 31)) return cudaErrorInvalidValue;
   ProfScope prof("pack_i8", st);
-  pack_i8_kernel<<<grid_of(a), NTH, 0, st>>>(a);
+  pack_i8_kernel<<<(unsigned)blocks, NTH, 0, st>>>(a, ktiles, rtiles);
   note_launch();
   return cudaGetLastError();
 }

@@ -50,6 +50,22 @@ def test_i8_direct_tn(S, shape):
     np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
 
 
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("m,n,k", [(130, 201, 300), (257, 64, 129)])
+def test_i8_pack_aligned(S, ta, tb, m, n, k):
+    """The pack pre-pass with 4-byte aligned instances and leading dimensions (word loads of
+    4 x 4 byte blocks, transposed in registers) and row counts that leave a partial group of 4
+    rows: bit-exact."""
+    from ssblasex_b200 import workloads as W
+    al = lambda x: -(-x // 16) * 16
+    lda = al(m if ta == 0 else k)
+    ldb = al(k if tb == 0 else n)
+    p = W.make_problem("i8", ta, tb, m, n, k, 3, 2, -1, lda=lda, ldb=ldb, ldc=m + 3, seed=m + 3 * ta + tb)
+    C = run(p)
+    assert S.last_run_info()["path"] == "i8_tcgen05"
+    np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+
+
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 1), (1, 0)])
 def test_i8_packed_layouts(S, ta, tb):
     from ssblasex_b200 import workloads as W

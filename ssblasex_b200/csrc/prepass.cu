@@ -28,7 +28,11 @@
 //               distributed shared memory and write the digits; tiles arrive by TMA (equally
 //               spaced instances) or cp.async two items ahead, digit rows leave by bulk copies.
 //               Each operand is read once.
-//   K > 2048    ozaki_rowexp_kernel (row exponents) then ozaki_digits_kernel (one CTA per
+//   K > 2048    ozaki_rowmax_kernel (row maxima of |x| per 32 rows x 256 k part, combined by
+//               atomicMax) then ozaki_cluster_kernel in its BITS form (clusters of one CTA,
+//               persistent over 16 rows x 512 k slabs, exponents from the maxima); or (the
+//               allocation-free entry point, which has no room for the maxima)
+//               ozaki_rowexp_kernel (row exponents) then ozaki_digits_kernel (one CTA per
 //               32 rows x 128 k chunk) when there are enough rows to fill the GPU, else
 //               ozaki_slice_kernel (both passes inside one CTA per 32 rows).
 // All forms pack the 4 digits of 4 consecutive k into one word per plane with a 4 x 4 byte
@@ -677,11 +681,13 @@ __device__ __forceinline__ void cluster_tma(double* stage, uint64_t* bar, const 
   }
 }
 
-template <int S, bool TMA, int R, int KC, int NTH, int RUNS>
+template <int S, bool TMA, int R, int KC, int NTH, int RUNS, bool BITS>
 __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_cluster_kernel(const __grid_constant__ CUtensorMap tm0,
                                                                   const __grid_constant__ CUtensorMap tm1, PlaneArgs a0,
                                                                   int32_t* e0, long n0, PlaneArgs a1, int32_t* e1,
-                                                                  long n_items, int CS, int* err) {
+                                                                  long n_items, int CS, int* err,
+                                                                  const unsigned long long* bits0,
+                                                                  const unsigned long long* bits1, int KB) {
   using Sh = ClShape<R, KC, NTH, RUNS>;
   constexpr int NC = Sh::NC, LR = Sh::LR, RG = Sh::RG, NW = Sh::NW, PW = Sh::PW, TILE = Sh::TILE;
   extern __shared__ __align__(16) uint8_t dyn[];
@@ -694,10 +700,21 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
 
   const int rank = (int)(blockIdx.x % CS);           // rank in the cluster (cluster dims CS x 1 x 1)
   const long cluster = blockIdx.x / CS, nclusters = gridDim.x / CS;
-  const long kbase = (long)rank * KC;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
   const uint32_t bpi0 = (uint32_t)((a0.rows + R - 1) / R);
   const uint32_t bpi1 = (uint32_t)((a1.rows + R - 1) / R);
+  // item -> (operand, instance, first row) and the first k of this CTA's slab: the cluster rank's
+  // KC-wide slab, or with BITS (clusters of one CTA, items = row blocks x KB slabs) the item's own
+  auto item_at = [&](long item, long& kbase) -> ClusterItem {
+    if constexpr (BITS) {
+      const uint32_t rb = (uint32_t)item / (uint32_t)KB;
+      kbase = (long)((uint32_t)item - rb * (uint32_t)KB) * KC;
+      return cluster_item<R>(rb, n0, bpi0, bpi1);
+    } else {
+      kbase = (long)rank * KC;
+      return cluster_item<R>(item, n0, bpi0, bpi1);
+    }
+  };
 
   if (TMA && t == 0) {
     ptx::mbar_init(ptx::smem_u32(&full[0]), 1);
@@ -710,7 +727,8 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
   for (int s = 0; s < 2; ++s) {
     const long item = cluster + s * nclusters;
     if (item < n_items) {
-      const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
+      long kbase;
+      const ClusterItem ci = item_at(item, kbase);
       if (TMA) {
         if (t == 0) cluster_tma<R, KC, NTH, RUNS>(stages + s * TILE, &full[s], ci.second ? &tm1 : &tm0,
                                        ci.second ? a1.kcontig : a0.kcontig, ci, kbase);
@@ -724,7 +742,8 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
   long iter = 0;
   for (long item = cluster; item < n_items; item += nclusters, ++iter) {
     const int s = (int)(iter & 1);
-    const ClusterItem ci = cluster_item<R>(item, n0, bpi0, bpi1);
+    long kbase;
+    const ClusterItem ci = item_at(item, kbase);
     const PlaneArgs a = ci.second ? a1 : a0;
     int32_t* __restrict__ exps = ci.second ? e1 : e0;
     const int r = a.kcontig ? t / NC : lane % LR + LR * (warp % RG);
@@ -755,52 +774,63 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 4 * NC * j + i) * R + r];
     }
 
-    // partial row maxima of this CTA's K range (bit patterns of |x|; the shared-memory buffers
-    // hold them as doubles, bit for bit)
-    unsigned long long mx = 0;
-#pragma unroll
-    for (int e = 0; e < 4 * RUNS; ++e) mx = max_u64(mx, abs_bits(v[e]));
-    double* pm = pmax + s * R;
-    auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
-    auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
-    if (a.kcontig && NC <= 32) {
-      // the NC threads of row r are consecutive lanes
-#pragma unroll
-      for (int off = 1; off < NC; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (c == 0) pm[r] = as_d(mx);
-    } else if (a.kcontig) {
-      // row r spans the NC / 32 warps r * NC / 32 ..
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (lane == 0) red[warp] = as_d(mx);
-      __syncthreads();
+    if constexpr (BITS) {
+      // the row maxima of the whole K range come from the K-parallel pass
       if (t < R) {
-        unsigned long long m2 = as_u(red[t * (NC / 32)]);
-        for (int w = 1; w < NC / 32; ++w) m2 = max_u64(m2, as_u(red[t * (NC / 32) + w]));
-        pm[t] = as_d(m2);
+        const long gr = ci.row0 + t;
+        const unsigned long long m2 = gr < a.rows ? (ci.second ? bits1 : bits0)[ci.b * a.rows + gr] : 0ull;
+        const int e = row_exponent(m2);
+        if (kbase == 0 && gr < a.rows) exps[ci.b * a.rows + gr] = e;
+        row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
       }
     } else {
-      // row r: lanes with lane % LR == r % LR of the NW warps with w % RG == r / LR
+      // partial row maxima of this CTA's K range (bit patterns of |x|; the shared-memory buffers
+      // hold them as doubles, bit for bit)
+      unsigned long long mx = 0;
 #pragma unroll
-      for (int off = LR; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (lane < LR) red[(warp / RG) * 32 + r] = as_d(mx);
-      __syncthreads();
-      if (t < R) {
-        unsigned long long m2 = as_u(red[t]);
+      for (int e = 0; e < 4 * RUNS; ++e) mx = max_u64(mx, abs_bits(v[e]));
+      double* pm = pmax + s * R;
+      auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
+      auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
+      if (a.kcontig && NC <= 32) {
+        // the NC threads of row r are consecutive lanes
 #pragma unroll
-        for (int w = 1; w < NW; ++w) m2 = max_u64(m2, as_u(red[w * 32 + t]));
-        pm[t] = as_d(m2);
+        for (int off = 1; off < NC; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (c == 0) pm[r] = as_d(mx);
+      } else if (a.kcontig) {
+        // row r spans the NC / 32 warps r * NC / 32 ..
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane == 0) red[warp] = as_d(mx);
+        __syncthreads();
+        if (t < R) {
+          unsigned long long m2 = as_u(red[t * (NC / 32)]);
+          for (int w = 1; w < NC / 32; ++w) m2 = max_u64(m2, as_u(red[t * (NC / 32) + w]));
+          pm[t] = as_d(m2);
+        }
+      } else {
+        // row r: lanes with lane % LR == r % LR of the NW warps with w % RG == r / LR
+#pragma unroll
+        for (int off = LR; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane < LR) red[(warp / RG) * 32 + r] = as_d(mx);
+        __syncthreads();
+        if (t < R) {
+          unsigned long long m2 = as_u(red[t]);
+#pragma unroll
+          for (int w = 1; w < NW; ++w) m2 = max_u64(m2, as_u(red[w * 32 + t]));
+          pm[t] = as_d(m2);
+        }
       }
-    }
-    cluster_arrive();   // every CTA's pmax[s] is visible after the wait
-    cluster_wait();
-    if (t < R) {
-      unsigned long long m2 = 0;
-      for (int q = 0; q < CS; ++q) m2 = max_u64(m2, as_u(ld_cluster_f64(pm + t, (uint32_t)q)));
-      const int e = row_exponent(m2);
-      if (rank == 0 && ci.row0 + t < a.rows) exps[ci.b * a.rows + ci.row0 + t] = e;
-      // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
-      row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
+      cluster_arrive();   // every CTA's pmax[s] is visible after the wait
+      cluster_wait();
+      if (t < R) {
+        unsigned long long m2 = 0;
+        for (int q = 0; q < CS; ++q) m2 = max_u64(m2, as_u(ld_cluster_f64(pm + t, (uint32_t)q)));
+        const int e = row_exponent(m2);
+        if (rank == 0 && ci.row0 + t < a.rows) exps[ci.b * a.rows + ci.row0 + t] = e;
+        // x * 2^(8S-2-e) as two exact power-of-two factors (each within the double range)
+        row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
+      }
     }
     __syncthreads();   // rscale visible; stage s fully read into registers
 
@@ -808,12 +838,13 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     {
       const long nxt = item + 2 * nclusters;
       if (nxt < n_items) {
-        const ClusterItem cn = cluster_item<R>(nxt, n0, bpi0, bpi1);
+        long kn;
+        const ClusterItem cn = item_at(nxt, kn);
         if (TMA) {
           if (t == 0) cluster_tma<R, KC, NTH, RUNS>(stages + s * TILE, &full[s], cn.second ? &tm1 : &tm0,
-                                         cn.second ? a1.kcontig : a0.kcontig, cn, kbase);
+                                         cn.second ? a1.kcontig : a0.kcontig, cn, kn);
         } else {
-          cluster_load<R, KC, NTH, RUNS>(stages + s * TILE, cn.second ? a1 : a0, cn, kbase);
+          cluster_load<R, KC, NTH, RUNS>(stages + s * TILE, cn.second ? a1 : a0, cn, kn);
         }
       }
       if (!TMA) cpa_commit();
@@ -863,11 +894,14 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
   cluster_wait();
 }
 
-template <int S, bool TMA, int R, int KC, int NTH, int RUNS>
+// BITS: row maxima in bits0/bits1, CS = 1 and KB k slabs per row block
+template <int S, bool TMA, int R, int KC, int NTH, int RUNS, bool BITS = false>
 cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, const PlaneArgs& a0, int32_t* e0,
-                              long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st) {
+                              long n0, const PlaneArgs& a1, int32_t* e1, long n1, int CS, cudaStream_t st,
+                              const unsigned long long* bits0 = nullptr, const unsigned long long* bits1 = nullptr,
+                              int KB = 1) {
   constexpr int SMEM = ClShape<R, KC, NTH, RUNS>::template smem_bytes<S>();
-  auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH, RUNS>;
+  auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH, RUNS, BITS>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
@@ -897,10 +931,11 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
     }
     max_clusters[CS] = nc > 0 ? nc : 1;
   }
-  const long n_items = n0 + n1;
+  const long n_items = (n0 + n1) * KB;
   const long nclusters = n_items < max_clusters[CS] ? n_items : max_clusters[CS];
   cfg.gridDim = dim3((unsigned)(nclusters * CS), 1, 1);
-  return cudaLaunchKernelEx(&cfg, kern, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS, device_error_flag());
+  return cudaLaunchKernelEx(&cfg, kern, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS, device_error_flag(), bits0,
+                            bits1, KB);
 }
 
 // 3-D map (innermost dimension first) over an equally spaced fp64 operand with an R x 256 box.
@@ -946,6 +981,24 @@ cudaError_t launch_cluster_s(const PlaneArgs& a0, int32_t* e0, const PlaneArgs& 
   if (shape == 2) return launch_cluster_shape<S, 32, 256>(a0, e0, a1, e1, two, st);
   if (shape == 4) return launch_cluster_shape<S, 8, 1024>(a0, e0, a1, e1, two, st);
   return launch_cluster_shape<S, 16, 512>(a0, e0, a1, e1, two, st);
+}
+
+// Digits of one or two operands (same Kp) whose row maxima are in bits0/bits1: persistent CTAs
+// over (16 rows, 512 k) items, tiles by TMA or cp.async two items ahead, no cluster exchange.
+template <int S>
+cudaError_t launch_digits_from_bits(const PlaneArgs& a0, int32_t* e0, const unsigned long long* bits0,
+                                    const PlaneArgs& a1, int32_t* e1, const unsigned long long* bits1,
+                                    cudaStream_t st) {
+  constexpr int R = 16, KC = 512;
+  const long KB = (a0.Kp + KC - 1) / KC;
+  const long n0 = (a0.rows + R - 1) / R * a0.batch, n1 = (a1.rows + R - 1) / R * a1.batch;
+  if ((n0 + n1) * KB >= (1L << 31)) return cudaErrorInvalidValue;
+  CUtensorMap tm0, tm1;
+  if (slicer_map(&tm0, a0, R) && slicer_map(&tm1, a1, R))
+    return launch_cluster_st<S, true, R, KC, CL_NTH, 4, true>(tm0, tm1, a0, e0, n0, a1, e1, n1, 1, st, bits0, bits1,
+                                                             (int)KB);
+  return launch_cluster_st<S, false, R, KC, CL_NTH, 4, true>(tm0, tm1, a0, e0, n0, a1, e1, n1, 1, st, bits0, bits1,
+                                                            (int)KB);
 }
 
 }  // namespace
@@ -1000,8 +1053,9 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
   const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0);
   if (form != 1 && cluster_kernel_fits(a) && b.K == a.K)
     return launch_ozaki_cluster(a, ea, b, eb, true, slices, form, st);
-  // two passes over both operands: row maxima per (32 rows, 256 k) part, then digits per
-  // (32 rows, 128 k) chunk -- both spread over all SMs whatever the row count
+  // two passes over both operands: row maxima per (32 rows, 256 k) part, then the digits --
+  // by persistent CTAs over (16 rows, 512 k) slabs, or (form 1) per (32 rows, 128 k) chunk; both
+  // passes spread over all SMs whatever the row count
   const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
   const long parts_a = items_a * ((a.K + MKT - 1) / MKT), parts_b = items_b * ((b.K + MKT - 1) / MKT);
   const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);
@@ -1021,6 +1075,21 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
     note_launch();
   }
   ProfScope prof("ozaki_slice", st);
+  if (form != 1 && a.Kp == b.Kp) {
+    // digits by the persistent slab kernel
+    switch (slices) {
+      case 3: e = launch_digits_from_bits<3>(a, ea, bits, b, eb, bits_b, st); break;
+      case 4: e = launch_digits_from_bits<4>(a, ea, bits, b, eb, bits_b, st); break;
+      case 5: e = launch_digits_from_bits<5>(a, ea, bits, b, eb, bits_b, st); break;
+      case 6: e = launch_digits_from_bits<6>(a, ea, bits, b, eb, bits_b, st); break;
+      case 7: e = launch_digits_from_bits<7>(a, ea, bits, b, eb, bits_b, st); break;
+      case 8: e = launch_digits_from_bits<8>(a, ea, bits, b, eb, bits_b, st); break;
+      default: return cudaErrorInvalidValue;
+    }
+    note_launch();
+    return e;
+  }
+  // form 1: digits per (32 rows, 128 k) chunk
   const unsigned g = (unsigned)(chunks_a + chunks_b);
   switch (slices) {
     case 3: ozaki_digits_kernel<3, true><<<g, NTH, 0, st>>>(a, ea, chunks_a, b, eb, bits, bits_b); break;

@@ -126,14 +126,17 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     (0, 1, 64, 48, 2500, 2),      # K > 2048 with few rows: K-parallel row maxima, digit chunks
     (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows
     (1, 1, 40, 200, 9000, 1),     # K > 2048, several row-maximum parts per row, ragged last part
+    (1, 0, 48, 17, 4608, 3),      # K > 2048, K-contiguous, 9 whole 512-k slabs, odd column count
 ])
 def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
     """Every slicing kernel (the two-pass form 1 -- row maxima per (32 rows, 256 k) part, then
     digits per (32 rows, 128 k) chunk -- and the one-pass item shapes: form 2 = 32 rows x 256 k
     per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k, 5 = 16 rows x 256 k with two 256-thread
-    CTAs per SM, 6 = 4 rows x 256 k per 128-thread CTA, the slim form that runs beside the GEMM)
-    produces the planes the CPU restatement produces: the product is bit-exact against
-    oracle.ozaki_f64 whichever kernel sliced the operands."""
+    CTAs per SM, 6 = 4 rows x 256 k per 128-thread CTA, the slim form that runs beside the GEMM;
+    for k > 2048 form 3 is the row-maximum pass followed by persistent CTAs over 16 rows x 512 k
+    slabs that take their exponents from the maxima) produces the planes the CPU restatement
+    produces: the product is bit-exact against oracle.ozaki_f64 whichever kernel sliced the
+    operands."""
     from ssblasex_b200 import workloads as W
     if k > 2048 and form in (2, 4, 5, 6):
         pytest.skip("the one-pass forms apply to k <= 2048")

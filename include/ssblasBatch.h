@@ -113,8 +113,11 @@ typedef enum {
                                       pre-pass. 0 (default) and 3: one pass with thread-block
                                       clusters of 16 rows x 512 k per CTA when k <= 2048; 2: the
                                       same with 32 rows x 256 k; 4: 8 rows x 1024 k; 5: 16 rows x
-                                      256 k per 256-thread CTA, two CTAs per SM; 1: exponent
-                                      pass then digit pass */
+                                      256 k per 256-thread CTA, two CTAs per SM; 6: 4 rows x
+                                      256 k per 128-thread CTA; 1: row-maximum pass then digits
+                                      per 32 rows x 128 k chunk; 7: row-maximum pass then digits
+                                      by persistent CTAs over 16 rows x 512 k slabs (what every
+                                      form but 1 does when k > 2048) */
   SSBLAS_PATH_SPLITK_I8 = 8,       /* not a path: ssblasSetKernelConfig keys of the split-K factor */
   SSBLAS_PATH_SPLITK_OZAKI = 9,    /* of the int8 and Ozaki tcgen05 GEMMs. config = number of K
                                       pieces per output tile (1 = none, at most 64), 0 = automatic

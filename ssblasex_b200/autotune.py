@@ -32,10 +32,11 @@ FAMILIES = {
         dict(row="f64", transa=1, transb=0, m=256, n=256, k=2048, batch=32, alpha=1.0, beta=0.0,
              dist="expspread"),
     ]),
-    # slicing pre-pass of the Ozaki path: two passes (1) or one pass with thread-block clusters of
-    # 32 x 256 (2), 16 x 512 (3) or 8 x 1024 (4) per 512-thread CTA, or 16 x 256 per 256-thread
-    # CTA, two CTAs per SM (5) -- the cluster size is ceil(k / that K)
-    "ozaki_slicer": (SSBLAS_MATH_FP64_OZAKI, [1, 2, 3, 4, 5], "(all)", [
+    # slicing pre-pass of the Ozaki path: two passes (1: digits per 32 x 128 chunk; 7: digits by
+    # persistent CTAs over 16 x 512 slabs) or one pass with thread-block clusters of 32 x 256 (2),
+    # 16 x 512 (3) or 8 x 1024 (4) per 512-thread CTA, or 16 x 256 per 256-thread CTA, two CTAs
+    # per SM (5) -- the cluster size is ceil(k / that K)
+    "ozaki_slicer": (SSBLAS_MATH_FP64_OZAKI, [1, 2, 3, 4, 5, 7], "(all)", [
         dict(row="f64", transa=0, transb=1, m=1024, n=1024, k=1024, batch=32, alpha=1.0, beta=0.0,
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=1, transb=0, m=256, n=256, k=2048, batch=32, alpha=1.0, beta=0.0,

@@ -21,6 +21,25 @@ static __device__ __forceinline__ unsigned long long abs_bits(double x) {
 static __device__ __forceinline__ unsigned long long max_u64(unsigned long long a, unsigned long long b) {
   return a > b ? a : b;
 }
+// A key for the row maximum of N values, ordered like their largest |x| bit pattern as far as
+// row_exponent can tell: the high word of |x| (exponent and top 20 fraction bits) fixes frexp's
+// exponent whenever it is nonzero, so the key is max(high words) << 32; only when every high
+// word is zero (|x| below 2^-1042: zeros and the smallest subnormals) is the key the largest low
+// word. Inf and NaN keep a high word >= 0x7FF00000. Two integer operations per value instead of
+// the five of a 64-bit compare-and-select; the row maximum of the per-thread keys is then taken
+// with max_u64 as for bit patterns.
+template <int N>
+static __device__ __forceinline__ unsigned long long row_key(const double (&v)[N]) {
+  uint32_t mh = 0;
+#pragma unroll
+  for (int e = 0; e < N; ++e) mh = max(mh, (uint32_t)__double2hiint(v[e]) & 0x7FFFFFFFu);
+  if (mh != 0) return (unsigned long long)mh << 32;
+  uint32_t ml = 0;
+#pragma unroll
+  for (int e = 0; e < N; ++e) ml = max(ml, (uint32_t)__double2loint(v[e]));
+  return ml;
+}
+
 // e with max|x| < 2^e (0 for an all-zero row), or kNonFiniteExp
 static __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
   if (maxbits >= 0x7FF0000000000000ull) return kNonFiniteExp;

@@ -784,11 +784,9 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
       }
     } else {
-      // partial row maxima of this CTA's K range (bit patterns of |x|; the shared-memory buffers
-      // hold them as doubles, bit for bit)
-      unsigned long long mx = 0;
-#pragma unroll
-      for (int e = 0; e < 4 * RUNS; ++e) mx = max_u64(mx, abs_bits(v[e]));
+      // partial row maxima of this CTA's K range (row_key of |x|; the shared-memory buffers hold
+      // them as doubles, bit for bit)
+      unsigned long long mx = row_key(v);
       double* pm = pmax + s * R;
       auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
       auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
@@ -1049,13 +1047,13 @@ cudaError_t launch_split_bf16_pair(const PlaneArgs& a, const PlaneArgs& b, cudaS
 
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
                                     cudaStream_t st) {
-  // K up to 2048: one pass over both operands (unless the two-pass form is configured)
+  // K up to 2048: one pass over both operands (unless a two-pass form, 1 or 7, is configured)
   const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0);
-  if (form != 1 && cluster_kernel_fits(a) && b.K == a.K)
+  if (form != 1 && form != 7 && cluster_kernel_fits(a) && b.K == a.K)
     return launch_ozaki_cluster(a, ea, b, eb, true, slices, form, st);
   // two passes over both operands: row maxima per (32 rows, 256 k) part, then the digits --
-  // by persistent CTAs over (16 rows, 512 k) slabs, or (form 1) per (32 rows, 128 k) chunk; both
-  // passes spread over all SMs whatever the row count
+  // by persistent CTAs over (16 rows, 512 k) slabs (form 7, and every form but 1 when K > 2048),
+  // or (form 1) per (32 rows, 128 k) chunk; both passes spread over all SMs whatever the row count
   const long items_a = (a.rows + RT - 1) / RT * a.batch, items_b = (b.rows + RT - 1) / RT * b.batch;
   const long parts_a = items_a * ((a.K + MKT - 1) / MKT), parts_b = items_b * ((b.K + MKT - 1) / MKT);
   const long chunks_a = items_a * ((a.K + DKT - 1) / DKT), chunks_b = items_b * ((b.K + DKT - 1) / DKT);

@@ -118,7 +118,7 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     assert O.normalized_error(p, C) <= 4 * p.k * 2.0 ** -53
 
 
-@pytest.mark.parametrize("form", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("ta,tb,m,n,k,batch", [
     (1, 0, 200, 96, 2048, 2),     # single pass, clusters of 8 (4) CTAs, K contiguous, 16-byte loads
     (1, 0, 67, 45, 257, 3),       # single pass, clusters of 2 (1), odd ld (8-byte loads)
@@ -133,10 +133,10 @@ def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
     digits per (32 rows, 128 k) chunk -- and the one-pass item shapes: form 2 = 32 rows x 256 k
     per CTA, 3 = 16 rows x 512 k, 4 = 8 rows x 1024 k, 5 = 16 rows x 256 k with two 256-thread
     CTAs per SM, 6 = 4 rows x 256 k per 128-thread CTA, the slim form that runs beside the GEMM;
-    for k > 2048 form 3 is the row-maximum pass followed by persistent CTAs over 16 rows x 512 k
-    slabs that take their exponents from the maxima) produces the planes the CPU restatement
-    produces: the product is bit-exact against oracle.ozaki_f64 whichever kernel sliced the
-    operands."""
+    form 7, and form 3 for k > 2048, is the row-maximum pass followed by persistent CTAs over
+    16 rows x 512 k slabs that take their exponents from the maxima) produces the planes the CPU
+    restatement produces: the product is bit-exact against oracle.ozaki_f64 whichever kernel
+    sliced the operands."""
     from ssblasex_b200 import workloads as W
     if k > 2048 and form in (2, 4, 5, 6):
         pytest.skip("the one-pass forms apply to k <= 2048")
@@ -161,6 +161,40 @@ def test_ozaki_zero_rows_and_tiny_shapes(S):
         p.A[0][: p.lda] = 0.0      # first stored column of A[0] is zero
         C = run(p)
         np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
+
+
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("ta,tb", [(0, 1), (1, 0)])
+def test_ozaki_subnormal_rows(S, form, ta, tb):
+    """Rows of op(A) and columns of op(B) made of subnormals: below 2^-1042 (every high word
+    zero, so the row maximum comes from the low words), between 2^-1042 and 2^-1022, one normal
+    value among tiny subnormals, and negative tiny subnormals only; a column of op(B) near 2^1000
+    keeps some products representable. Every slicing form gives the exponents and digits of the
+    CPU restatement (bit-exact product)."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_slicer", form)
+    m, n, k, batch = 70, 40, 600, 2
+    p = W.make_problem("f64", ta, tb, m, n, k, batch, 1.0, 0.0, seed=11, dist="expspread")
+    rng = np.random.default_rng(5)
+    tiny = 2.0 ** -1074
+    for b in range(batch):
+        opa, opb = p.op_a(b), p.op_b(b)
+        opa[0, :] = rng.integers(-2 ** 31, 2 ** 31, k) * tiny
+        opa[1, :] = rng.integers(-2 ** 50, 2 ** 50, k) * tiny
+        opa[2, :] = rng.integers(-2 ** 20, 2 ** 20, k) * tiny
+        opa[2, 17 + b] = 3.0
+        opa[3, :] = -(rng.integers(0, 2 ** 10, k) * tiny)
+        opb[:, 0] = rng.integers(-2 ** 31, 2 ** 31, k) * tiny
+        opb[:, 1] = rng.integers(-2 ** 45, 2 ** 45, k) * tiny
+        opb[:, 5] = rng.standard_normal(k) * 2.0 ** 1000
+    try:
+        C = run(p)
+    finally:
+        S.set_kernel_config("ozaki_slicer", -1)
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
 
 
 # ------------------------------------------------------------------------- 3 x BF16 --------

@@ -153,20 +153,25 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 6 : MODE == 0 ? 6 : 8) gprep_
     }
   };
 
-  // Ozaki: row maxima over all of K (bit patterns of |x|, stored in the double buffers bit for
-  // bit); the digit pass reads the values again, mostly from L1/L2
+  // Ozaki: row maxima over all of K (row-maximum keys of |x|, stored in the double buffers bit
+  // for bit); the digit pass reads the values again, mostly from L1/L2
   if constexpr (MODE == 2) {
     unsigned long long mx[PER];
+    {
+      uint32_t mh[PER], ml[PER];
 #pragma unroll
-    for (int q = 0; q < PER; ++q) mx[q] = 0;
-    for (long k0 = 0; k0 < K; k0 += KC) {
+      for (int q = 0; q < PER; ++q) mh[q] = ml[q] = 0;
+      for (long k0 = 0; k0 < K; k0 += KC) {
 #pragma unroll
-      for (int q = 0; q < PER; ++q) {
-        T x[4];
-        load4(q, k0, x);
+        for (int q = 0; q < PER; ++q) {
+          T x[4];
+          load4(q, k0, x);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) mx[q] = max_u64(mx[q], abs_bits(x[i]));
+          for (int i = 0; i < 4; ++i) key_fold(x[i], mh[q], ml[q]);
+        }
       }
+#pragma unroll
+      for (int q = 0; q < PER; ++q) mx[q] = key_of(mh[q], ml[q]);
     }
     if (kc) {
       // the RPR threads of a row are consecutive lanes

@@ -40,6 +40,17 @@ static __device__ __forceinline__ unsigned long long row_key(const double (&v)[N
   return ml;
 }
 
+// Running form of row_key for values that arrive one at a time: fold each into the maxima of the
+// high words of |x| (mh) and of the low words (ml); key_of(mh, ml) is then the key. The low-word
+// maximum runs over every value, which is the right one whenever it is used (all high words zero).
+static __device__ __forceinline__ void key_fold(double x, uint32_t& mh, uint32_t& ml) {
+  mh = max(mh, (uint32_t)__double2hiint(x) & 0x7FFFFFFFu);
+  ml = max(ml, (uint32_t)__double2loint(x));
+}
+static __device__ __forceinline__ unsigned long long key_of(uint32_t mh, uint32_t ml) {
+  return mh != 0 ? (unsigned long long)mh << 32 : (unsigned long long)ml;
+}
+
 // e with max|x| < 2^e (0 for an all-zero row), or kNonFiniteExp
 static __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
   if (maxbits >= 0x7FF0000000000000ull) return kNonFiniteExp;

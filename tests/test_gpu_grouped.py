@@ -150,6 +150,36 @@ def test_grouped_ozaki_nonfinite_inputs():
         S.set_math_mode(0)
 
 
+def test_grouped_ozaki_subnormal_rows():
+    """Rows of op(A) and columns of op(B) made of subnormals (below 2^-1042, where the row
+    maximum comes from the low words, and above it), in instances of every layout: the grouped
+    pre-pass finds the exponents of the CPU restatement (bit-exact product)."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    rng = np.random.default_rng(21)
+    tiny = 2.0 ** -1074
+    probs = []
+    for i, (ta, tb) in enumerate([(0, 0), (1, 1), (0, 1), (1, 0)]):
+        p = W.make_problem("f64", ta, tb, 50 + 13 * i, 36 + 7 * i, 70 + 45 * i, 1, 1.0, 0.0, seed=800 + i,
+                           dist="expspread")
+        opa, opb = p.op_a(0), p.op_b(0)
+        opa[1, :] = rng.integers(-2 ** 31, 2 ** 31, p.k) * tiny
+        opa[2, :] = rng.integers(-2 ** 48, 2 ** 48, p.k) * tiny
+        opa[4, :] = -(rng.integers(0, 2 ** 12, p.k) * tiny)
+        opb[:, 0] = rng.integers(-2 ** 31, 2 ** 31, p.k) * tiny
+        opb[:, 3] = rng.standard_normal(p.k) * 2.0 ** 1000
+        probs.append(p)
+    S.set_math_mode(1)
+    try:
+        gd = runner.GroupedDevice(probs)
+        gd.reset_c()
+        assert gd.call(device_arrays=True) == 0
+        for p, C in zip(probs, gd.results()):
+            _check(p, C, 1)
+    finally:
+        S.set_math_mode(0)
+
+
 @pytest.mark.parametrize("mode", [0, 3])
 def test_grouped_transposed_orientation(mode):
     """Ozaki instances whose transposed product fills the 128-row tiles better (m small, n large)

@@ -538,6 +538,9 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
 //   (KC contiguous bytes).
 // Each operand is read from HBM once, and the next item's tile is in flight while the current
 // one is converted.
+// BITS form (k > 2048, after ozaki_rowmax_kernel): clusters of one CTA, items = (row block, KC
+// slab) pairs, and the row exponents come from the maxima instead of the partial-maximum
+// exchange; the rest of the item sequence is the same.
 //
 // Thread t (warp w, lane l) owns row r and 4 runs of 4 consecutive k: k = KC q + 4c + 4 NC j + i
 // (j < 4, i < 4, NC = KC / 16 runs per row), with

@@ -92,6 +92,34 @@ def test_i8_unequally_spaced_instances(S):
 
 
 # ------------------------------------------------------------------------- Ozaki -----------
+@pytest.mark.parametrize("k", [1000, 3000])
+@pytest.mark.parametrize("form", [3, 7])
+def test_ozaki_unequally_spaced_instances(S, k, form):
+    """Host array of device pointers in shuffled order: no uniform stride, so both slicing forms
+    (one pass with clusters; row maxima then slab digits) load their tiles by cp.async instead of
+    TMA, and the product is bit-exact against the CPU restatement."""
+    from ssblasex_b200 import runner, workloads as W
+    m, n, batch = 96, 80, 4
+    p = W.make_problem("f64", 0, 1, m, n, k, batch, 1.5, 0.5, seed=k + form, dist="expspread")
+    dp = runner.DeviceProblem(p)
+    order = [2, 0, 3, 1]
+    A, B, C = (dp.ptrs(t) for t in (dp.A, dp.B, dp.C))
+    arr = [(ct.c_void_p * batch)(*[x[o] for o in order]) for x in (A, B, C)]
+    al, be = np.array([1.5]), np.array([0.5])
+    ta, tb, tc = p.types
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_slicer", form)
+    try:
+        st = S.lib().ssblasGemmBatchedEx(0, 1, m, n, k, al.ctypes.data, arr[0], ta, p.lda, arr[1], tb, p.ldb,
+                                         be.ctypes.data, arr[2], tc, p.ldc, batch, 0, 0)
+    finally:
+        S.set_kernel_config("ozaki_slicer", -1)
+    assert st == 0
+    assert S.last_run_info()["path"] == "ozaki_tcgen05"
+    C_o = O.ozaki_f64(p, 7)[1]
+    np.testing.assert_array_equal(dp.C.cpu().numpy().view(np.uint64), C_o.view(np.uint64))
+
+
 @pytest.mark.parametrize("slices", [3, 4, 5, 6, 7, 8])
 def test_ozaki_bit_exact_per_slice_count(S, slices):
     from ssblasex_b200 import workloads as W

@@ -26,7 +26,7 @@
 //   K <= 2048   ozaki_cluster_kernel: one pass, persistent thread-block clusters. The ceil(K/256)
 //               CTAs of a cluster share 32 rows, exchange their partial row maxima through
 //               distributed shared memory and write the digits; tiles arrive by TMA (equally
-//               spaced instances) or cp.async two items ahead, digit rows leave by bulk copies.
+//               spaced instances) or cp.async two items ahead, digit rows leave as 16-byte stores.
 //               Each operand is read once.
 //   K > 2048    ozaki_rowmax_kernel (row maxima of |x| per 32 rows x 256 k part, combined by
 //               atomicMax) then ozaki_cluster_kernel in its BITS form (clusters of one CTA,
@@ -534,8 +534,9 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
 //   (16 values per thread); partial row maxima go to this CTA's pmax[item parity]; a cluster
 //   barrier; every CTA reads all CS partial maxima through distributed shared memory and derives
 //   the row exponents; the copies of the item two ahead are issued into the stage just read; the
-//   digits are staged [plane][row][k] in shared memory and leave by one bulk copy per plane row
-//   (KC contiguous bytes).
+//   digits are staged [plane][row][k] in shared memory and leave as 16-byte stores spread over
+//   all threads, a warp per 512 contiguous bytes of a plane row (bulk copies per plane row, tried
+//   before, needed a proxy fence in every thread and left 112 threads doing the write-out).
 // Each operand is read from HBM once, and the next item's tile is in flight while the current
 // one is converted.
 // BITS form (k > 2048, after ozaki_rowmax_kernel): clusters of one CTA, items = (row block, KC
@@ -660,14 +661,6 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
       "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
 }
-__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reinterpret_cast<uint64_t>(gdst)),
-               "r"((uint32_t)__cvta_generic_to_shared(ssrc)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // TMA: the item's R x KC tile of one operand through its 3-D tensor map (box: R rows x 256 k,
 // zero outside), one box per 256 k.
@@ -758,7 +751,6 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     } else {
       cpa_wait1();
     }
-    if (t < S * R) bulk_wait_read0();   // the previous item's digit rows have left st
     __syncthreads();
     const double* tile = stages + s * TILE;
     double v[4 * RUNS];
@@ -865,23 +857,26 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
 #pragma unroll
       for (int p = 0; p < S; ++p) st[(p * R + r) * PW + c + NC * j] = wd[p];
     }
-    // the bulk copies read st through the async proxy
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
-    // write-out: one bulk copy per (plane, row) of this CTA's KC bytes of K (k >= K holds zero
-    // digits, up to Kp)
-    if (t < S * R) {
-      const int p = t / R, rr = t % R;
+    // write-out: each (plane, row) of this CTA's KC bytes of K (k >= K holds zero digits, up to
+    // Kp) as 16-byte stores, a warp per 512 contiguous bytes, spread over all threads
+    {
+      constexpr int CPRW = KC / 16;                       // 16-byte chunks per staged row
+      constexpr int NCH = S * R * CPRW;                   // chunks of the item
       const long bytes = a.Kp - kbase < KC ? a.Kp - kbase : KC;
-      if (ci.row0 + rr < a.rows && bytes > 0) {
-        uint8_t* out = (uint8_t*)a.out + ci.b * a.batch_stride + p * a.plane_stride + (ci.row0 + rr) * a.Kp + kbase;
-        bulk_store(out, st + (p * R + rr) * PW, (uint32_t)bytes);
+      uint8_t* const out0 = (uint8_t*)a.out + ci.b * a.batch_stride + ci.row0 * a.Kp + kbase;
+#pragma unroll
+      for (int q = 0; q < (NCH + NTH - 1) / NTH; ++q) {
+        const int ch = t + q * NTH, pr = ch / CPRW, cc = ch % CPRW;
+        const int p = pr / R, rr = pr % R;
+        if (ch < NCH && ci.row0 + rr < a.rows && 16L * cc < bytes) {
+          const uint4 w = *(const uint4*)(st + pr * PW + 4 * cc);
+          *(uint4*)(out0 + p * a.plane_stride + (long)rr * a.Kp + 16 * cc) = w;
+        }
       }
-      bulk_commit();
     }
   }
-  if (t < S * R) bulk_wait0();
   if (!TMA) cpa_wait0();
   if (TMA && t == 0) {
     // no copy may still be in flight when the CTA exits (bounded, like every wait here)

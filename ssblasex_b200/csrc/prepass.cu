@@ -751,7 +751,11 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     } else {
       cpa_wait1();
     }
-    __syncthreads();
+    // Every thread has waited for the TMA tile itself. The barrier is needed for cp.async tiles
+    // (other threads' copies) and in the BITS form (rscale is rewritten below before any other
+    // barrier); in the exchange form the partial-maximum or cluster barrier already separates
+    // the previous item's reads of st, red and rscale from this item's writes.
+    if (!TMA || BITS) __syncthreads();
     const double* tile = stages + s * TILE;
     double v[4 * RUNS];
     if (a.kcontig) {

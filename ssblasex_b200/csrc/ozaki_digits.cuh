@@ -51,15 +51,21 @@ static __device__ __forceinline__ unsigned long long key_of(uint32_t mh, uint32_
   return mh != 0 ? (unsigned long long)mh << 32 : (unsigned long long)ml;
 }
 
-// e with max|x| < 2^e (0 for an all-zero row), or kNonFiniteExp
+// e with max|x| < 2^e (0 for an all-zero row), or kNonFiniteExp -- frexp's exponent, read off the
+// bit pattern: E - 1022 for a biased exponent E > 0, and for a subnormal f * 2^-1074 (f < 2^52)
+// the position of f's leading bit, 64 - clz(f) - 1074.
 static __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
   if (maxbits >= 0x7FF0000000000000ull) return kNonFiniteExp;
-  int e = 0;
-  const double m = __longlong_as_double((long long)maxbits);
-  if (m > 0.0) frexp(m, &e);
-  return e;
+  const int E = (int)(maxbits >> 52);
+  if (E > 0) return E - 1022;
+  return maxbits ? 64 - __clzll((long long)maxbits) - 1074 : 0;
 }
-// the two power-of-two factors of 2^(8S-2-e) (0 for a non-finite row: its digits are zero)
+// 2^h for -1022 <= h <= 1023, built from its bit pattern
+static __device__ __forceinline__ double pow2(int h) {
+  return __longlong_as_double((long long)(h + 1023) << 52);
+}
+// the two power-of-two factors of 2^(8S-2-e) (0 for a non-finite row: its digits are zero);
+// with e in [-1073, 1024] both halves of the shift stay inside the normal range
 static __device__ __forceinline__ void row_scale(int S, int e, double& s0, double& s1) {
   if (e == kNonFiniteExp) {
     s0 = s1 = 0.0;
@@ -67,8 +73,8 @@ static __device__ __forceinline__ void row_scale(int S, int e, double& s0, doubl
   }
   const int sh = 8 * S - 2 - e;
   const int h1 = sh / 2;
-  s0 = ldexp(1.0, h1);
-  s1 = ldexp(1.0, sh - h1);
+  s0 = pow2(h1);
+  s1 = pow2(sh - h1);
 }
 
 // 4 x 4 byte transpose: out[b] holds byte b of w[0..3] (byte j of out[b] = byte b of w[j]).

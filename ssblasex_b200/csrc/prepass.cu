@@ -773,6 +773,11 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         for (int i = 0; i < 4; ++i) v[4 * j + i] = tile[(4 * c + 4 * NC * j + i) * R + r];
     }
 
+    // A cluster of one CTA (k <= KC) holds whole rows: every thread takes its row's maximum from
+    // the reduction itself and derives the scale in registers -- no cluster exchange, no
+    // rscale buffer, two barriers per item instead of four.
+    const bool local = !BITS && CS == 1;
+    double s0 = 0.0, s1 = 0.0;
     if constexpr (BITS) {
       // the row maxima of the whole K range come from the K-parallel pass
       if (t < R) {
@@ -782,6 +787,36 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         if (kbase == 0 && gr < a.rows) exps[ci.b * a.rows + gr] = e;
         row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
       }
+    } else if (local) {
+      unsigned long long mx = row_key(v);
+      auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
+      auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
+      if (a.kcontig && NC <= 32) {
+        // the NC threads of row r are consecutive lanes: the xor reduction leaves the maximum in
+        // all of them
+#pragma unroll
+        for (int off = 1; off < NC; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      } else if (a.kcontig) {
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane == 0) red[warp] = as_d(mx);
+      } else {
+#pragma unroll
+        for (int off = LR; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane < LR) red[(warp / RG) * 32 + r] = as_d(mx);
+      }
+      __syncthreads();   // red visible; stage s fully read; the previous item's st reads done
+      if (a.kcontig && NC > 32) {
+        mx = as_u(red[r * (NC / 32)]);
+        for (int w = 1; w < NC / 32; ++w) mx = max_u64(mx, as_u(red[r * (NC / 32) + w]));
+      } else if (!a.kcontig) {
+        mx = as_u(red[r]);
+#pragma unroll
+        for (int w = 1; w < NW; ++w) mx = max_u64(mx, as_u(red[w * 32 + r]));
+      }
+      const int e = row_exponent(mx);
+      if (c == 0 && ci.row0 + r < a.rows) exps[ci.b * a.rows + ci.row0 + r] = e;
+      row_scale(S, e, s0, s1);
     } else {
       // partial row maxima of this CTA's K range (row_key of |x|; the shared-memory buffers hold
       // them as doubles, bit for bit)
@@ -829,7 +864,11 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
       }
     }
-    __syncthreads();   // rscale visible; stage s fully read into registers
+    if (!local) {
+      __syncthreads();   // rscale visible; stage s fully read into registers
+      s0 = rscale[2 * r];
+      s1 = rscale[2 * r + 1];
+    }
 
     // the item two ahead goes into the stage just read
     {
@@ -848,7 +887,6 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     }
 
     // digits: one 32-bit word per plane per run of 4 k, staged [p][r][k/4]
-    const double s0 = rscale[2 * r], s1 = rscale[2 * r + 1];
     if (s0 == 0.0) {   // a non-finite row has zero digits
 #pragma unroll
       for (int e = 0; e < 4 * RUNS; ++e) v[e] = 0.0;

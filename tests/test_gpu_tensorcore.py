@@ -155,6 +155,8 @@ def test_ozaki_layouts_and_error(S, ta, tb):
     (0, 0, 1984, 9, 2101, 5),     # K > 2048 with many rows
     (1, 1, 40, 200, 9000, 1),     # K > 2048, several row-maximum parts per row, ragged last part
     (1, 0, 48, 17, 4608, 3),      # K > 2048, K-contiguous, 9 whole 512-k slabs, odd column count
+    (1, 0, 77, 50, 200, 3),       # k <= 256: clusters of one CTA in every one-pass form, K contiguous
+    (0, 1, 90, 64, 64, 2),        # the same with rows contiguous
 ])
 def test_ozaki_slicer_paths(S, form, ta, tb, m, n, k, batch):
     """Every slicing kernel (the two-pass form 1 -- row maxima per (32 rows, 256 k) part, then

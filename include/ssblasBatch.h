@@ -110,9 +110,10 @@ typedef enum {
   SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch */
   SSBLAS_PATH_DMMA = 6,            /* plain fp64 on the FP64 tensor cores (mma.sync f64) */
   SSBLAS_PATH_OZAKI_SLICER = 7,    /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
-                                      pre-pass. 0 (default) and 3: one pass with thread-block
-                                      clusters of 16 rows x 512 k per CTA when k <= 2048; 2: the
-                                      same with 32 rows x 256 k; 4: 8 rows x 1024 k; 5: 16 rows x
+                                      pre-pass. 3: one pass with thread-block clusters of 16 rows
+                                      x 512 k per CTA when k <= 2048 (the default for k <= 512);
+                                      2: the same with 32 rows x 256 k; 4: 8 rows x 1024 k (the
+                                      default for 512 < k <= 2048); 5: 16 rows x
                                       256 k per 256-thread CTA, two CTAs per SM; 6: 4 rows x
                                       256 k per 128-thread CTA; 1: row-maximum pass then digits
                                       per 32 rows x 128 k chunk; 7: row-maximum pass then digits

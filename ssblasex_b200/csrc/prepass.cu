@@ -1087,8 +1087,10 @@ cudaError_t launch_split_bf16_pair(const PlaneArgs& a, const PlaneArgs& b, cudaS
 
 cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const PlaneArgs& b, int32_t* eb, int slices,
                                     cudaStream_t st) {
-  // K up to 2048: one pass over both operands (unless a two-pass form, 1 or 7, is configured)
-  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, 0);
+  // K up to 2048: one pass over both operands (unless a two-pass form, 1 or 7, is configured).
+  // Untuned default: 16 x 512 items while one CTA holds a whole row (k <= 512), else 8 x 1024
+  // (clusters of one CTA up to k = 1024, half as many CTAs exchanging maxima above).
+  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, b.rows, a.K, a.batch, a.Kp <= 512 ? 3 : 4);
   if (form != 1 && form != 7 && cluster_kernel_fits(a) && b.K == a.K)
     return launch_ozaki_cluster(a, ea, b, eb, true, slices, form, st);
   // two passes over both operands: row maxima per (32 rows, 256 k) part, then the digits --
@@ -1143,8 +1145,9 @@ cudaError_t launch_ozaki_slice_pair(const PlaneArgs& a, int32_t* ea, const Plane
 }
 
 cudaError_t launch_ozaki_slice(const PlaneArgs& a, int slices, int32_t* exps, cudaStream_t st) {
-  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, a.rows, a.K, a.batch, 0);
-  if (form != 1 && cluster_kernel_fits(a)) return launch_ozaki_cluster(a, exps, a, exps, false, slices, form, st);
+  const int form = choose_config(SSBLAS_PATH_OZAKI_SLICER, a.rows, a.rows, a.K, a.batch, a.Kp <= 512 ? 3 : 4);
+  if (form != 1 && form != 7 && cluster_kernel_fits(a))
+    return launch_ozaki_cluster(a, exps, a, exps, false, slices, form, st);
   const long items = (a.rows + RT - 1) / RT * a.batch;
   const long chunks = items * ((a.K + DKT - 1) / DKT);
   if (items >= 2L * num_sms() && chunks < (1L << 31)) {

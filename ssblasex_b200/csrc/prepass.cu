@@ -752,10 +752,9 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
       cpa_wait1();
     }
     // Every thread has waited for the TMA tile itself. The barrier is needed for cp.async tiles
-    // (other threads' copies) and in the BITS form (rscale is rewritten below before any other
-    // barrier); in the exchange form the partial-maximum or cluster barrier already separates
-    // the previous item's reads of st, red and rscale from this item's writes.
-    if (!TMA || BITS) __syncthreads();
+    // (other threads' copies); otherwise the barrier after the row maxima (or the cluster
+    // barrier) separates the previous item's reads of st, red and rscale from this item's writes.
+    if (!TMA) __syncthreads();
     const double* tile = stages + s * TILE;
     double v[4 * RUNS];
     if (a.kcontig) {
@@ -775,18 +774,18 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
 
     // A cluster of one CTA (k <= KC) holds whole rows: every thread takes its row's maximum from
     // the reduction itself and derives the scale in registers -- no cluster exchange, no
-    // rscale buffer, two barriers per item instead of four.
-    const bool local = !BITS && CS == 1;
+    // rscale buffer, two barriers per item instead of four. The BITS form does the same with
+    // the maxima of the K-parallel pass.
+    const bool local = BITS || CS == 1;
     double s0 = 0.0, s1 = 0.0;
     if constexpr (BITS) {
       // the row maxima of the whole K range come from the K-parallel pass
-      if (t < R) {
-        const long gr = ci.row0 + t;
-        const unsigned long long m2 = gr < a.rows ? (ci.second ? bits1 : bits0)[ci.b * a.rows + gr] : 0ull;
-        const int e = row_exponent(m2);
-        if (kbase == 0 && gr < a.rows) exps[ci.b * a.rows + gr] = e;
-        row_scale(S, e, rscale[2 * t], rscale[2 * t + 1]);
-      }
+      const long gr = ci.row0 + r;
+      const unsigned long long m2 = gr < a.rows ? (ci.second ? bits1 : bits0)[ci.b * a.rows + gr] : 0ull;
+      const int e = row_exponent(m2);
+      if (kbase == 0 && c == 0 && gr < a.rows) exps[ci.b * a.rows + gr] = e;
+      row_scale(S, e, s0, s1);
+      __syncthreads();   // stage s fully read; the previous item's st reads done
     } else if (local) {
       unsigned long long mx = row_key(v);
       auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };

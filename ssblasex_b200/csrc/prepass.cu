@@ -787,33 +787,38 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
       row_scale(S, e, s0, s1);
       __syncthreads();   // stage s fully read; the previous item's st reads done
     } else if (local) {
-      unsigned long long mx = row_key(v);
-      auto as_d = [](unsigned long long u) { return __longlong_as_double((long long)u); };
-      auto as_u = [](double d) { return (unsigned long long)__double_as_longlong(d); };
+      // row_exponent is monotonic in nonzero keys, so the row's exponent is the maximum of the
+      // threads' exponents: 32-bit reductions instead of 64-bit keys. A thread whose values are
+      // all zero (the fill past k, or zeros) takes a sentinel below every exponent (-1073 is the
+      // smallest), and a row that is zero throughout gets 0 back.
+      constexpr int kZeroKey = -0x40000000;
+      const unsigned long long key = row_key(v);
+      int e = key ? row_exponent(key) : kZeroKey;
+      int* const redi = (int*)red;
       if (a.kcontig && NC <= 32) {
         // the NC threads of row r are consecutive lanes: the xor reduction leaves the maximum in
         // all of them
 #pragma unroll
-        for (int off = 1; off < NC; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        for (int off = 1; off < NC; off <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, off));
       } else if (a.kcontig) {
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-        if (lane == 0) red[warp] = as_d(mx);
+        for (int off = 1; off < 32; off <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, off));
+        if (lane == 0) redi[warp] = e;
       } else {
 #pragma unroll
-        for (int off = LR; off < 32; off <<= 1) mx = max_u64(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-        if (lane < LR) red[(warp / RG) * 32 + r] = as_d(mx);
+        for (int off = LR; off < 32; off <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, off));
+        if (lane < LR) redi[(warp / RG) * 32 + r] = e;
       }
       __syncthreads();   // red visible; stage s fully read; the previous item's st reads done
       if (a.kcontig && NC > 32) {
-        mx = as_u(red[r * (NC / 32)]);
-        for (int w = 1; w < NC / 32; ++w) mx = max_u64(mx, as_u(red[r * (NC / 32) + w]));
+        e = redi[r * (NC / 32)];
+        for (int w = 1; w < NC / 32; ++w) e = max(e, redi[r * (NC / 32) + w]);
       } else if (!a.kcontig) {
-        mx = as_u(red[r]);
+        e = redi[r];
 #pragma unroll
-        for (int w = 1; w < NW; ++w) mx = max_u64(mx, as_u(red[w * 32 + r]));
+        for (int w = 1; w < NW; ++w) e = max(e, redi[w * 32 + r]);
       }
-      const int e = row_exponent(mx);
+      if (e == kZeroKey) e = 0;
       if (c == 0 && ci.row0 + r < a.rows) exps[ci.b * a.rows + ci.row0 + r] = e;
       row_scale(S, e, s0, s1);
     } else {

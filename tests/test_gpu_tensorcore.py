@@ -193,6 +193,28 @@ def test_ozaki_zero_rows_and_tiny_shapes(S):
         np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
 
 
+@pytest.mark.parametrize("form", [2, 3, 4, 5, 6])
+@pytest.mark.parametrize("ta,tb,k", [(1, 0, 200), (0, 1, 200), (1, 0, 700), (0, 1, 700)])
+def test_ozaki_slicer_rows_below_one(S, form, ta, tb, k):
+    """Entries in [-1, 1) (every row exponent <= 0) with k short of the item width, so part of
+    each item is zero fill: the threads that hold only zeros must not raise a row's exponent to
+    0 (the clusters-of-one path reduces per-thread exponents with a sentinel for zero). Bit-exact
+    against the CPU restatement."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_slicer", form)
+    p = W.make_problem("f64", ta, tb, 70, 45, k, 2, 1.0, 0.0, seed=k + form, dist="uniform")
+    p.op_a(0)[3, :] = 0.0                       # a zero row
+    p.op_a(1)[5, :] *= 2.0 ** -900              # a row far below 1
+    try:
+        C = run(p)
+    finally:
+        S.set_kernel_config("ozaki_slicer", -1)
+    st, C_o = O.ozaki_f64(p, 7)
+    assert st == 0
+    np.testing.assert_array_equal(C.view(np.uint64), C_o.view(np.uint64))
+
+
 @pytest.mark.parametrize("form", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("ta,tb", [(0, 1), (1, 0)])
 def test_ozaki_subnormal_rows(S, form, ta, tb):

@@ -96,3 +96,17 @@ def test_ozaki_restatement_nonfinite_rule():
     nan[:, 9] = True
     np.testing.assert_array_equal(np.isnan(got), nan)
     assert np.all(got[nan].view(np.uint64) == np.uint64(0x7FF8000000000000))
+
+
+def test_exponent_reduction_with_zero_sentinel():
+    """The clusters-of-one slicing path reduces per-thread exponents instead of keys: a thread
+    whose values are all zero contributes a sentinel below every exponent, and the maximum over
+    the threads is the exponent of the whole row (0 for a zero row)."""
+    rng = np.random.default_rng(7)
+    sentinel = -0x40000000
+    for r in _rows(rng, n=160, k=96):
+        parts = np.split(np.concatenate([r, np.zeros(32)]), 8)   # zero fill past k, as in a slab
+        es = [key_exponent(q) if np.any(q.view(np.uint64) & np.uint64(0x7FFFFFFFFFFFFFFF)) else sentinel
+              for q in parts]
+        e = max(es)
+        assert (0 if e == sentinel else e) == true_exponent(r)

@@ -86,9 +86,74 @@ ssblasStatus_t ssblasSetSyncMode(int synchronous);
 ssblasStatus_t ssblasSetMathMode(int mode);
 ssblasStatus_t ssblasGetMathMode(int* mode);
 
-/* Number of int8 slices per operand in SSBLAS_MATH_FP64_OZAKI mode (3..8); 0 selects it from the
- * error bound (the default). */
+/* Slice count of SSBLAS_MATH_FP64_OZAKI mode and its error bound.
+ *
+ * Each row i of op(A) is scaled by its power of two 2^e_i (the smallest above max_k |op(A)_ik|),
+ * rounded to an integer of 8S-2 bits and cut into S signed int8 slices; likewise each column j of
+ * op(B) with 2^f_j. The slice pairs p + q < S are multiplied exactly on the int8 tensor cores and
+ * recombined in FP64. For finite inputs and a result that neither overflows nor underflows:
+ *
+ *   |C_computed(i,j) - C_exact(i,j)| <= |alpha| * k * 2^(e_i + f_j) * (S + 1) * 2^(2 - 8S)
+ *                                        + (S + 1) * u * (|alpha| * sum_k |op(A)_ik op(B)_kj| + |beta C(i,j)|)
+ *
+ * with u = 2^-53. The first term covers the rounding of op(A) and op(B) to 8S-2 bits and the
+ * dropped pairs p + q >= S; the second the FP64 recombination and the alpha/beta epilogue.
+ *
+ * ssblasSetOzakiSlices(S), S in 3..8, fixes the count; 0 (the default) chooses the smallest S
+ * whose per-term bound (S + 1) * 2^(2 - 8S) is at most the tolerance of ssblasSetOzakiTolerance:
+ * by default 4u = 2^-51 (the FP64 tolerance 4*k*u spread over the k product terms), which selects
+ * S = 7 for every k. A tolerance of 0 restores the default; a negative tolerance, or one below the
+ * 8-slice bound (9 * 2^-62), returns SSBLAS_STATUS_INVALID_VALUE. ssblasGetOzakiSlices returns the
+ * count the next call will use; ssblasGetLastRunInfo reports the count a call used.
+ * ssblasGemmGroupedBatchedEx always uses 7 slices: its fp64 instances return
+ * SSBLAS_STATUS_NOTIMPLEMENTED_ERROR when another count is fixed or the tolerance needs 8. */
 ssblasStatus_t ssblasSetOzakiSlices(int slices);
+ssblasStatus_t ssblasSetOzakiTolerance(double tolerance);
+ssblasStatus_t ssblasGetOzakiSlices(int* slices);
+
+/* Type and semantics extensions (none is in the reference; all are off by default, and with a flag
+ * off the call behaves as the reference does). Bitwise OR of:
+ *   SSBLAS_EXT_R16F: the row (R_16F, R_16F, R_16F or R_32F): fp16 op(A) and op(B), fp16 or fp32 C,
+ *     float alpha/beta, fp32 accumulation on tcgen05 kind::f16 (declared but unimplemented in the
+ *     reference: ssblasBatch_type.h, ssblasGemmBatchedExSelector.hpp:105-107).
+ *   SSBLAS_EXT_R8U: SSBLAS_R_8U for either int8 operand (C SSBLAS_R_32I, int32 alpha/beta):
+ *     unsigned bytes, exact int32 products with wrap-around.
+ *   SSBLAS_EXT_OP_C: op C accepted on every row as op T (the conjugate transpose of a real
+ *     matrix); the reference rejects it on the fp rows and mis-computes it on the int8 row.
+ *   SSBLAS_EXT_K0_BETA: k == 0 computes C <- beta*C (BLAS; beta == 0 writes zeros without reading
+ *     C) instead of leaving C untouched, and k < 0 returns SSBLAS_STATUS_INVALID_VALUE.
+ *   SSBLAS_EXT_COMPUTE_TYPE: computeType is checked against the row and honoured:
+ *     SSBLAS_COMPUTE_32I only with int8 operands; SSBLAS_COMPUTE_32F only on the fp32 and fp16 rows,
+ *     where it asks for FP32 arithmetic (the fp32 row then never uses the 3xBF16 emulation); other
+ *     combinations return SSBLAS_STATUS_INVALID_VALUE. Without the flag computeType is ignored.
+ * The grouped entry point keeps the reference's three rows. Unknown flags return
+ * SSBLAS_STATUS_INVALID_VALUE. */
+typedef enum {
+  SSBLAS_EXT_NONE = 0,
+  SSBLAS_EXT_R16F = 1,
+  SSBLAS_EXT_R8U = 2,
+  SSBLAS_EXT_OP_C = 4,
+  SSBLAS_EXT_K0_BETA = 8,
+  SSBLAS_EXT_COMPUTE_TYPE = 16
+} ssblasExtension_t;
+ssblasStatus_t ssblasSetExtensions(int flags);
+ssblasStatus_t ssblasGetExtensions(int* flags);
+
+/* Fault injection for tests of the failure paths (no GPU is faulted or hung). The armed fault
+ * applies once, to the next point it names, then disarms:
+ *   SSBLAS_FAULT_SKIP_COPY: the next tensor-core GEMM launch (int8, Ozaki or 3xBF16 path) skips
+ *     one operand copy in its first thread block and gives every bounded wait a short limit; the
+ *     waits on that copy run out, the kernel records the error and exits, and the call returns
+ *     SSBLAS_STATUS_INTERNAL_ERROR with ssblasRunInfo_t.device_error set. The next call is normal.
+ *   SSBLAS_FAULT_ALLOC: the next request for library workspace fails as if the device were out
+ *     of memory; the call returns SSBLAS_STATUS_ALLOC_FAILED before launching anything.
+ * SSBLAS_FAULT_NONE disarms. Other values return SSBLAS_STATUS_INVALID_VALUE. */
+typedef enum {
+  SSBLAS_FAULT_NONE = 0,
+  SSBLAS_FAULT_SKIP_COPY = 1,
+  SSBLAS_FAULT_ALLOC = 2
+} ssblasFault_t;
+ssblasStatus_t ssblasSetFaultInjection(int fault);
 
 /* Description of the most recent call on this process. */
 typedef struct {
@@ -129,7 +194,8 @@ typedef enum {
   SSBLAS_PATH_OZAKI_PIPELINE = 10  /* not a path: ssblasSetKernelConfig key of the Ozaki slicing /
                                       GEMM pipeline: config = chunks of the batch (1 = none, at most
                                       8), 0 = automatic (none); the slicing of chunk c + 1 runs
-                                      beside the GEMM of chunk c. */
+                                      beside the GEMM of chunk c. */,
+  SSBLAS_PATH_F16_TCGEN05 = 11      /* fp16 inputs (SSBLAS_EXT_R16F row) on tcgen05.mma kind::f16 */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

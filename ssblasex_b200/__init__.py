@@ -34,14 +34,18 @@ SSBLAS_COMPUTE_DEFAULT = 0
 # extensions
 SSBLAS_MATH_PLAIN, SSBLAS_MATH_FP64_OZAKI, SSBLAS_MATH_FP32_BF16X3 = 0, 1, 2
 PATH_NAMES = {0: "none", 1: "simt", 2: "i8_tcgen05", 3: "ozaki_tcgen05", 4: "bf16x3_tcgen05", 5: "grouped",
-              6: "dmma"}
+              6: "dmma", 11: "f16_tcgen05"}
+# type and semantics extensions (ssblasSetExtensions)
+SSBLAS_EXT_NONE, SSBLAS_EXT_R16F, SSBLAS_EXT_R8U, SSBLAS_EXT_OP_C, SSBLAS_EXT_K0_BETA, SSBLAS_EXT_COMPUTE_TYPE = (
+    0, 1, 2, 4, 8, 16)
 
 EXPORTED_SYMBOLS = (
     "ssblasGemmBatchedEx", "ssblasGemmBatchedEx_64", "ssblasGemmGroupedBatchedEx",
     "ssblasSetStream", "ssblasGetStream", "ssblasSetSyncMode", "ssblasSetMathMode",
     "ssblasGetMathMode", "ssblasSetOzakiSlices", "ssblasGetLastRunInfo", "ssblasReleaseWorkspace",
     "ssblasSetProfiling", "ssblasGetProfile", "ssblasGemmBatchedExNoAlloc",
-    "ssblasSetKernelConfig", "ssblasReloadTuning",
+    "ssblasSetKernelConfig", "ssblasReloadTuning", "ssblasSetOzakiTolerance", "ssblasGetOzakiSlices",
+    "ssblasSetFaultInjection", "ssblasSetExtensions", "ssblasGetExtensions",
 )
 
 
@@ -80,6 +84,11 @@ def lib() -> ct.CDLL:
         L.ssblasSetMathMode.argtypes = [i]
         L.ssblasGetMathMode.argtypes = [ct.POINTER(i)]
         L.ssblasSetOzakiSlices.argtypes = [i]
+        L.ssblasSetOzakiTolerance.argtypes = [ct.c_double]
+        L.ssblasGetOzakiSlices.argtypes = [ct.POINTER(i)]
+        L.ssblasSetFaultInjection.argtypes = [i]
+        L.ssblasSetExtensions.argtypes = [i]
+        L.ssblasGetExtensions.argtypes = [ct.POINTER(i)]
         L.ssblasGetLastRunInfo.argtypes = [ct.POINTER(RunInfo)]
         L.ssblasReleaseWorkspace.argtypes = []
         L.ssblasSetProfiling.argtypes = [i]
@@ -129,6 +138,44 @@ def get_math_mode() -> int:
 
 def set_ozaki_slices(slices: int) -> int:
     return lib().ssblasSetOzakiSlices(slices)
+
+
+def set_ozaki_tolerance(tolerance: float) -> int:
+    """Per-term error target of the automatic Ozaki slice count (0 = the default 2^-51)."""
+    return lib().ssblasSetOzakiTolerance(float(tolerance))
+
+
+def get_ozaki_slices() -> int:
+    """Slice count the next fp64 Ozaki call will use."""
+    v = ct.c_int()
+    lib().ssblasGetOzakiSlices(ct.byref(v))
+    return v.value
+
+
+def ozaki_term_bound(slices: int) -> float:
+    """Per-term error bound (S + 1) * 2^(2 - 8S) of the Ozaki emulation, in units of
+    |alpha| * 2^(e_i + f_j) (the row and column power-of-two scales)."""
+    import math
+    return (slices + 1) * math.ldexp(1.0, 2 - 8 * slices)
+
+
+SSBLAS_FAULT_NONE, SSBLAS_FAULT_SKIP_COPY, SSBLAS_FAULT_ALLOC = 0, 1, 2
+
+
+def set_extensions(flags: int) -> int:
+    """Enables type / semantics extensions (SSBLAS_EXT_* flags OR-ed; 0 = the reference's behaviour)."""
+    return lib().ssblasSetExtensions(flags)
+
+
+def get_extensions() -> int:
+    v = ct.c_int()
+    lib().ssblasGetExtensions(ct.byref(v))
+    return v.value
+
+
+def set_fault_injection(fault: int) -> int:
+    """Arms a one-shot test fault (SSBLAS_FAULT_SKIP_COPY / SSBLAS_FAULT_ALLOC); 0 disarms."""
+    return lib().ssblasSetFaultInjection(fault)
 
 
 def last_run_info() -> dict:

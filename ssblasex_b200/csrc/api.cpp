@@ -40,10 +40,14 @@ Settings& settings() {
 static std::mutex g_mutex;
 static ssblasRunInfo_t g_info;
 
+std::unique_lock<std::mutex> lock_api() { return std::unique_lock<std::mutex>(g_mutex); }
+void reset_run_info() { g_info = ssblasRunInfo_t{}; }
+
 // ---------------------------------------------------------------- kernel profiling -----------
 struct ProfPending {
   const char* name;
   cudaEvent_t a, b;
+  int dev;
 };
 struct ProfTotal {
   std::string name;
@@ -53,13 +57,14 @@ struct ProfTotal {
 static bool g_prof_on = false;
 static std::vector<ProfPending> g_prof_pending;
 static std::vector<ProfTotal> g_prof_total;
-static std::vector<cudaEvent_t> g_prof_free;
+static std::vector<cudaEvent_t> g_prof_free[kMaxDevices];   // events are created on one device
 
-static cudaEvent_t prof_event() {
+static cudaEvent_t prof_event(int dev) {
   cudaEvent_t e = nullptr;
-  if (!g_prof_free.empty()) {
-    e = g_prof_free.back();
-    g_prof_free.pop_back();
+  if (dev < 0) return nullptr;
+  if (!g_prof_free[dev].empty()) {
+    e = g_prof_free[dev].back();
+    g_prof_free[dev].pop_back();
   } else if (cudaEventCreate(&e) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
@@ -69,7 +74,8 @@ static cudaEvent_t prof_event() {
 
 void prof_start(const char* name, cudaStream_t st) {
   if (!g_prof_on) return;
-  ProfPending p{name, prof_event(), prof_event()};
+  const int dev = current_device();
+  ProfPending p{name, prof_event(dev), prof_event(dev), dev};
   if (p.a) cudaEventRecord(p.a, st);
   g_prof_pending.push_back(p);
 }
@@ -96,8 +102,8 @@ static void prof_resolve() {
       t->ms += ms;
     }
     cudaGetLastError();
-    if (p.a) g_prof_free.push_back(p.a);
-    if (p.b) g_prof_free.push_back(p.b);
+    if (p.a) g_prof_free[p.dev].push_back(p.a);
+    if (p.b) g_prof_free[p.dev].push_back(p.b);
   }
   g_prof_pending.clear();
 }
@@ -109,16 +115,28 @@ void note_path(int path, int slices) {
   g_info.slices = slices;
 }
 
-int num_sms() {
-  static int sms = [] {
-    int dev = 0, v = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
-      return v;
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
-    return 148;
-  }();
-  return sms;
+    return -1;
+  }
+  return (dev >= 0 && dev < kMaxDevices) ? dev : -1;
+}
+
+int num_sms() {
+  static int sms[kMaxDevices] = {};
+  const int dev = current_device();
+  if (dev < 0) return 148;
+  if (!sms[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    sms[dev] = v;
+  }
+  return sms[dev];
 }
 
 // ---------------------------------------------------------------- workspace ------------------
@@ -135,6 +153,12 @@ void* workspace(WsSlot slot, size_t bytes, cudaError_t* err) {
   if ((int)g_ws.size() <= dev) g_ws.resize(dev + 1);
   DeviceWs& w = g_ws[dev];
   if (bytes == 0) bytes = 256;
+  if (settings().fault == SSBLAS_FAULT_ALLOC) {
+    // one-shot test fault: this request fails as if the device were out of memory
+    settings().fault = SSBLAS_FAULT_NONE;
+    *err = cudaErrorMemoryAllocation;
+    return nullptr;
+  }
   if (w.size[slot] >= bytes) return w.ptr[slot];
   if (w.ptr[slot]) {
     // the old buffer may still be read by work in flight
@@ -247,6 +271,7 @@ static PtrKind kind_of(const void* p) {
 static size_t elem_size(Row r, bool c_operand) {
   if (r == ROW_F32) return 4;
   if (r == ROW_F64) return 8;
+  if (r == ROW_F16) return 2;   // C of the fp16 row may be fp32 instead (BatchDesc::c_f32)
   return c_operand ? 4 : 1;
 }
 
@@ -270,13 +295,19 @@ struct PinnedSlot {
   cudaEvent_t done = nullptr;
   bool pending = false;
 };
-static PinnedSlot g_pins[kPinSlots];
-static int g_pin_cur = 0;
+// One ring per device: a slot's event belongs to the device whose stream recorded it.
+static PinnedSlot g_pins[kMaxDevices][kPinSlots];
+static int g_pin_cur[kMaxDevices] = {};
 
 static void* pinned(size_t bytes, cudaError_t* err) {
   *err = cudaSuccess;
-  g_pin_cur = (g_pin_cur + 1) % kPinSlots;
-  PinnedSlot& s = g_pins[g_pin_cur];
+  const int dev = current_device();
+  if (dev < 0) {
+    *err = cudaErrorInvalidDevice;
+    return nullptr;
+  }
+  g_pin_cur[dev] = (g_pin_cur[dev] + 1) % kPinSlots;
+  PinnedSlot& s = g_pins[dev][g_pin_cur[dev]];
   if (s.pending) cudaEventSynchronize(s.done);
   s.pending = false;
   if (s.size < bytes) {
@@ -297,7 +328,9 @@ static void* pinned(size_t bytes, cudaError_t* err) {
 
 // marks the current slot as read by an upload just enqueued on `st`
 static void pinned_done(cudaStream_t st) {
-  PinnedSlot& s = g_pins[g_pin_cur];
+  const int dev = current_device();
+  if (dev < 0) return;
+  PinnedSlot& s = g_pins[dev][g_pin_cur[dev]];
   if (cudaEventRecord(s.done, st) == cudaSuccess) s.pending = true;
 }
 
@@ -345,27 +378,56 @@ static cudaError_t stage_operand(WsSlot slot, const void* const* hptr, long batc
 struct Rowsel {
   Row row;
   bool ok;
+  bool a_unsigned = false, b_unsigned = false, c_f32 = false;
 };
 
-static Rowsel select_row(ssblasDataType_t a, ssblasDataType_t b, ssblasDataType_t c) {
+// The reference's three type rows (ssblasGemmBatchedExSelector.hpp:35-107), plus the rows the
+// type extensions enable: R_8U for either int8 operand, and fp16 inputs with fp16 or fp32 C.
+static Rowsel select_row(ssblasDataType_t a, ssblasDataType_t b, ssblasDataType_t c, int ext = 0) {
   if (a == SSBLAS_R_8I && b == SSBLAS_R_8I && c == SSBLAS_R_32I) return {ROW_I8, true};
   if (a == SSBLAS_R_64F && b == SSBLAS_R_64F && c == SSBLAS_R_64F) return {ROW_F64, true};
   if (a == SSBLAS_R_32F && b == SSBLAS_R_32F && c == SSBLAS_R_32F) return {ROW_F32, true};
+  const auto i8 = [](ssblasDataType_t t) { return t == SSBLAS_R_8I || t == SSBLAS_R_8U; };
+  if ((ext & SSBLAS_EXT_R8U) && i8(a) && i8(b) && c == SSBLAS_R_32I)
+    return {ROW_I8, true, a == SSBLAS_R_8U, b == SSBLAS_R_8U, false};
+  if ((ext & SSBLAS_EXT_R16F) && a == SSBLAS_R_16F && b == SSBLAS_R_16F && (c == SSBLAS_R_16F || c == SSBLAS_R_32F))
+    return {ROW_F16, true, false, false, c == SSBLAS_R_32F};
   return {ROW_F32, false};
+}
+
+// computeType under SSBLAS_EXT_COMPUTE_TYPE: DEFAULT fits every row, 32I the int8 rows, 32F the
+// fp32 and fp16 rows (on the fp32 row it asks for FP32 arithmetic, so the 3xBF16 emulation is not
+// used). Without the extension computeType is ignored, as in the reference
+// (ssblasGemmBatchedEx_ALLDATASIZESAME.hpp:46-49).
+static bool compute_type_fits(ssblasComputeType_t c, Row row) {
+  if (c == SSBLAS_COMPUTE_DEFAULT_TYPE) return true;
+  if (c == SSBLAS_COMPUTE_32I) return row == ROW_I8;
+  if (c == SSBLAS_COMPUTE_32F) return row == ROW_F32 || row == ROW_F16;
+  return false;
 }
 
 // Runs the row's kernels on device-resident data.
 static cudaError_t dispatch(const BatchDesc& d, cudaStream_t st) {
-  const int mode = settings().math_mode;
-  if (d.row == ROW_I8) {
+  const int mode = d.exact_f32 ? (settings().math_mode & ~SSBLAS_MATH_FP32_BF16X3) : settings().math_mode;
+  if (d.k == 0) {
+    // k = 0 under SSBLAS_EXT_K0_BETA: C <- beta * C (no operand is read)
+    note_path(SSBLAS_PATH_SIMT);
+    return launch_simt_gemm(d, st);
+  }
+  if (d.row == ROW_F16) {
+    cudaError_t e = launch_f16_tcgen05(d, st);
+    if (e != cudaErrorNotSupported) {
+      if (e == cudaSuccess) note_path(SSBLAS_PATH_F16_TCGEN05);
+      return e;
+    }
+  } else if (d.row == ROW_I8) {
     cudaError_t e = launch_i8_tcgen05(d, st);
     if (e != cudaErrorNotSupported) {
       if (e == cudaSuccess) note_path(SSBLAS_PATH_I8_TCGEN05);
       return e;
     }
   } else if (d.row == ROW_F64 && (mode & SSBLAS_MATH_FP64_OZAKI)) {
-    int s = settings().ozaki_slices;
-    cudaError_t e = launch_ozaki_f64(d, s, st);
+    cudaError_t e = launch_ozaki_f64(d, ozaki_slices_for_call(), st);
     if (e != cudaErrorNotSupported) return e;
   } else if (d.row == ROW_F64 && choose_config(SSBLAS_PATH_DMMA, d.m, d.n, d.k, d.batch, 0) != 2) {
     // plain fp64: DMMA tiles (configuration 2 selects the DFMA SIMT kernel instead)
@@ -382,7 +444,7 @@ static cudaError_t dispatch(const BatchDesc& d, cudaStream_t st) {
   return launch_simt_gemm(d, st);
 }
 
-static ssblasStatus_t check_device_error(cudaStream_t st) {
+ssblasStatus_t check_device_error(cudaStream_t st) {
   int* flag = device_error_flag();
   if (!flag) return SSBLAS_STATUS_INTERNAL_ERROR;
   int h = 0;
@@ -399,7 +461,6 @@ static ssblasStatus_t check_device_error(cudaStream_t st) {
   return SSBLAS_STATUS_SUCCESS;
 }
 
-static ssblasStatus_t check_device_error(cudaStream_t st);
 static ssblasStatus_t map_err(cudaError_t e);
 static void* pinned(size_t bytes, cudaError_t* err);
 
@@ -442,6 +503,14 @@ static ssblasStatus_t grouped_device(
   }
   std::lock_guard<std::mutex> lock(g_mutex);
   g_info = ssblasRunInfo_t{};
+  if (settings().math_mode & SSBLAS_MATH_FP64_OZAKI) {
+    // the grouped kernels are built for 7 slices: a fixed other count, or a tolerance that needs
+    // 8, cannot be honoured (a looser tolerance is met by 7 slices as well)
+    bool any_f64 = false;
+    for (const GroupedInst& in : g.inst) any_f64 |= in.row == ROW_F64;
+    const int S = ozaki_slices_for_call();
+    if (any_f64 && (settings().ozaki_slices != 0 ? S != 7 : S > 7)) return SSBLAS_STATUS_NOTIMPLEMENTED_ERROR;
+  }
   cudaStream_t st = settings().stream;
   cudaError_t e;
   const bool dev_arrays = kind_of((const void*)A) == PK_DEVICE;
@@ -490,9 +559,19 @@ static ssblasStatus_t run_host_pipelined(BatchDesc d, const void* const A[], con
   auto dense = [](long s, size_t bytes) { return s > 0 && (size_t)s >= bytes && (size_t)s <= 2 * bytes + 4096; };
   if (!dense(sa, a_bytes) || !dense(sb, b_bytes) || !dense(sc, c_bytes)) return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
 
-  static cudaStream_t s_in = nullptr, s_out = nullptr;
   constexpr int NCH = 16;  // chunks: copies of chunk c+1 overlap the GEMM of chunk c and the copy-back of c-1
-  static cudaEvent_t ev_start = nullptr, ev_in[NCH], ev_cp[NCH];
+  struct PipeStreams {
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_in[NCH] = {}, ev_cp[NCH] = {};
+  };
+  static PipeStreams per_dev[kMaxDevices];   // streams and events belong to one device
+  const int dev = current_device();
+  if (dev < 0) return SSBLAS_STATUS_INTERNAL_ERROR;
+  cudaStream_t& s_in = per_dev[dev].s_in;
+  cudaStream_t& s_out = per_dev[dev].s_out;
+  cudaEvent_t& ev_start = per_dev[dev].ev_start;
+  cudaEvent_t* ev_in = per_dev[dev].ev_in;
+  cudaEvent_t* ev_cp = per_dev[dev].ev_cp;
   cudaError_t e;
   if (!s_in) {
     if ((e = cudaStreamCreateWithFlags(&s_in, cudaStreamNonBlocking)) ||
@@ -570,17 +649,27 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
                                    ssblasGemmAlgo_t algo) {
   if (getenv("SSBLAS_GEMMBATCHEDEX_DEBUG") != nullptr)
     debug_dump(transa, transb, m, n, k, Atype, lda, Btype, ldb, Ctype, ldc, batchCount, computeType, algo);
+  ApiRange range("ssblasGemmBatchedEx");
 
-  Rowsel rs = select_row(Atype, Btype, Ctype);
+  const int ext = settings().extensions;
+  Rowsel rs = select_row(Atype, Btype, Ctype, ext);
   if (!rs.ok) return SSBLAS_STATUS_INVALID_VALUE;
+  // op C: rejected (the reference rejects it on the fp rows and mis-computes it on the int8 row);
+  // under SSBLAS_EXT_OP_C it is op T, the conjugate transpose of a real matrix
+  if ((ext & SSBLAS_EXT_OP_C) && transa == SSBLAS_OP_C) transa = SSBLAS_OP_T;
+  if ((ext & SSBLAS_EXT_OP_C) && transb == SSBLAS_OP_C) transb = SSBLAS_OP_T;
   if ((transa != SSBLAS_OP_N && transa != SSBLAS_OP_T) || (transb != SSBLAS_OP_N && transb != SSBLAS_OP_T))
     return SSBLAS_STATUS_INVALID_VALUE;
+  if ((ext & SSBLAS_EXT_COMPUTE_TYPE) && !compute_type_fits(computeType, rs.row)) return SSBLAS_STATUS_INVALID_VALUE;
   if (m <= 0 || n <= 0 || batchCount <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
-  if (k <= 0) return SSBLAS_STATUS_SUCCESS;  // the reference leaves C untouched
+  const bool k0_beta = (ext & SSBLAS_EXT_K0_BETA) != 0;
+  if (k < 0 && k0_beta) return SSBLAS_STATUS_INVALID_VALUE;
+  if (k <= 0 && !k0_beta) return SSBLAS_STATUS_SUCCESS;  // the reference leaves C untouched
   if (!alpha || !beta || !A || !B || !C) return SSBLAS_STATUS_INVALID_VALUE;
   const long arows = (transa == SSBLAS_OP_N) ? m : k, acols = (transa == SSBLAS_OP_N) ? k : m;
   const long brows = (transb == SSBLAS_OP_N) ? k : n, bcols = (transb == SSBLAS_OP_N) ? n : k;
-  if (lda < arows || ldb < brows || ldc < m) return SSBLAS_STATUS_INVALID_VALUE;
+  if (ldc < m) return SSBLAS_STATUS_INVALID_VALUE;
+  if (k > 0 && (lda < arows || ldb < brows)) return SSBLAS_STATUS_INVALID_VALUE;
 
   std::lock_guard<std::mutex> lock(g_mutex);
   g_info = ssblasRunInfo_t{};
@@ -591,7 +680,9 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
   d.row = rs.row;
   d.transa = transa; d.transb = transb;
   d.m = m; d.n = n; d.k = k; d.lda = lda; d.ldb = ldb; d.ldc = ldc; d.batch = batchCount;
-  if (rs.row == ROW_F32) {
+  d.a_unsigned = rs.a_unsigned; d.b_unsigned = rs.b_unsigned; d.c_f32 = rs.c_f32;
+  d.exact_f32 = (ext & SSBLAS_EXT_COMPUTE_TYPE) && computeType == SSBLAS_COMPUTE_32F;
+  if (rs.row == ROW_F32 || rs.row == ROW_F16) {
     d.alpha_f = *(const float*)alpha; d.beta_f = *(const float*)beta;
   } else if (rs.row == ROW_F64) {
     d.alpha_d = *(const double*)alpha; d.beta_d = *(const double*)beta;
@@ -599,9 +690,10 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
     d.alpha_i = *(const int32_t*)alpha; d.beta_i = *(const int32_t*)beta;
   }
 
-  const size_t ea = elem_size(rs.row, false), ec = elem_size(rs.row, true);
-  const size_t a_bytes = (size_t)(lda * (acols - 1) + arows) * ea;
-  const size_t b_bytes = (size_t)(ldb * (bcols - 1) + brows) * ea;
+  const size_t ea = elem_size(rs.row, false), ec = rs.c_f32 ? 4 : elem_size(rs.row, true);
+  // with k = 0 (SSBLAS_EXT_K0_BETA) no operand is read: nothing of A or B is staged
+  const size_t a_bytes = k > 0 ? (size_t)(lda * (acols - 1) + arows) * ea : 0;
+  const size_t b_bytes = k > 0 ? (size_t)(ldb * (bcols - 1) + brows) * ea : 0;
   const size_t c_bytes = (size_t)(ldc * (n - 1) + m) * ec;
 
   const PtrKind arr_kind = kind_of((const void*)A);
@@ -738,6 +830,7 @@ ssblasStatus_t ssblasGemmGroupedBatchedEx(
     const SSINT ldb_array[], const void* const beta_array[], void* const C[],
     const ssblasDataType_t Ctype_array[], const SSINT ldc_array[], const SSINT group_count,
     const SSINT group_size[], ssblasComputeType_t computeType, ssblasGemmAlgo_t algo) {
+  ApiRange range("ssblasGemmGroupedBatchedEx");
   if (group_count <= 0) return SSBLAS_STATUS_INTERNAL_ERROR;
   if (!transa_array || !transb_array || !m_array || !n_array || !k_array || !alpha_array || !A ||
       !Atype_array || !lda_array || !B || !Btype_array || !ldb_array || !beta_array || !C ||
@@ -797,6 +890,44 @@ ssblasStatus_t ssblasSetOzakiSlices(int slices) {
   if (slices != 0 && (slices < 3 || slices > 8)) return SSBLAS_STATUS_INVALID_VALUE;
   std::lock_guard<std::mutex> lock(g_mutex);
   settings().ozaki_slices = slices;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetOzakiTolerance(double tolerance) {
+  // NaN and negative targets are refused; a target below the 8-slice bound cannot be met
+  if (!(tolerance >= 0.0) || (tolerance > 0.0 && tolerance < ozaki_term_bound(8)))
+    return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().ozaki_tolerance = tolerance;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetOzakiSlices(int* slices) {
+  if (!slices) return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  *slices = ozaki_slices_for_call();
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetExtensions(int flags) {
+  if (flags & ~(SSBLAS_EXT_R16F | SSBLAS_EXT_R8U | SSBLAS_EXT_OP_C | SSBLAS_EXT_K0_BETA | SSBLAS_EXT_COMPUTE_TYPE))
+    return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().extensions = flags;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasGetExtensions(int* flags) {
+  if (!flags) return SSBLAS_STATUS_INVALID_VALUE;
+  *flags = settings().extensions;
+  return SSBLAS_STATUS_SUCCESS;
+}
+
+ssblasStatus_t ssblasSetFaultInjection(int fault) {
+  if (fault != SSBLAS_FAULT_NONE && fault != SSBLAS_FAULT_SKIP_COPY && fault != SSBLAS_FAULT_ALLOC)
+    return SSBLAS_STATUS_INVALID_VALUE;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  settings().fault = fault;
   return SSBLAS_STATUS_SUCCESS;
 }
 

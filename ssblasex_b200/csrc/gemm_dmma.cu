@@ -199,12 +199,8 @@ cudaError_t launch_cfg(const DmmaArgs& a, cudaStream_t st) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int SMEM = STAGES * DmmaSmem<BM, BN, BK>::STAGE * 8;
   auto kern = dmma_gemm_kernel<BM, BN, BK, WM, WN, STAGES, MINB, A_MN, B_MN>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
   const long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
   if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
   dim3 grid((unsigned)tiles, (unsigned)(a.batch < 65535 ? a.batch : 65535));

@@ -333,7 +333,10 @@ cudaError_t launch_small(const SgemmArgs& a, cudaStream_t st) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int SMEM = 2 * KS * BK * (BM + 4 + BN + 4) * 4;
   auto kern = sgemm_small_kernel<BM, BN, BK, TM, TN, KS, MINB, A_MN, B_MN>;
-  static int per_sm = 0;
+  static int per_sm_dev[kMaxDevices] = {};
+  const int dev = current_device();
+  if (dev < 0) return cudaErrorInvalidDevice;
+  int& per_sm = per_sm_dev[dev];
   if (!per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, SMEM);
@@ -353,12 +356,8 @@ cudaError_t launch_s(const SgemmArgs& a, cudaStream_t st) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int SMEM = STAGES * BK * (BM + 4 + BN + 4) * 4;
   auto kern = sgemm_async_kernel<BM, BN, BK, TM, TN, STAGES, MINB, A_MN, B_MN>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
   const long tiles = ((a.m + BM - 1) / BM) * ((a.n + BN - 1) / BN);
   if (tiles > 0x7fffffffL) return cudaErrorInvalidValue;
   dim3 grid((unsigned)tiles, (unsigned)(a.batch < 65535 ? a.batch : 65535));

@@ -12,6 +12,7 @@
 // memory k-major (the transposes are absorbed by the staging loads), double-buffered through
 // registers; each thread owns a TM x TN sub-tile whose rows are spaced by BM/TM so that the
 // column-major C stores of a warp are contiguous.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -49,12 +50,32 @@ template <> struct RowTraits<int8_t> {
   }
 };
 
+// fp16 row of the type extensions: fp16 inputs, fp32 scale and accumulation, C in fp16 or fp32
+struct HalfC16 {};
+struct HalfC32 {};
+template <> struct RowTraits<HalfC16> {
+  using AB = __half; using Acc = float; using C = __half; using S = float;
+  static __device__ __forceinline__ Acc mac(Acc acc, AB a, AB b) { return fmaf(__half2float(a), __half2float(b), acc); }
+  static __device__ __forceinline__ C epi(Acc acc, S alpha, S beta, const C* cptr) {
+    const float t = (beta == 0.0f) ? 0.0f : beta * __half2float(*cptr);
+    return __float2half_rn(fmaf(acc, alpha, t));
+  }
+};
+template <> struct RowTraits<HalfC32> {
+  using AB = __half; using Acc = float; using C = float; using S = float;
+  static __device__ __forceinline__ Acc mac(Acc acc, AB a, AB b) { return fmaf(__half2float(a), __half2float(b), acc); }
+  static __device__ __forceinline__ C epi(Acc acc, S alpha, S beta, const C* cptr) {
+    const float t = (beta == 0.0f) ? 0.0f : beta * (*cptr);
+    return fmaf(acc, alpha, t);
+  }
+};
+
 template <typename T>
 struct SimtArgs {
   int transa, transb;
   long m, n, k, lda, ldb, ldc, batch;
-  const T* const* A;
-  const T* const* B;
+  const typename RowTraits<T>::AB* const* A;
+  const typename RowTraits<T>::AB* const* B;
   typename RowTraits<T>::C* const* C;
   typename RowTraits<T>::S alpha, beta;
 };
@@ -95,7 +116,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
         if (a_n) { ii = idx % BM; kk = idx / BM; }   // rows contiguous
         else { kk = idx % BK; ii = idx / BK; }                              // k contiguous
         long gi = m0 + ii, gk = k0 + kk;
-        AB v = AB(0);
+        AB v = AB(0.0f);
         if (gi < args.m && gk < args.k)
           v = (a_n) ? A[gi + gk * args.lda] : A[gi * args.lda + gk];
         ra[e] = v;
@@ -107,7 +128,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
         if (b_n) { kk = idx % BK; jj = idx / BK; }   // k contiguous
         else { jj = idx % BN; kk = idx / BN; }                              // cols contiguous
         long gj = n0 + jj, gk = k0 + kk;
-        AB v = AB(0);
+        AB v = AB(0.0f);
         if (gj < args.n && gk < args.k)
           v = (b_n) ? B[gk + gj * args.ldb] : B[gk * args.ldb + gj];
         rb[e] = v;
@@ -173,7 +194,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs<T>& args, long b, long 
 #pragma unroll
       for (int r = 0; r < TM; ++r) {
         const long gi = m0 + tx + r * TX;
-        cv[r] = (read_c && gi < args.m) ? Cm[gi + gj * args.ldc] : typename Tr::C(0);
+        cv[r] = (read_c && gi < args.m) ? Cm[gi + gj * args.ldc] : typename Tr::C(0.0f);
       }
 #pragma unroll
       for (int r = 0; r < TM; ++r) {
@@ -230,7 +251,7 @@ SimtArgs<T> make_args(const BatchDesc& d) {
   SimtArgs<T> a;
   a.transa = d.transa; a.transb = d.transb;
   a.m = d.m; a.n = d.n; a.k = d.k; a.lda = d.lda; a.ldb = d.ldb; a.ldc = d.ldc; a.batch = d.batch;
-  a.A = (const T* const*)d.A; a.B = (const T* const*)d.B;
+  a.A = (const typename RowTraits<T>::AB* const*)d.A; a.B = (const typename RowTraits<T>::AB* const*)d.B;
   a.C = (typename RowTraits<T>::C* const*)d.C;
   return a;
 }
@@ -261,9 +282,22 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
                  : launch_tile<double, 64, 64, 16, 4, 4>(a, stream);
     }
     case ROW_I8: {
+      // signed operands only (the unsigned ones of the type extensions take the tensor-core
+      // path; with k = 0 no operand is read)
+      if ((d.a_unsigned || d.b_unsigned) && d.k > 0) return cudaErrorNotSupported;
       auto a = make_args<int8_t>(d);
       a.alpha = d.alpha_i; a.beta = d.beta_i;
       return launch_tile<int8_t, 64, 64, 32, 4, 4>(a, stream);
+    }
+    case ROW_F16: {
+      if (d.c_f32) {
+        auto a = make_args<HalfC32>(d);
+        a.alpha = d.alpha_f; a.beta = d.beta_f;
+        return launch_tile<HalfC32, 64, 64, 16, 4, 4>(a, stream);
+      }
+      auto a = make_args<HalfC16>(d);
+      a.alpha = d.alpha_f; a.beta = d.beta_f;
+      return launch_tile<HalfC16, 64, 64, 16, 4, 4>(a, stream);
     }
   }
   return cudaErrorInvalidValue;

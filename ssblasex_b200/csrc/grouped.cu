@@ -386,13 +386,8 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tc::tc_gemm_kernel<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cfg::SMEM);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static bool attr_set[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr_set, tc::tc_gemm_kernel<Cfg, true>, Cfg::SMEM)) return e;
   tc::Params prm{};
   prm.total_tiles = kd.ntiles;
   prm.tiles_m = prm.tiles_n = 1;

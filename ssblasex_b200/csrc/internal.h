@@ -5,11 +5,18 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/ssblasBatch.h"
+#include "per_device.h"
 
 namespace ssb {
 
-enum Row { ROW_F32 = 0, ROW_F64 = 1, ROW_I8 = 2 };
+// Type rows: the reference's three (fp32, fp64, int8 -> int32), plus the fp16 row of the type
+// extensions (fp16 inputs, fp16 or fp32 C, fp32 scale and accumulation).
+enum Row { ROW_F32 = 0, ROW_F64 = 1, ROW_I8 = 2, ROW_F16 = 3 };
 
 // One uniform batch: every instance has the same shape; the pointer arrays live in device memory.
 struct BatchDesc {
@@ -30,6 +37,12 @@ struct BatchDesc {
   double alpha_d, beta_d;
   float alpha_f, beta_f;
   int32_t alpha_i, beta_i;
+  // int8 row: operands of type SSBLAS_R_8U (type extensions); fp16 row: C in fp32 instead of fp16
+  bool a_unsigned, b_unsigned;
+  bool c_f32;
+  // fp32 row with computeType SSBLAS_COMPUTE_32F under SSBLAS_EXT_COMPUTE_TYPE: FP32 arithmetic
+  // (no 3xBF16 emulation)
+  bool exact_f32;
 };
 
 // Process-wide knobs (set through the extension entry points)
@@ -37,9 +50,36 @@ struct Settings {
   cudaStream_t stream = nullptr;
   bool synchronous = true;
   int math_mode = SSBLAS_MATH_PLAIN;
-  int ozaki_slices = 0;        // 0 = automatic
+  int ozaki_slices = 0;        // 0 = automatic: from ozaki_tolerance
+  double ozaki_tolerance = 0;  // 0 = kOzakiDefaultTolerance
+  int fault = 0;               // one-shot ssblasFault_t armed by ssblasSetFaultInjection
+  int extensions = 0;          // ssblasExtension_t flags (ssblasSetExtensions)
 };
 Settings& settings();
+
+// Host-side lock of the library state (settings, run info, workspaces, per-device tables): every
+// entry point that launches work holds it for the whole call.
+std::unique_lock<std::mutex> lock_api();
+// Clears the run info of ssblasGetLastRunInfo at the start of a call.
+void reset_run_info();
+// Waits for `st`, reads and clears the device error flag; INTERNAL_ERROR (and the flag's code in
+// the run info) when a kernel's bounded wait gave up.
+ssblasStatus_t check_device_error(cudaStream_t st);
+
+// ---- Ozaki slice count ----
+// A-priori bound of the Ozaki emulation with S int8 slices per operand, per product term, in units
+// of |alpha| * 2^(e_i + f_j) (2^e_i, 2^f_j: the powers of two just above the largest magnitude of
+// row i of op(A) and of column j of op(B)): (S + 1) * 2^(2 - 8S). It covers rounding op(A) and
+// op(B) to 8S - 2 bits below their row (column) exponent and the dropped slice pairs p + q >= S.
+double ozaki_term_bound(int slices);
+// Default target of the slice choice: 4u (u = 2^-53), the 4*k*u tolerance of an FP64 GEMM spread
+// over its k product terms. It gives 7 slices.
+constexpr double kOzakiDefaultTolerance = 0x1p-51;
+// Slices of the next fp64 Ozaki call: the forced count (ssblasSetOzakiSlices), else the smallest
+// count in [3, 8] whose bound meets the tolerance (ssblasSetOzakiTolerance).
+int ozaki_slices_for_call();
+// The tensor-core paths can run here (sm_100 device, tensor-map encoder present).
+bool tcgen05_available();
 
 // Device workspace: a grow-only cached allocation per device and slot.
 enum WsSlot { WS_PTRS = 0, WS_PACK_A, WS_PACK_B, WS_EXP, WS_STAGE_A, WS_STAGE_B, WS_STAGE_C, WS_MISC, WS_SPLIT,
@@ -70,7 +110,23 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int slices, const int8_t* p
                                  const int32_t* exps, long Kp, cudaStream_t stream);
 // fp32 via three BF16 products
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t stream);
+// fp16 inputs (type extension row) on tcgen05 kind::f16, fp32 accumulation
+cudaError_t launch_f16_tcgen05(const BatchDesc& d, cudaStream_t stream);
 
+// Ordinal of the current device, or -1 when it cannot be read or lies outside the per-device
+// tables (per_device.h).
+int current_device();
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) of `kern` on the current device, once per
+// device (`done` is the caller's per-kernel table): the attribute belongs to one device's context.
+template <class K>
+inline cudaError_t smem_attr_once(bool (&done)[kMaxDevices], K kern, int bytes) {
+  return (cudaError_t)once_per_device(
+      done, current_device(),
+      [&] { return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); },
+      (int)cudaErrorInvalidDevice);
+}
+
+// SM count of the current device.
 int num_sms();
 
 // Tiled TMA tensor map of `rank` dimensions (dims[0] innermost; strides_bytes[i] is the stride
@@ -83,13 +139,26 @@ bool make_tiled_map(CUtensorMap* map, CUtensorMapDataType dt, int rank, const vo
 int choose_config(int path, long m, long n, long k, long batch, int fallback);
 
 // Optional per-kernel CUDA-event timing (ssblasSetProfiling): records an event pair around each
-// launch on its stream; ssblasGetProfile resolves them.
+// launch on its stream; ssblasGetProfile resolves them. Each launch is also an NVTX range of the
+// same name (slicing, GEMM, pre-pass phases), nested in the range of the API call, for timeline
+// tools; with no tool attached an NVTX call is a test of one function pointer.
 void prof_start(const char* name, cudaStream_t st);
 void prof_stop(cudaStream_t st);
 struct ProfScope {
   cudaStream_t st;
-  ProfScope(const char* name, cudaStream_t s) : st(s) { prof_start(name, s); }
-  ~ProfScope() { prof_stop(st); }
+  ProfScope(const char* name, cudaStream_t s) : st(s) {
+    nvtxRangePushA(name);
+    prof_start(name, s);
+  }
+  ~ProfScope() {
+    prof_stop(st);
+    nvtxRangePop();
+  }
+};
+// NVTX range of one API call.
+struct ApiRange {
+  explicit ApiRange(const char* name) { nvtxRangePushA(name); }
+  ~ApiRange() { nvtxRangePop(); }
 };
 
 }  // namespace ssb

@@ -25,7 +25,6 @@
 
 #include <cstdio>
 #include <cstdlib>
-#include <mutex>
 
 #include "internal.h"
 #include "prepass.h"
@@ -34,23 +33,20 @@ namespace ssb {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 64ull << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxDevices] = {};
+void* g_noalloc_ptr[kMaxDevices] = {};   // device address of the array, per device
 
 // Device address of g_noalloc_scratch on the current device (host code cannot use the symbol
-// itself: in host code its name is only a stand-in for the device object).
+// itself: in host code its name is only a stand-in for the device object). Called with the
+// library lock held.
 cudaError_t scratch_address(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  const int dev = current_device();
+  if (dev < 0) return cudaErrorInvalidDevice;
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_noalloc_ptr[dev] = p;
   }
@@ -67,7 +63,29 @@ bool on_device(const void* p) {
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
-inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
+inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Layout of the scratch array for one call: S slice planes of op(A), then of op(B) (each region
+// 256-byte aligned), then the int32 exponents of both. False when the sizes overflow or the
+// layout does not fit the array.
+struct ScratchLayout {
+  size_t off_b = 0, off_e = 0, need = 0;
+};
+bool scratch_layout(int S, long m, long n, long Kp, long batch, ScratchLayout* L) {
+  // every factor alone must fit before any product is formed
+  const size_t cap = kNoAllocScratchBytes;
+  if ((size_t)m > cap || (size_t)n > cap || (size_t)Kp > cap || (size_t)batch > cap) return false;
+  size_t bytes_a, bytes_b, bytes_e, t;
+  if (__builtin_mul_overflow((size_t)S * (size_t)m, (size_t)Kp, &t) || __builtin_mul_overflow(t, (size_t)batch, &bytes_a) ||
+      __builtin_mul_overflow((size_t)S * (size_t)n, (size_t)Kp, &t) || __builtin_mul_overflow(t, (size_t)batch, &bytes_b) ||
+      __builtin_mul_overflow(sizeof(int32_t) * ((size_t)m + (size_t)n), (size_t)batch, &bytes_e))
+    return false;
+  if (bytes_a > cap || bytes_b > cap || bytes_e > cap) return false;
+  L->off_b = round_up(bytes_a, 256);
+  L->off_e = round_up(L->off_b + bytes_b, 256);
+  L->need = L->off_e + bytes_e;
+  return L->need <= cap;
+}
 
 }  // namespace
 }  // namespace ssb
@@ -93,26 +111,26 @@ extern "C" ssblasStatus_t ssblasGemmBatchedExNoAlloc(
   const long arows = (transa == SSBLAS_OP_N) ? m : k, brows = (transb == SSBLAS_OP_N) ? k : n;
   if (lda < arows || ldb < brows || ldc < m) return SSBLAS_STATUS_INVALID_VALUE;
   if (k > 16384) return SSBLAS_STATUS_INVALID_VALUE;   // int32 exactness bound of the emulation
+
+  ApiRange range("ssblasGemmBatchedExNoAlloc");
+  auto lock = lock_api();
+  reset_run_info();
+  const int S = ozaki_slices_for_call();
+  const long Kp = (k + 15) / 16 * 16;
+  ScratchLayout L;
+  if (!scratch_layout(S, m, n, Kp, batchCount, &L)) {
+    fprintf(stderr,
+            "ssblasGemmBatchedExNoAlloc: a %ld x %ld x %ld problem of %ld instances with %d slices needs more "
+            "scratch than the static maximum of %zu bytes (use ssblasGemmBatchedEx, or split the batch)\n",
+            (long)m, (long)n, (long)k, (long)batchCount, S, kNoAllocScratchBytes);
+    return SSBLAS_STATUS_INVALID_VALUE;
+  }
+  // nothing is launched on a device the tensor-core kernels do not support
+  if (!tcgen05_available()) return SSBLAS_STATUS_NOTIMPLEMENTED_ERROR;
   // this entry point takes device arrays of device pointers only: staging host data would allocate
   if (!on_device((const void*)A) || !on_device((const void*)B) || !on_device((const void*)C))
     return SSBLAS_STATUS_INVALID_VALUE;
 
-  const int S = settings().ozaki_slices == 0 ? 7 : settings().ozaki_slices;
-  const long Kp = round_up(k, 16);
-  const size_t bytes_a = (size_t)S * m * Kp * batchCount;
-  const size_t bytes_b = (size_t)S * n * Kp * batchCount;
-  const size_t bytes_e = sizeof(int32_t) * (size_t)(m + n) * batchCount;
-  const size_t off_b = round_up((long)bytes_a, 256), off_e = round_up((long)(off_b + bytes_b), 256);
-  const size_t need = off_e + bytes_e;
-  if (need > kNoAllocScratchBytes) {
-    fprintf(stderr,
-            "ssblasGemmBatchedExNoAlloc: this problem needs %zu bytes of scratch; the static maximum is %zu "
-            "bytes (use ssblasGemmBatchedEx, or split the batch)\n",
-            need, kNoAllocScratchBytes);
-    return SSBLAS_STATUS_INVALID_VALUE;
-  }
-
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   void* scratch = nullptr;
   cudaError_t e = scratch_address(&scratch);
   if (e != cudaSuccess) {
@@ -120,8 +138,8 @@ extern "C" ssblasStatus_t ssblasGemmBatchedExNoAlloc(
     return SSBLAS_STATUS_INTERNAL_ERROR;
   }
   int8_t* pa = (int8_t*)scratch;
-  int8_t* pb = (int8_t*)scratch + off_b;
-  int32_t* ex = (int32_t*)((uint8_t*)scratch + off_e);
+  int8_t* pb = (int8_t*)scratch + L.off_b;
+  int32_t* ex = (int32_t*)((uint8_t*)scratch + L.off_e);
 
   BatchDesc d{};
   d.row = ROW_F64;
@@ -142,14 +160,6 @@ extern "C" ssblasStatus_t ssblasGemmBatchedExNoAlloc(
     return SSBLAS_STATUS_INTERNAL_ERROR;
   }
   if (!settings().synchronous) return SSBLAS_STATUS_SUCCESS;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return SSBLAS_STATUS_INTERNAL_ERROR;
-  int* flag = device_error_flag();
-  int h = 0;
-  if (!flag || cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SSBLAS_STATUS_INTERNAL_ERROR;
-  if (h != 0) {
-    const int zero = 0;
-    cudaMemcpy(flag, &zero, sizeof(int), cudaMemcpyHostToDevice);
-    return SSBLAS_STATUS_INTERNAL_ERROR;
-  }
-  return SSBLAS_STATUS_SUCCESS;
+  // same device-error reporting as the other entry points (run info records the flag's code)
+  return check_device_error(st);
 }

@@ -944,12 +944,8 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
                               int KB = 1) {
   constexpr int SMEM = ClShape<R, KC, NTH, RUNS>::template smem_bytes<S>();
   auto kern = ozaki_cluster_kernel<S, TMA, R, KC, NTH, RUNS, BITS>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.blockDim = dim3(NTH, 1, 1);
   cfg.dynamicSmemBytes = SMEM;
@@ -962,7 +958,10 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   cfg.attrs = at;
   cfg.numAttrs = 1;
   // persistent clusters: as many as fit at once (CL_NTH / NTH CTAs per SM), at most one per item
-  static int max_clusters[9] = {0};
+  static int max_clusters_dev[kMaxDevices][9] = {};
+  const int dev = current_device();
+  if (dev < 0) return cudaErrorInvalidDevice;
+  int (&max_clusters)[9] = max_clusters_dev[dev];
   if (max_clusters[CS] == 0) {
     cfg.gridDim = dim3((unsigned)(CS * num_sms() * (CL_NTH / NTH)), 1, 1);
     int nc = 0;

@@ -41,10 +41,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 
 // Every wait in the library's kernels is bounded. When a wait gives up, the kernel records
 // `code` in the device error flag and the caller abandons its loop; the host turns a set flag
-// into SSBLAS_STATUS_INTERNAL_ERROR.
+// into SSBLAS_STATUS_INTERNAL_ERROR. `limit` is the number of try_wait rounds (kWaitLimit unless
+// a launch asks for a shorter one, as the fault-injection test does).
 constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code,
+                                          uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   if (err) atomicExch(err, code);
   return false;
@@ -145,15 +147,37 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, int swz_byt
   return d;
 }
 
-// Instruction descriptor (kind::i8 / kind::f16, dense, both operands K-major).
+// Shared-memory matrix descriptor for an MN-major operand tile in the 128-byte swizzled layout:
+// the tile is stored as blocks of 128 bytes of M (or N) by the stage's K rows, each K row one
+// 128-byte line (8-row groups 1024 bytes apart: stride byte offset), consecutive 128-byte M blocks
+// `mn_block_bytes` apart (leading byte offset). The start address must sit on a 1024-byte boundary;
+// advancing along K by 8 rows adds 1024 bytes.
+__device__ __forceinline__ uint64_t smem_desc_mnmajor(uint32_t saddr, uint32_t mn_block_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);                // start address, bits 0-13
+  d |= (uint64_t)((mn_block_bytes >> 4) & 0x3FFF) << 16;  // leading byte offset: next M block
+  d |= (uint64_t)(1024 >> 4) << 32;                       // stride byte offset: next 8 K rows
+  d |= (uint64_t)1 << 46;                                 // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;                                 // 128-byte swizzle
+  return d;
+}
+
+// Instruction descriptor (kind::i8 / kind::f16, dense).
 //   c_format bits 4-5 (1 = f32, 2 = s32); a_format bits 7-9, b_format bits 10-12
-//   (i8: 1 = signed; f16 kind: 0 = f16, 1 = bf16); N >> 3 at bits 17-22; M >> 4 at bits 24-28.
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N, bool a_signed, bool b_signed) {
-  return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | ((b_signed ? 1u : 0u) << 10) |
-         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+//   (i8: 0 = unsigned, 1 = signed; f16 kind: 0 = f16, 1 = bf16); bits 15/16: A/B MN-major (else
+//   K-major); N >> 3 at bits 17-22; M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N, bool a_signed, bool b_signed, bool a_mn = false,
+                                                bool b_mn = false) {
+  return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | ((b_signed ? 1u : 0u) << 10) | ((a_mn ? 1u : 0u) << 15) |
+         ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// fp16 inputs, fp32 accumulation (kind::f16 with a_format = b_format = f16)
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn = false, bool b_mn = false) {
+  return (1u << 4) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
 }
 
 }  // namespace ptx

@@ -21,6 +21,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -38,8 +39,8 @@ constexpr int threads_of() { return GROUPED ? kThreadsGrouped : kThreads; }
 // (kNonFiniteExp of ozaki_digits.cuh)
 constexpr int kOzakiNonFiniteExp = 4096;
 
-enum Kind { KIND_I8 = 0, KIND_BF16 = 1 };
-enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2 };
+enum Kind { KIND_I8 = 0, KIND_BF16 = 1, KIND_F16 = 2 };
+enum Epi { EPI_I32 = 0, EPI_F32 = 1, EPI_OZAKI = 2, EPI_F16 = 3 };
 
 // Grouped launches: one entry per instance ...
 struct GInst {
@@ -95,6 +96,13 @@ struct Params {
   int kb_per_split;
   int32_t* split_ws;
   int* split_cnt;
+  // fault injection (ssblasSetFaultInjection): try_wait rounds of every wait (0 = kWaitLimit), and
+  // the stage (producer iteration) whose operand copy CTA 0 skips (-1 = none), so that the waits
+  // on it run out and the kernel reports through the error flag
+  uint32_t wait_limit;
+  long skip_copy;
+  // int8 kinds: bit 0 = op(A) unsigned, bit 1 = op(B) unsigned (0: both signed)
+  int ab_unsigned;
 };
 
 // Grouped launches take tiles from a device-side queue: a scheduler warp (warp 10) of each CTA
@@ -133,7 +141,8 @@ __device__ __forceinline__ TileInfo tile_info(const Params& p, long t, long tile
   return ti;
 }
 
-template <int KIND_, int PA_, int PB_, int BN_, int KB_, int STAGES_, int NLEV_, int ACCB_, int EPI_, int PAIRS_>
+template <int KIND_, int PA_, int PB_, int BN_, int KB_, int STAGES_, int NLEV_, int ACCB_, int EPI_, int PAIRS_,
+          int AMN_ = 0, int BMN_ = 0>
 struct Config {
   static constexpr int KIND = KIND_;
   static constexpr int PA = PA_;       // planes of A
@@ -146,7 +155,19 @@ struct Config {
   static constexpr int ACCB = ACCB_;   // accumulator buffers (2 = epilogue overlaps next tile)
   static constexpr int EPI = EPI_;
   static constexpr int PAIRS = PAIRS_; // 0: (0,0) only; 1: p+q <= 1 (bf16x3); 2: p+q < NLEV (Ozaki)
+  // Operand staging: K-major (K contiguous, the packed planes and transposed inputs) or MN-major
+  // (M or N contiguous: the caller's column-major op(A) = A, op(B) = B^T staged as they lie, so
+  // the transpose costs nothing). MN-major tiles are blocks of 128 bytes of M (N) by the stage's
+  // K rows, each K row one 128-byte swizzled line.
+  static constexpr bool AMN = AMN_ != 0;
+  static constexpr bool BMN = BMN_ != 0;
   static constexpr int ELEM = (KIND == KIND_I8) ? 1 : 2;
+  static constexpr int KROWS = KB_ / ELEM;             // K elements (MN-major: K rows) per stage
+  static constexpr int MN_BLOCK = KROWS * 128;         // bytes of one 128-byte-wide MN block
+  static_assert(!(AMN || BMN) || (PA_ == 1 && PB_ == 1 && PAIRS_ == 0 && KB_ == 128),
+                "MN-major staging is for single-plane operands with 128-byte K stages");
+  // split-K adds the pieces' sums afterwards: only exact integer sums give the unsplit result
+  static constexpr bool SPLITTABLE = EPI_ == EPI_I32 || EPI_ == EPI_OZAKI;
   static constexpr int A_STAGE = PA * BM * KB;
   static constexpr int B_STAGE = PB * BN * KB;
   static constexpr int STAGE = A_STAGE + B_STAGE;
@@ -408,6 +429,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   int* err = prm.err;
+  const uint32_t wl = prm.wait_limit ? prm.wait_limit : ptx::kWaitLimit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -456,7 +478,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         if constexpr (GROUPED) {
           // the next record of the tile queue
           const int slot = (int)(i % kTQ);
-          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((i / kTQ) & 1), err, 13)) break;
+          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((i / kTQ) & 1), err, 13, wl)) break;
           const TileDesc& d = tq[slot];
           if (!d.valid) break;
           ti.mt = d.mt; ti.nt = d.nt; ti.kb0 = 0; ti.kb1 = d.g.nk;
@@ -470,7 +492,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         for (int kb = ti.kb0; kb < ti.kb1; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
-          if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11)) { ok = false; break; }
+          if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11, wl)) { ok = false; break; }
+          if (!GROUPED && it == prm.skip_copy && blockIdx.x == 0) continue;   // injected fault
           const uint32_t fb = ptx::smem_u32(&full[s]);
           ptx::mbar_arrive_expect_tx(fb, Cfg::STAGE);
           uint8_t* sa = stages + (size_t)s * Cfg::STAGE;
@@ -478,20 +501,38 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             ptx::bulk_load(ptx::smem_u32(sa), srcA + (size_t)kb * Cfg::A_STAGE, Cfg::A_STAGE, fb);
             ptx::bulk_load(ptx::smem_u32(sa + Cfg::A_STAGE), srcB + (size_t)kb * Cfg::B_STAGE, Cfg::B_STAGE, fb);
           } else {
-            ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, ti.mt * Cfg::BM, 0, ti.b);
-            ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, ti.nt * Cfg::BN, 0, ti.b);
+            if constexpr (Cfg::AMN) {
+              // tensor map {M, K, 1, batch}: one 128-byte-wide M block per copy
+#pragma unroll
+              for (int j = 0; j < Cfg::BM * Cfg::ELEM / 128; ++j)
+                ptx::tma_load_4d(ptx::smem_u32(sa + j * Cfg::MN_BLOCK), &tmA, fb, ti.mt * Cfg::BM + j * (128 / Cfg::ELEM),
+                                 kb * KE, 0, ti.b);
+            } else {
+              ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, ti.mt * Cfg::BM, 0, ti.b);
+            }
+            if constexpr (Cfg::BMN) {
+#pragma unroll
+              for (int j = 0; j < Cfg::BN * Cfg::ELEM / 128; ++j)
+                ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE + j * Cfg::MN_BLOCK), &tmB, fb,
+                                 ti.nt * Cfg::BN + j * (128 / Cfg::ELEM), kb * KE, 0, ti.b);
+            } else {
+              ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, ti.nt * Cfg::BN, 0, ti.b);
+            }
           }
         }
       }
       // no copy may still be in flight when the CTA exits
       for (long j = (it > Cfg::STAGES ? it - Cfg::STAGES : 0); j < it; ++j)
-        ptx::mbar_wait(ptx::smem_u32(&full[j % Cfg::STAGES]), (uint32_t)((j / Cfg::STAGES) & 1), err, 12);
+        ptx::mbar_wait(ptx::smem_u32(&full[j % Cfg::STAGES]), (uint32_t)((j / Cfg::STAGES) & 1), err, 12, wl);
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------------ MMA issuer --------
     if (lane == 0) {
-      constexpr uint32_t IDESC = (Cfg::KIND == KIND_I8) ? ptx::idesc_i8(128, Cfg::BN, true, true)
-                                                        : ptx::idesc_bf16(128, Cfg::BN);
+      const uint32_t IDESC =
+          (Cfg::KIND == KIND_I8)
+              ? ptx::idesc_i8(128, Cfg::BN, !(prm.ab_unsigned & 1), !(prm.ab_unsigned & 2), Cfg::AMN, Cfg::BMN)
+          : (Cfg::KIND == KIND_F16) ? ptx::idesc_f16(128, Cfg::BN, Cfg::AMN, Cfg::BMN)
+                                    : ptx::idesc_bf16(128, Cfg::BN);
       long it = 0;
       int tcount = 0;
       bool ok = true;
@@ -500,7 +541,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         int slot = 0;
         if constexpr (GROUPED) {
           slot = tcount % kTQ;
-          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 24)) break;
+          if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 24, wl)) break;
           if (!tq[slot].valid) break;
           ti.kb0 = 0;
           ti.kb1 = tq[slot].g.nk;
@@ -511,14 +552,14 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         const int acc = tcount % Cfg::ACCB;
         const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
-        if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21)) { ok = false; break; }
+        if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21, wl)) { ok = false; break; }
         ptx::tc_fence_after();
         const uint32_t d_base = tmem_base + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
         for (int kb = ti.kb0; kb < ti.kb1; ++kb, ++it) {
           const int s = (int)(it % Cfg::STAGES);
           const uint32_t ph = (uint32_t)((it / Cfg::STAGES) & 1);
           const bool acc_k = kb > ti.kb0;   // this K block adds to the blocks before it
-          if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), ph, err, 22)) { ok = false; break; }
+          if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), ph, err, 22, wl)) { ok = false; break; }
           ptx::tc_fence_after();
           const uint32_t sa = ptx::smem_u32(stages + (size_t)s * Cfg::STAGE);
           const uint32_t sb = sa + Cfg::A_STAGE;
@@ -552,8 +593,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               const uint32_t d = d_base + (uint32_t)(Cfg::level(p, q) * Cfg::BN);
 #pragma unroll
               for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
-                const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
-                const uint64_t bd = ptx::smem_desc_kmajor(sb + q * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
+                // one MMA covers 32 bytes of K: 32 / ELEM K rows of an MN-major tile
+                const uint64_t ad = Cfg::AMN ? ptx::smem_desc_mnmajor(sa + kk * (32 / Cfg::ELEM) * 128, Cfg::MN_BLOCK)
+                                             : ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
+                const uint64_t bd = Cfg::BMN ? ptx::smem_desc_mnmajor(sb + kk * (32 / Cfg::ELEM) * 128, Cfg::MN_BLOCK)
+                                             : ptx::smem_desc_kmajor(sb + q * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
                 const uint32_t accum = (acc_k || kk > 0 || !Cfg::first_of_level(p, q)) ? 1u : 0u;
                 if (Cfg::KIND == KIND_I8) ptx::mma_i8(d, ad, bd, IDESC, accum);
                 else ptx::mma_f16(d, ad, bd, IDESC, accum);
@@ -567,7 +611,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         ptx::mma_commit(ptx::smem_u32(&tfull[acc]));     // accumulator ready for the epilogue
       }
       ptx::mma_commit(ptx::smem_u32(drain));
-      ptx::mbar_wait(ptx::smem_u32(drain), 0, err, 23);
+      ptx::mbar_wait(ptx::smem_u32(drain), 0, err, 23, wl);
     }
   } else if (GROUPED && warp == 10) {
     // ------------------------------------------------------------------ scheduler ---------
@@ -577,7 +621,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         const long rec = i + lane;
         const int slot = (int)(rec % kTQ);
         bool ok = true;
-        if (lane < kSB) ok = ptx::mbar_wait(ptx::smem_u32(&tq_empty[slot]), (uint32_t)(((rec / kTQ) & 1) ^ 1), err, 14);
+        if (lane < kSB) ok = ptx::mbar_wait(ptx::smem_u32(&tq_empty[slot]), (uint32_t)(((rec / kTQ) & 1) ^ 1), err, 14, wl);
         // dynamic order: kSB consecutive tiles per claim; static order: the CTA's stride
         unsigned long long base = 0;
         if (prm.queue && lane == 0) base = atomicAdd(prm.queue, (unsigned long long)kSB);
@@ -615,7 +659,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       int slot = 0;
       if constexpr (GROUPED) {
         slot = tcount % kTQ;
-        if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 32)) break;
+        if (!ptx::mbar_wait(ptx::smem_u32(&tq_full[slot]), (uint32_t)((tcount / kTQ) & 1), err, 32, wl)) break;
         if (!tq[slot].valid) break;
         ti.mt = tq[slot].mt;
         ti.nt = tq[slot].nt;
@@ -659,14 +703,14 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
       const int acc = tcount % Cfg::ACCB;
       const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
-      if (!ptx::mbar_wait(ptx::smem_u32(&tfull[acc]), acc_ph, err, 31)) break;
+      if (!ptx::mbar_wait(ptx::smem_u32(&tfull[acc]), acc_ph, err, 31, wl)) break;
       ptx::tc_fence_after();
       const long gi = (long)ti.mt * Cfg::BM + row_in_tile;
       const long n0 = (long)ti.nt * Cfg::BN + half * HALF;
       const uint32_t t_row = tmem_base + ((uint32_t)(quarter * 32) << 16) +
                              (uint32_t)(acc * Cfg::NLEV * Cfg::BN + half * HALF);
       const bool row_ok = gi < m;
-      if constexpr (SPLIT && !GROUPED && Cfg::EPI != EPI_F32) {
+      if constexpr (SPLIT && !GROUPED && Cfg::SPLITTABLE) {
         {
           split_k_region<Cfg, HALF>(t_row, prm.split_ws, prm.split_cnt, t / prm.splits, prm.splits, ti.sp, half,
                                     warp - 2, row_in_tile, lane, ptx::smem_u32(&tempty[acc]), row_ok, Cb, gi, n0, n,
@@ -724,6 +768,29 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         if (!row_ok) continue;
         if (Cfg::EPI == EPI_I32) {
           i32_store<GC>((int32_t*)Cb + gi * rs, n0 + g0, n, ldc, alpha_i, beta_i, raw);
+        } else if (Cfg::EPI == EPI_F16) {
+          // fp16 C: alpha * acc + beta * C in fp32, rounded once to fp16
+          __half* Ch = (__half*)Cb + gi * rs;
+          float cv[GC][16];
+          if (beta_f != 0.0f) {
+#pragma unroll
+            for (int c = 0; c < GC; ++c)
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                const long gj = n0 + g0 + 16 * c + j;
+                cv[c][j] = (gj < n) ? __half2float(Ch[gj * ldc]) : 0.0f;
+              }
+          }
+#pragma unroll
+          for (int c = 0; c < GC; ++c)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const long gj = n0 + g0 + 16 * c + j;
+              if (gj < n) {
+                const float tb = (beta_f == 0.0f) ? 0.0f : beta_f * cv[c][j];
+                Ch[gj * ldc] = __float2half_rn(fmaf(__uint_as_float(raw[c][j]), alpha_f, tb));
+              }
+            }
         } else {
           float* Cf = (float*)Cb + gi * rs;
           float cv[GC][16];

@@ -29,7 +29,17 @@ ROW_TYPES = {
     "f32": (R_32F, R_32F, R_32F, np.float32, np.float32, np.float32),
     "f64": (R_64F, R_64F, R_64F, np.float64, np.float64, np.float64),
     "i8": (R_8I, R_8I, R_32I, np.int8, np.int32, np.int32),
+    # rows of the type extensions (ssblasSetExtensions): fp16 inputs with fp16 or fp32 C (float
+    # scale), and unsigned int8 operands (int32 scale and C)
+    "f16": (R_16F, R_16F, R_16F, np.float16, np.float32, np.float16),
+    "f16c32": (R_16F, R_16F, R_32F, np.float16, np.float32, np.float32),
+    "u8": (R_8U, R_8U, R_32I, np.uint8, np.int32, np.int32),
+    "u8s8": (R_8U, R_8I, R_32I, np.uint8, np.int32, np.int32),
+    "s8u8": (R_8I, R_8U, R_32I, np.int8, np.int32, np.int32),
 }
+# element type of op(B) where it differs from op(A)'s
+B_DTYPE = {"u8s8": np.int8, "s8u8": np.uint8}
+INT_ROWS = ("i8", "u8", "u8s8", "s8u8")
 
 
 def stored_shape(trans: int, rows: int, cols: int) -> tuple[int, int]:
@@ -111,8 +121,8 @@ def make_problem(row: str, transa: int, transb: int, m: int, n: int, k: int, bat
                  ldc: int | None = None, seed: int = 0, dist: str = "uniform",
                  name: str = "") -> Problem:
     """Seeded problem. dist: "uniform" (U[-1,1) for fp, U{-128..127}/U{-2^20..2^20} for int8),
-    "expspread" (sign * U[1,2) * 2^U{-8..8}), "outliers" (U[-1,1) with 1% of entries x 1e4),
-    "small_int" (int8 in {-3..3}, C in {-64..64})."""
+    "expspread" (sign * U[1,2) * 2^U{-8..8}; "expspreadN" for 2^U{-N..N}), "outliers" (U[-1,1)
+    with 1% of entries x 1e4), "small_int" (int8 in {-3..3}, C in {-64..64})."""
     rng = np.random.default_rng(seed)
     ar, ac = stored_shape(transa, m, k)
     br, bc = stored_shape(transb, k, n)
@@ -121,15 +131,19 @@ def make_problem(row: str, transa: int, transb: int, m: int, n: int, k: int, bat
     ldc = ldc if ldc is not None else max(1, m)
     _, _, _, abt, st, ct = ROW_TYPES[row]
 
-    def gen_ab(shape):
-        if row == "i8":
+    def gen_ab(shape, dtype=abt):
+        if row in INT_ROWS:
+            if dtype == np.uint8:
+                return rng.integers(0, 4 if dist == "small_int" else 256, size=shape, dtype=np.uint8)
             lo, hi = (-3, 4) if dist == "small_int" else (-128, 128)
-            return rng.integers(lo, hi, size=shape, dtype=np.int64).astype(np.int8)
-        if dist == "expspread":
-            sign = np.where(rng.random(shape) < 0.5, -1.0, 1.0)
-            mant = rng.uniform(1.0, 2.0, size=shape)
-            ex = rng.integers(-8, 9, size=shape)
-            return (sign * np.ldexp(mant, ex)).astype(abt)
+            return rng.integers(lo, hi, size=shape, dtype=np.int8)
+        if dist.startswith("expspread"):
+            span = int(dist[len("expspread"):] or 8)
+            # sign * U[1,2) as one uniform draw on (-2,-1] u [1,2), times 2^U{-span..span}
+            u = rng.uniform(-1.0, 1.0, size=shape)
+            mant = u + np.copysign(1.0, u)
+            ex = rng.integers(-span, span + 1, size=shape, dtype=np.int32)
+            return np.ldexp(mant, ex).astype(abt, copy=False)
         x = rng.uniform(-1.0, 1.0, size=shape)
         if dist == "outliers":
             mask = rng.random(shape) < 0.01
@@ -137,9 +151,9 @@ def make_problem(row: str, transa: int, transb: int, m: int, n: int, k: int, bat
         return x.astype(abt)
 
     def gen_c(shape):
-        if row == "i8":
+        if row in INT_ROWS:
             lim = 64 if dist == "small_int" else (1 << 20)
-            return rng.integers(-lim, lim + 1, size=shape, dtype=np.int64).astype(np.int32)
+            return rng.integers(-lim, lim + 1, size=shape, dtype=np.int32)
         return gen_ab(shape).astype(ct)
 
     def fill_operand(arr, srows, scols, ld, gen):
@@ -148,8 +162,9 @@ def make_problem(row: str, transa: int, transb: int, m: int, n: int, k: int, bat
 
     A = np.zeros((batch, lda * ac), dtype=abt)
     fill_operand(A, ar, ac, lda, gen_ab)
-    B = np.zeros((batch, ldb * bc), dtype=abt)
-    fill_operand(B, br, bc, ldb, gen_ab)
+    bbt = B_DTYPE.get(row, abt)
+    B = np.zeros((batch, ldb * bc), dtype=bbt)
+    fill_operand(B, br, bc, ldb, lambda shape: gen_ab(shape, bbt))
     C = np.zeros((batch, ldc * n), dtype=ct)
     fill_operand(C, m, n, ldc, gen_c)
     return Problem(row, transa, transb, m, n, k, lda, ldb, ldc, batch,

@@ -81,9 +81,43 @@ def status_cases():
     yield "m0_i8", dict(base, row="i8", alpha=1, beta=2), dict(m=0)
 
 
+# The benchmark configurations at their full shapes: the reference runs on the instances listed
+# (all of the 64 x 128^3 workload, a slice of the larger ones); the fixture keeps its output on
+# sampled rows of those instances plus the column sums over all rows (int64 for the int8 row, so
+# those compare exactly). The inputs are not stored: tests regenerate them from the workload's seed
+# (tests/test_oracle_golden.py checks that the regenerated inputs are the ones the reference saw).
+CONFIG_FIXTURES = [
+    ("fp32_batch64_128", list(range(64)), list(range(0, 128, 9))),
+    ("f64_batch32_1024", [0, 1], list(range(5, 1024, 67))),
+    ("i8_batch512_512", [0, 1], list(range(3, 512, 37))),
+    ("fp32_batch4096_64", list(range(0, 4096, 256)), list(range(64))),
+]
+CONFIG_OUT = pathlib.Path(__file__).resolve().parent / "config_cases.npz"
+
+
+def config_fixtures():
+    out = {}
+    for name, inst, rows in CONFIG_FIXTURES:
+        full = W.workload(name)
+        q = W.Problem(**{**full.__dict__, "batch": len(inst), "A": full.A[inst], "B": full.B[inst],
+                         "C": full.C[inst].copy()})
+        st, C = O.reference_gemm(q)
+        assert st == 0, (name, st)
+        views = [q.c_view(C, b) for b in range(q.batch)]
+        out[name + "_inst"] = np.array(inst, np.int64)
+        out[name + "_rows"] = np.array(rows, np.int64)
+        out[name + "_C"] = np.stack([v[rows, :] for v in views])
+        acc = np.int64 if q.row == "i8" else np.float64
+        out[name + "_colsum"] = np.stack([v.astype(acc).sum(axis=0) for v in views])
+        print(f"  {name}: {len(inst)} instances")
+    np.savez_compressed(CONFIG_OUT, **out)
+    print(f"wrote {CONFIG_OUT} ({CONFIG_OUT.stat().st_size / 1e6:.2f} MB)")
+
+
 def main():
     if os.environ.get("OMP_NUM_THREADS", "").strip() in {"2", "3", "4", "6"}:
         raise SystemExit("OMP_NUM_THREADS in {2,3,4,6} crashes the reference")
+    config_fixtures()
     out = {}
     meta = []
     for i, kw in enumerate(cases()):

@@ -63,7 +63,6 @@ def test_invalid_arguments_the_reference_does_not_check():
     p = W.make_problem("f32", 0, 0, 9, 8, 7, 2, 1.0, 0.0, seed=1)
     assert runner.call(p, mode="host_matrices", lda=8)[0] == S.SSBLAS_STATUS_INVALID_VALUE
     assert runner.call(p, mode="host_matrices", ldc=3)[0] == S.SSBLAS_STATUS_INVALID_VALUE
-    q = W.make_problem("i8", 2, 0, 9, 8, 7, 2, 1, 0, seed=1) if False else None
     # op C on the int8 row: the reference reads through NULL; here it is rejected
     p8 = W.make_problem("i8", 0, 0, 9, 8, 7, 2, 1, 0, seed=1)
     assert runner.call(p8, mode="host_matrices", transa=2)[0] == S.SSBLAS_STATUS_INVALID_VALUE
@@ -93,3 +92,104 @@ def test_debug_dump_is_the_reference_text():
     got = mg.dump_text(str(S.LIB_PATH))
     want = (ROOT / "tests" / "golden" / "debug_dump.txt").read_text()
     assert got == want
+
+
+def test_noalloc_refuses_sizes_whose_scratch_product_overflows():
+    """The allocation-free entry point sizes its scratch with overflow-checked products and refuses
+    a problem before any CUDA call: here (no GPU) a refusal that came later would read as
+    NOTIMPLEMENTED or INTERNAL_ERROR, not INVALID_VALUE."""
+    import ssblasex_b200 as S
+    al = np.array([1.0], np.float64)
+    arr = (ct.c_void_p * 1)()
+    f = S.lib().ssblasGemmBatchedExNoAlloc
+    R = S.SSBLAS_R_64F
+    cases = [
+        # 7 * 2^26 * 16384 * 2^26 bytes wraps a 64-bit size; every factor alone fits the array
+        (1 << 26, 1, 16384, 1 << 26),
+        # a dimension larger than the whole array
+        (1 << 40, 1, 16, 1),
+        (1, 1 << 40, 16, 1),
+        (1, 1, 16, 1 << 40),
+        # fits no wrap, still too big: 7 * (4096 + 4096) * 1024 * 2 bytes = 117 MB
+        (4096, 4096, 1024, 2),
+    ]
+    for m, n, k, batch in cases:
+        st = f(0, 0, m, n, k, al.ctypes.data, arr, R, m, arr, R, k, al.ctypes.data, arr, R, m, batch, 0, 0)
+        assert st == S.SSBLAS_STATUS_INVALID_VALUE, (m, n, k, batch, st)
+    # k beyond the exact int32 range of one piece
+    st = f(0, 0, 8, 8, 16385, al.ctypes.data, arr, R, 8, arr, R, 16385, al.ctypes.data, arr, R, 8, 1, 0, 0)
+    assert st == S.SSBLAS_STATUS_INVALID_VALUE
+
+
+def test_per_device_tables(tmp_path):
+    """The per-device tables (csrc/per_device.h) keep one entry per device ordinal: a kernel
+    attribute set on device 0 is set again on device 1, a failed set-up is retried, and ordinals
+    outside the table are refused without touching it."""
+    src = tmp_path / "t.cpp"
+    src.write_text(r'''
+#include "per_device.h"
+#include <cstdio>
+using namespace ssb;
+int main() {
+  bool done[kMaxDevices] = {};
+  int calls = 0, fail = 1;
+  auto init = [&] { ++calls; return fail ? 7 : 0; };
+  if (once_per_device(done, 0, init, -9) != 7 || calls != 1 || done[0]) return 1;     // failure not cached
+  fail = 0;
+  if (once_per_device(done, 0, init, -9) != 0 || calls != 2 || !done[0]) return 2;
+  if (once_per_device(done, 0, init, -9) != 0 || calls != 2) return 3;                 // cached
+  if (once_per_device(done, 1, init, -9) != 0 || calls != 3 || !done[1]) return 4;     // per device
+  if (once_per_device(done, -1, init, -9) != -9 || calls != 3) return 5;               // refused
+  if (once_per_device(done, kMaxDevices, init, -9) != -9 || calls != 3) return 6;
+  for (int d = 2; d < kMaxDevices; ++d) if (done[d]) return 7;
+  std::puts("ok");
+  return 0;
+}
+''')
+    exe = tmp_path / "t"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(ROOT / "ssblasex_b200" / "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout)
+
+
+def test_fault_injection_setter():
+    import ssblasex_b200 as S
+    for f in (S.SSBLAS_FAULT_SKIP_COPY, S.SSBLAS_FAULT_ALLOC, S.SSBLAS_FAULT_NONE):
+        assert S.set_fault_injection(f) == 0
+    for bad in (-1, 3, 99):
+        assert S.set_fault_injection(bad) == S.SSBLAS_STATUS_INVALID_VALUE
+
+
+def test_extension_flags_and_their_status_rules():
+    """Extensions are off by default; each changes a status rule in the documented way, checked
+    before any device work (no GPU here)."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    try:
+        assert S.get_extensions() == 0
+        assert S.set_extensions(32) == S.SSBLAS_STATUS_INVALID_VALUE
+        p = W.make_problem("f32", 0, 0, 9, 8, 7, 2, 1.0, 0.0, seed=1)
+        # computeType is ignored without the extension (the reference's behaviour) ...
+        assert S.set_extensions(S.SSBLAS_EXT_COMPUTE_TYPE) == 0
+        al = np.array([1.0], np.float32)
+        arr = (ct.c_void_p * 2)()
+        f = S.lib().ssblasGemmBatchedEx
+        # ... and checked against the row with it: 32I on the fp32 row is refused
+        assert f(0, 0, 4, 4, 4, al.ctypes.data, arr, 4, 4, arr, 4, 4, al.ctypes.data, arr, 4, 4, 2,
+                 S.SSBLAS_COMPUTE_32I, 0) == S.SSBLAS_STATUS_INVALID_VALUE
+        assert f(0, 0, 4, 4, 4, al.ctypes.data, arr, 4, 4, arr, 4, 4, al.ctypes.data, arr, 4, 4, 2,
+                 7, 0) == S.SSBLAS_STATUS_INVALID_VALUE
+        # k < 0 is refused under the k = 0 extension (the reference treats it as k = 0)
+        S.set_extensions(S.SSBLAS_EXT_K0_BETA)
+        assert runner.call(p, mode="host_matrices", k=-1)[0] == S.SSBLAS_STATUS_INVALID_VALUE
+        S.set_extensions(0)
+        assert runner.call(p, mode="host_matrices", k=-1)[0] == S.SSBLAS_STATUS_SUCCESS
+        # fp16 and unsigned int8 rows exist only with their flags
+        for row in ("f16", "f16c32", "u8", "u8s8"):
+            q = W.make_problem(row, 0, 0, 9, 8, 7, 2, 1, 0, seed=1)
+            assert runner.call(q, mode="host_matrices")[0] == S.SSBLAS_STATUS_INVALID_VALUE
+        # op C without the extension
+        assert runner.call(p, mode="host_matrices", transb=2)[0] == S.SSBLAS_STATUS_INVALID_VALUE
+    finally:
+        S.set_extensions(0)

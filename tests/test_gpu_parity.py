@@ -165,3 +165,28 @@ def test_fp32_batch4096_64_full(S):
     assert st == 0
     tol = fp_tolerance(p)
     assert O.normalized_error(p, C, instances=range(0, 4096, 257)) <= tol
+
+
+@pytest.fixture(scope="module")
+def config_fixtures():
+    import pathlib
+    return np.load(pathlib.Path(__file__).resolve().parent / "golden" / "config_cases.npz")
+
+
+@pytest.mark.parametrize("name,mode", [("fp32_batch64_128", 0), ("f64_batch32_1024", 0), ("f64_batch32_1024", 1),
+                                       ("i8_batch512_512", 0), ("fp32_batch4096_64", 0), ("fp32_batch4096_64", 2)])
+def test_reference_output_at_benchmark_shapes(S, config_fixtures, name, mode):
+    """The CUDA path against the reference's own output at the benchmark configurations' shapes
+    (tests/golden/config_cases.npz, made by running the reference): int8 bit-exact; plain fp and
+    the Ozaki FP64 mode within 4*k*u normalised; 3xBF16 within its stated 2^-14."""
+    from golden_cases import check_against_config_fixture, load_config_case
+    from ssblasex_b200 import runner
+    p, rows, ref_rows, ref_colsum = load_config_case(config_fixtures, name)
+    S.set_math_mode(mode)
+    try:
+        st, C = runner.call(p, mode="device_array")
+    finally:
+        S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+    assert st == 0
+    tol = 0.0 if p.row == "i8" else (2.0 ** -14 if mode == 2 else fp_tolerance(p))
+    check_against_config_fixture(p, C, rows, ref_rows, ref_colsum, O.exact_f64, tol)

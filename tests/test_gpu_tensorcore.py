@@ -1,8 +1,9 @@
 """The tcgen05 paths against their CPU restatements, through the C ABI, on a B200.
 
   * int8 -> int32 (kind::i8): bit-exact against the reference semantics, on the direct TMA path
-    (op(A)=T, op(B)=N, equally spaced instances) and through the pack pre-pass (every other
-    layout, unequal spacing, odd leading dimensions);
+    (every layout with 16-byte aligned leading dimensions and equally spaced instances: K-major
+    staging for op(A) = A^T and op(B) = B, MN-major staging for op(A) = A and op(B) = B^T) and
+    through the pack pre-pass (unequal spacing, leading dimensions not a multiple of 16);
   * FP64 Ozaki emulation: bit-exact against oracle.ozaki_f64 (the same algorithm on the CPU) for
     every slice count, and its error against the FP64-exact oracle;
   * FP32 three-BF16 emulation: within FP32 accumulation error of the FP64-exact value of the
@@ -50,6 +51,29 @@ def test_i8_direct_tn(S, shape):
     np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
 
 
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 1), (1, 0)])
+@pytest.mark.parametrize("m,n,k", [(128, 256, 128), (130, 201, 300), (257, 64, 129), (37, 29, 45), (1, 1, 1),
+                                   (300, 520, 1040)])
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_i8_direct_every_layout(S, ta, tb, m, n, k, cfg):
+    """Direct staging from the caller's matrices in all four layouts (MN-major tiles where op(A)
+    or op(B) is stored M- or N-contiguous), both tile widths, ragged shapes: one kernel launch,
+    bit-exact."""
+    from ssblasex_b200 import workloads as W
+    al = lambda x: -(-x // 16) * 16
+    lda = al(m if ta == 0 else k)
+    ldb = al(k if tb == 0 else n)
+    p = W.make_problem("i8", ta, tb, m, n, k, 3, -2, 3, lda=lda, ldb=ldb, ldc=m + 1, seed=m + k + 5 * ta + 7 * tb)
+    S.set_kernel_config("i8_tcgen05", cfg)
+    try:
+        C = run(p)
+        info = S.last_run_info()
+    finally:
+        S.set_kernel_config("i8_tcgen05", -1)
+    assert info["path"] == "i8_tcgen05" and info["kernel_launches"] == 1
+    np.testing.assert_array_equal(C, O.restated_gemm(p)[1])
+
+
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 1)])
 @pytest.mark.parametrize("m,n,k", [(130, 201, 300), (257, 64, 129)])
 def test_i8_pack_aligned(S, ta, tb, m, n, k):
@@ -57,7 +81,8 @@ def test_i8_pack_aligned(S, ta, tb, m, n, k):
     4 x 4 byte blocks, transposed in registers) and row counts that leave a partial group of 4
     rows: bit-exact."""
     from ssblasex_b200 import workloads as W
-    al = lambda x: -(-x // 16) * 16
+    # multiples of 4 but not of 16: not eligible for direct staging
+    al = lambda x: -(-x // 4) * 4 + (4 if -(-x // 4) * 4 % 16 == 0 else 0)
     lda = al(m if ta == 0 else k)
     ldb = al(k if tb == 0 else n)
     p = W.make_problem("i8", ta, tb, m, n, k, 3, 2, -1, lda=lda, ldb=ldb, ldc=m + 3, seed=m + 3 * ta + tb)

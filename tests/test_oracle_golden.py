@@ -66,3 +66,22 @@ def test_exact_oracle_against_longdouble():
     c0 = p.c_view(p.C, 0).astype(np.longdouble)
     want = np.longdouble(p.alpha) * (a @ b) + np.longdouble(p.beta) * c0
     assert np.max(np.abs(ex - want.astype(np.float64)) / nrm) < 2.0 ** -52
+
+
+@pytest.fixture(scope="module")
+def config_fixtures():
+    import pathlib
+    return np.load(pathlib.Path(__file__).resolve().parent / "golden" / "config_cases.npz")
+
+
+@pytest.mark.parametrize("name", ["fp32_batch64_128", "f64_batch32_1024", "i8_batch512_512", "fp32_batch4096_64"])
+def test_restatement_matches_reference_at_benchmark_shapes(config_fixtures, name):
+    """The reference's output at the benchmark configurations' full shapes (all of 64 x 128^3, a
+    slice of the others) against the C restatement on regenerated inputs: pins the restatement at
+    those sizes and that the seeded inputs are the ones the reference saw."""
+    from golden_cases import check_against_config_fixture, load_config_case
+    p, rows, ref_rows, ref_colsum = load_config_case(config_fixtures, name)
+    st, C = O.restated_gemm(p)
+    assert st == 0
+    tol = 0.0 if p.row == "i8" else fp_tolerance(p)
+    check_against_config_fixture(p, C, rows, ref_rows, ref_colsum, O.exact_f64, tol)

@@ -110,3 +110,56 @@ def test_exponent_reduction_with_zero_sentinel():
               for q in parts]
         e = max(es)
         assert (0 if e == sentinel else e) == true_exponent(r)
+
+
+@pytest.mark.parametrize("S", [3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("dist", ["expspread", "expspread30", "uniform", "outliers"])
+def test_ozaki_restatement_meets_the_stated_bound(S, dist):
+    """The a-priori bound of include/ssblasBatch.h holds entry by entry for every slice count, on
+    rows whose entries span up to 2^+-30 (where the small entries keep few of their bits) and on
+    the other input distributions; the GPU result equals this restatement bit for bit."""
+    from ssblasex_b200 import workloads as W
+    from bounds import check_ozaki
+    for ta, tb in [(0, 1), (1, 0)]:
+        p = W.make_problem("f64", ta, tb, 23, 19, 157, 2, -1.5, 0.25, seed=S * 10 + ta, dist=dist)
+        st, C = O.ozaki_f64(p, S)
+        assert st == 0
+        check_ozaki(p, C, S, range(p.batch), np.arange(p.m), O.exact_f64)
+
+
+def test_ozaki_bound_is_tight_enough_to_choose_the_slices():
+    """Rows of a single power of two against full-mantissa columns: the dropped pairs and the
+    rounding then sit near their worst case, and the measured error approaches the bound's first
+    term (the bound is not vacuous)."""
+    from ssblasex_b200 import workloads as W
+    from bounds import term_bound
+    p = W.make_problem("f64", 0, 0, 16, 16, 64, 1, 1.0, 0.0, seed=3, dist="uniform")
+    p.op_a(0)[:] = np.where(np.random.default_rng(1).random((16, 64)) < 0.5, -1.0, 1.0) * (1 - 2.0 ** -30)
+    st, C = O.ozaki_f64(p, 3)
+    ex, _ = O.exact_f64(p, 0)
+    err = np.max(np.abs(p.c_view(C, 0) - ex))
+    assert err > 1e-3 * p.k * term_bound(3)
+
+
+def test_slice_count_follows_the_tolerance():
+    """The automatic count is the smallest S in 3..8 with (S + 1) 2^(2 - 8S) <= tolerance; the
+    default tolerance 2^-51 gives 7. Refused: negative or NaN tolerances, and ones below the
+    8-slice bound."""
+    import ssblasex_b200 as S
+    from bounds import term_bound
+    try:
+        assert S.set_ozaki_slices(0) == 0
+        assert S.set_ozaki_tolerance(0) == 0 and S.get_ozaki_slices() == 7
+        for tol in [2.0 ** -20, 2.0 ** -30, 2.0 ** -40, 2.0 ** -45, 2.0 ** -51, 2.0 ** -55, 2.0 ** -58.5, 1.0]:
+            assert S.set_ozaki_tolerance(tol) == 0
+            want = next((s for s in range(3, 8) if term_bound(s) <= tol), 8)
+            assert S.get_ozaki_slices() == want, (tol, want)
+        assert S.set_ozaki_tolerance(2.0 ** -20) == 0 and S.get_ozaki_slices() == 3
+        assert S.set_ozaki_tolerance(term_bound(7)) == 0 and S.get_ozaki_slices() == 7
+        assert S.set_ozaki_tolerance(term_bound(7) * 0.999) == 0 and S.get_ozaki_slices() == 8
+        for bad in [-1.0, float("nan"), term_bound(8) / 2]:
+            assert S.set_ozaki_tolerance(bad) == S.SSBLAS_STATUS_INVALID_VALUE
+        assert S.set_ozaki_slices(5) == 0 and S.get_ozaki_slices() == 5   # a fixed count wins
+    finally:
+        S.set_ozaki_slices(0)
+        S.set_ozaki_tolerance(0)

@@ -71,3 +71,46 @@ def test_noalloc_refuses_problems_beyond_its_scratch():
                                             arr.data_ptr(), S.SSBLAS_R_32F, 4, al.ctypes.data, arr.data_ptr(),
                                             S.SSBLAS_R_32F, 4, 1, 0, 0)
     assert st == S.SSBLAS_STATUS_NOTIMPLEMENTED_ERROR
+
+
+@pytest.mark.parametrize("slices,shape", [
+    # few rows: both operands through the one-kernel slicer for long K
+    (7, (128, 128, 4096, 4)),
+    # one operand with enough rows for the two-kernel form (exponents, then digits per chunk);
+    # (320 row blocks of 32 >= two per SM); 3 slices, so 3 * (10240 + 16) * 2064 bytes still fit
+    (3, (10240, 16, 2064, 1)),
+])
+def test_noalloc_long_k_matches_the_regular_entry_point(slices, shape):
+    """For 2048 < k <= 16384 the allocation-free entry point slices with its own kernels (the
+    regular path uses the two-pass row-maximum / slab form, which needs workspace): the digits and
+    therefore the results must still agree bit for bit."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    m, n, k, batch = shape
+    p = W.make_problem("f64", 0, 1, m, n, k, batch, 1.0, 0.5, seed=k, dist="expspread")
+    S.set_ozaki_slices(slices)
+    try:
+        S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+        st, want = runner.call(p, mode="device_array")
+        assert st == 0 and S.last_run_info()["slices"] == slices
+        S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+        for _ in range(2):
+            dp = runner.DeviceProblem(p)
+            assert _noalloc(S, p, dp) == 0
+            info = S.last_run_info()
+            assert info["path"] == "ozaki_tcgen05" and info["slices"] == slices
+            np.testing.assert_array_equal(dp.C.cpu().numpy().view(np.uint64), want.view(np.uint64))
+    finally:
+        S.set_ozaki_slices(0)
+        S.set_math_mode(S.SSBLAS_MATH_PLAIN)
+
+
+def test_noalloc_refuses_k_beyond_one_exact_piece():
+    import torch
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    p = W.make_problem("f64", 0, 1, 16, 16, 16385, 1, 1.0, 0.0, seed=2)
+    dp = runner.DeviceProblem(p)
+    before = dp.C.clone()
+    assert _noalloc(S, p, dp) == S.SSBLAS_STATUS_INVALID_VALUE
+    assert torch.equal(dp.C, before)

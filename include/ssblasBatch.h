@@ -20,6 +20,8 @@
  *      m, n or batchCount <= 0 -> SSBLAS_STATUS_INTERNAL_ERROR;  k <= 0 -> success, C unchanged;
  *      beta == 0 -> C is not read; int8 arithmetic wraps modulo 2^32;
  *      alpha/beta point to float (fp32 row), double (fp64 row) or int32 (int8 row), in host memory.
+ *    ssblasSetExtensions can replace some of these rules (op C, k = 0, more type rows); all of
+ *    its flags are off by default.
  *  - If SSBLAS_GEMMBATCHEDEX_DEBUG is set in the environment, every call first prints the
  *    reference's argument dump (reference src/include/Impl/GemmBatchedEx/ssblasGemmBatchedEx.cpp:48-93).
  */
@@ -233,9 +235,11 @@ ssblasStatus_t ssblasReloadTuning(void);
  * loading the library holds until the process exits.
  *  - A[], B[], C[] must be device arrays of device pointers; other type rows return
  *    SSBLAS_STATUS_NOTIMPLEMENTED_ERROR.
- *  - A problem needs S*(m+n)*Kp*batchCount + 4*(m+n)*batchCount bytes (S = Ozaki slices, 7 by
- *    default; Kp = k rounded up to 16); larger problems, or k > 16384, return
- *    SSBLAS_STATUS_INVALID_VALUE (with a message on stderr) and leave C untouched.
+ *  - A problem needs S*(m+n)*Kp*batchCount + 4*(m+n)*batchCount bytes (S = Ozaki slices, as
+ *    ssblasGetOzakiSlices reports: 7 by default; Kp = k rounded up to 16); larger problems, or
+ *    k > 16384, return SSBLAS_STATUS_INVALID_VALUE (with a message on stderr) and leave C
+ *    untouched. On a device the tensor-core kernels do not support it returns
+ *    SSBLAS_STATUS_NOTIMPLEMENTED_ERROR without launching anything.
  *  - All calls share the array; calls whose GPU work overlaps race on it and must be ordered by
  *    the caller. Its contents carry over between calls; nothing in it needs to start at zero.
  *  - The first call on a device looks the array's address up for that device; make it before

@@ -142,7 +142,7 @@ __device__ __forceinline__ TileInfo tile_info(const Params& p, long t, long tile
 }
 
 template <int KIND_, int PA_, int PB_, int BN_, int KB_, int STAGES_, int NLEV_, int ACCB_, int EPI_, int PAIRS_,
-          int AMN_ = 0, int BMN_ = 0>
+          int AMN_ = 0, int BMN_ = 0, int OPT_ = 0>
 struct Config {
   static constexpr int KIND = KIND_;
   static constexpr int PA = PA_;       // planes of A
@@ -161,6 +161,12 @@ struct Config {
   // K rows, each K row one 128-byte swizzled line.
   static constexpr bool AMN = AMN_ != 0;
   static constexpr bool BMN = BMN_ != 0;
+  // Ozaki options (bit 0): an A slice plane whose products need two MMAs (more B planes than one
+  // MMA's N) is read from shared memory once and kept in the tensor core's A collector for the
+  // second; (bit 1) the epilogue drains the accumulator in four batches of tensor-memory loads,
+  // each issued before the previous batch is combined, so only the first load latency is exposed
+  static constexpr bool AREUSE = (OPT_ & 1) != 0;
+  static constexpr bool DRAIN_PIPE = (OPT_ & 2) != 0;
   static constexpr int ELEM = (KIND == KIND_I8) ? 1 : 2;
   static constexpr int KROWS = KB_ / ELEM;             // K elements (MN-major: K rows) per stage
   static constexpr int MN_BLOCK = KROWS * 128;         // bytes of one 128-byte-wide MN block
@@ -569,6 +575,31 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             // multiplies A_p by j planes of B at once and adds each product into its own level.
             // Every level is first written by the p = 0 MMAs of the first K step.
             constexpr int MAXQ = 256 / Cfg::BN;
+            if constexpr (Cfg::AREUSE) {
+              static_assert(Cfg::NLEV <= 2 * MAXQ, "at most two MMAs per A plane");
+              // per (A plane, 32-byte K step): its MMAs back to back, the first filling the A
+              // collector and the second (when the plane's B planes need two) reusing it
+#pragma unroll
+              for (int p = 0; p < Cfg::PA; ++p) {
+#pragma unroll
+                for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
+                  const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
+                  const uint32_t accum = (acc_k || kk > 0 || p > 0) ? 1u : 0u;
+                  if (Cfg::NLEV - p > MAXQ) {
+                    const int nq1 = (Cfg::NLEV - p - MAXQ) < MAXQ ? (Cfg::NLEV - p - MAXQ) : MAXQ;
+                    ptx::mma_i8_collect<1>(d_base + (uint32_t)(p * Cfg::BN),
+                                           ad, ptx::smem_desc_kmajor(sb + kk * 32, Cfg::KB),
+                                           ptx::idesc_i8(128, MAXQ * Cfg::BN, true, true), accum);
+                    ptx::mma_i8_collect<2>(d_base + (uint32_t)((p + MAXQ) * Cfg::BN), ad,
+                                           ptx::smem_desc_kmajor(sb + MAXQ * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB),
+                                           ptx::idesc_i8(128, nq1 * Cfg::BN, true, true), accum);
+                  } else {
+                    ptx::mma_i8(d_base + (uint32_t)(p * Cfg::BN), ad, ptx::smem_desc_kmajor(sb + kk * 32, Cfg::KB),
+                                ptx::idesc_i8(128, (Cfg::NLEV - p) * Cfg::BN, true, true), accum);
+                  }
+                }
+              }
+            } else {
 #pragma unroll
             for (int p = 0; p < Cfg::PA; ++p) {
 #pragma unroll
@@ -583,6 +614,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                   ptx::mma_i8(d, ad, bd, idesc, (acc_k || kk > 0 || p > 0) ? 1u : 0u);
                 }
               }
+            }
             }
           } else {
 #pragma unroll
@@ -725,6 +757,47 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // warp before the (slower) scaling and global stores.
         constexpr int CH = HALF / 16;
         double v[CH][16];
+        if constexpr (Cfg::DRAIN_PIPE && CH == 2 && Cfg::NLEV == 7) {
+          // batches: chunk 0 levels 6..3, chunk 1 levels 6..3, chunk 0 levels 2..0, chunk 1
+          // levels 2..0; each batch's loads go out before the previous batch is combined (the
+          // same Horner order and operations as below, so the same results bit for bit)
+          uint32_t r0[4][16], r1[4][16];
+          const uint32_t t0 = t_row, t1 = t_row + 16;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) ptx::tmem_ld16(t0 + (uint32_t)((6 - q) * Cfg::BN), r0[q]);
+          ptx::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 4; ++q) ptx::tmem_ld16(t1 + (uint32_t)((6 - q) * Cfg::BN), r1[q]);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            double x = fma(0.0, 0x1p-8, i32_to_f64(r0[0][j]));
+#pragma unroll
+            for (int q = 1; q < 4; ++q) x = fma(x, 0x1p-8, i32_to_f64(r0[q][j]));
+            v[0][j] = x;
+          }
+          ptx::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 3; ++q) ptx::tmem_ld16(t0 + (uint32_t)((2 - q) * Cfg::BN), r0[q]);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            double x = fma(0.0, 0x1p-8, i32_to_f64(r1[0][j]));
+#pragma unroll
+            for (int q = 1; q < 4; ++q) x = fma(x, 0x1p-8, i32_to_f64(r1[q][j]));
+            v[1][j] = x;
+          }
+          ptx::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 3; ++q) ptx::tmem_ld16(t1 + (uint32_t)((2 - q) * Cfg::BN), r1[q]);
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) v[0][j] = fma(v[0][j], 0x1p-8, i32_to_f64(r0[q][j]));
+          ptx::tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) v[1][j] = fma(v[1][j], 0x1p-8, i32_to_f64(r1[q][j]));
+        } else
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
 #pragma unroll

@@ -195,6 +195,13 @@ template <> struct OzCfg<8> { using T = tc::Config<tc::KIND_I8, 8, 8, 64, 32, 4,
 //   2: 128 x 32 tiles with a double-buffered accumulator (the epilogue overlaps the next tile)
 using OzCfg7KB64 = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2>;
 using OzCfg7N32 = tc::Config<tc::KIND_I8, 7, 7, 32, 32, 6, 7, 2, tc::EPI_OZAKI, 2>;
+//   3: configuration 1 with the A collector: an A plane with two MMAs per K step is read from
+//      shared memory once
+//   4: configuration 1 with the accumulator drained in four overlapped batches of loads
+//   5: both
+using OzCfg7KB64R = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 1>;
+using OzCfg7KB64D = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 2>;
+using OzCfg7KB64RD = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 3>;
 
 // Ozaki split-K: a piece holds at most 16384 k (its int32 level sums stay exact); automatic
 // pieces keep at least 512 k.
@@ -241,6 +248,9 @@ cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t
       const int c = choose_config(SSBLAS_PATH_OZAKI_TCGEN05, d.m, d.n, d.k, d.batch, 1);
       if (c == 1) return ozaki_gemm_cfg<OzCfg7KB64>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       if (c == 2) return ozaki_gemm_cfg<OzCfg7N32>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 3) return ozaki_gemm_cfg<OzCfg7KB64R>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 4) return ozaki_gemm_cfg<OzCfg7KB64D>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 5) return ozaki_gemm_cfg<OzCfg7KB64RD>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
     }
     default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);

@@ -295,7 +295,7 @@ def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
 
 
 # ------------------------------------------------------------------------- configurations ---
-@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2),
+@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2), ("ozaki_tcgen05", 3), ("ozaki_tcgen05", 4), ("ozaki_tcgen05", 5),
                                         ("i8_tcgen05", 0), ("i8_tcgen05", 1),
                                         ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1),
                                         ("dmma", 0), ("dmma", 1), ("dmma", 2), ("dmma", 3), ("dmma", 4)])

@@ -174,7 +174,10 @@ typedef enum {
   SSBLAS_PATH_I8_TCGEN05 = 2,      /* int8 -> int32 on tcgen05.mma kind::i8, TMA staging */
   SSBLAS_PATH_OZAKI_TCGEN05 = 3,   /* fp64 via int8 slices on tcgen05.mma kind::i8 */
   SSBLAS_PATH_BF16X3_TCGEN05 = 4,  /* fp32 via three BF16 split products, tcgen05 kind::f16 */
-  SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch */
+  SSBLAS_PATH_GROUPED = 5,         /* grouped persistent launch; as a ssblasSetKernelConfig key:
+                                      0 = all Ozaki instances on 128 x 64 tiles, 1 (default) = tile
+                                      shape per size bucket (key 12), 2 = all on 128 x 32 tiles
+                                      with a static tile order */
   SSBLAS_PATH_DMMA = 6,            /* plain fp64 on the FP64 tensor cores (mma.sync f64) */
   SSBLAS_PATH_OZAKI_SLICER = 7,    /* not a path: ssblasSetKernelConfig key of the Ozaki slicing
                                       pre-pass. 3: one pass with thread-block clusters of 16 rows
@@ -197,7 +200,11 @@ typedef enum {
                                       GEMM pipeline: config = chunks of the batch (1 = none, at most
                                       8), 0 = automatic (none); the slicing of chunk c + 1 runs
                                       beside the GEMM of chunk c. */,
-  SSBLAS_PATH_F16_TCGEN05 = 11      /* fp16 inputs (SSBLAS_EXT_R16F row) on tcgen05.mma kind::f16 */
+  SSBLAS_PATH_F16_TCGEN05 = 11,     /* fp16 inputs (SSBLAS_EXT_R16F row) on tcgen05.mma kind::f16 */
+  SSBLAS_PATH_GROUPED_OZAKI_TILE = 12 /* not a path: ssblasSetKernelConfig / tuning key of the tile
+                                      shape of a grouped call's Ozaki instances per size bucket
+                                      (batch 1): 0 = 128 x 64 tiles, one accumulator; 1 = 128 x 32
+                                      tiles, two accumulators */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

@@ -204,7 +204,8 @@ def get_profile() -> dict:
 
 
 PATH_IDS = {"simt": 1, "i8_tcgen05": 2, "ozaki_tcgen05": 3, "bf16x3_tcgen05": 4, "grouped": 5, "dmma": 6,
-            "ozaki_slicer": 7, "splitk_i8": 8, "splitk_ozaki": 9, "ozaki_pipeline": 10}
+            "ozaki_slicer": 7, "splitk_i8": 8, "splitk_ozaki": 9, "ozaki_pipeline": 10, "f16_tcgen05": 11,
+            "grouped_ozaki_tile": 12}
 
 
 def set_kernel_config(path: str, config: int) -> int:

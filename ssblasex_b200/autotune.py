@@ -24,7 +24,7 @@ OUT = pathlib.Path(__file__).resolve().parent / "tune" / "ssblas_tune.json"
 
 # path -> (math mode, configurations, kernel name, problems)
 FAMILIES = {
-    "ozaki_tcgen05": (SSBLAS_MATH_FP64_OZAKI, [0, 1, 2], "ozaki_gemm", [
+    "ozaki_tcgen05": (SSBLAS_MATH_FP64_OZAKI, [0, 1, 2, 3, 4, 5, 6, 7, 8, 9], "ozaki_gemm", [
         dict(row="f64", transa=0, transb=1, m=1024, n=1024, k=1024, batch=32, alpha=1.0, beta=0.0,
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=0, transb=0, m=512, n=512, k=512, batch=64, alpha=1.0, beta=0.0,
@@ -71,7 +71,7 @@ FAMILIES = {
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),
     ]),
-    "bf16x3_tcgen05": (SSBLAS_MATH_FP32_BF16X3, [0, 1], "bf16x3_gemm", [
+    "bf16x3_tcgen05": (SSBLAS_MATH_FP32_BF16X3, [0, 1, 2], "(all)", [
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),
         dict(row="f32", transa=0, transb=0, m=256, n=256, k=256, batch=256, alpha=1.0, beta=0.0),
@@ -109,6 +109,56 @@ def time_kernel(p, dp, kernel, reps):
     return sum(ms for _, ms in prof.values()) / reps
 
 
+# grouped calls: the Ozaki tile shape per instance size bucket (0: 128 x 64 tiles, one
+# accumulator; 1: 128 x 32 tiles, two), timed on groups of equal-size instances (m, n, k)
+GROUPED_OZAKI_BUCKETS = [(64, 64, 64), (128, 128, 128), (256, 256, 256), (512, 512, 512), (64, 64, 512),
+                         (256, 256, 64), (512, 64, 512), (128, 128, 512), (256, 256, 512)]
+
+
+def time_grouped(gd, reps):
+    import torch
+    set_sync_mode(False)
+    for _ in range(3):                     # plan, capture, first replay
+        assert gd.call(device_arrays=True) == 0
+    torch.cuda.synchronize()
+    set_profiling(True)
+    for _ in range(reps):
+        assert gd.call(device_arrays=True) == 0
+    prof = get_profile()
+    set_profiling(False)
+    set_sync_mode(True)
+    return sum(ms for _, ms in prof.values()) / reps
+
+
+def tune_grouped_ozaki(entries, report, quick):
+    from . import release_workspace
+    set_math_mode(SSBLAS_MATH_FP64_OZAKI)
+    for m, n, k in GROUPED_OZAKI_BUCKETS[: 2 if quick else None]:
+        count = max(8, min(600, (1 << 27) // (m * n * k)))
+        probs = [W.make_problem("f64", i % 2, (i // 2) % 2, m, n, k, 1, 1.0, 0.0, seed=300 + i, dist="expspread",
+                                name=f"t{i}") for i in range(count)]
+        gd = runner.GroupedDevice(probs)
+        times, ref = {}, None
+        for cfg in (0, 1):
+            set_kernel_config("grouped_ozaki_tile", cfg)
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            res = np.concatenate([c.ravel() for c in gd.results()])
+            if ref is None:
+                ref = res
+            elif not np.array_equal(res.view(np.uint64), ref.view(np.uint64)):
+                continue
+            times[cfg] = time_grouped(gd, 5)
+        set_kernel_config("grouped_ozaki_tile", -1)
+        release_workspace()               # drop the cached grouped plan
+        best = min(times, key=times.get)
+        b = bucket(m, n, k, 1)
+        entries.append({"path": PATH_IDS["grouped_ozaki_tile"], "bucket": b, "config": best})
+        report.append({"family": "grouped_ozaki_tile", "bucket": b, "instances": count, "ms": times, "best": best})
+        print(json.dumps(report[-1]), flush=True)
+    set_math_mode(SSBLAS_MATH_PLAIN)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(OUT))
@@ -141,6 +191,7 @@ def main():
             entries.append({"path": PATH_IDS[family], "bucket": b, "config": best})
             report.append({"family": family, "bucket": b, "ms": times, "best": best})
             print(json.dumps(report[-1]), flush=True)
+    tune_grouped_ozaki(entries, report, args.quick)
     set_math_mode(SSBLAS_MATH_PLAIN)
     out = pathlib.Path(args.out)
     out.parent.mkdir(parents=True, exist_ok=True)

@@ -411,7 +411,7 @@ cudaError_t launch_kind(const KindDev& kd, void* const* C, cudaStream_t st, cons
   memset(&dummy, 0, sizeof(dummy));
   const long grid = kd.ntiles < num_sms() ? kd.ntiles : num_sms();
   ProfScope prof(gemm_name, st);
-  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, tc::kThreadsGrouped, Cfg::SMEM, st>>>(dummy, dummy, prm);
+  tc::tc_gemm_kernel<Cfg, true><<<(unsigned)grid, tc::kThreadsGrouped, Cfg::SMEM, st>>>(dummy, dummy, dummy, prm);
   note_launch();
   return cudaGetLastError();
 }
@@ -428,9 +428,10 @@ using GCfgI8 = tc::Config<tc::KIND_I8, 1, 1, 128, 128, 6, 1, 2, tc::EPI_I32, 0>;
 // and (after the first replay request) the captured CUDA graph of all its launches.
 struct Plan {
   std::vector<uint64_t> key;
-  int oz_cfg = 0;            // Ozaki tile configuration (0: 128 x 64, 1: 128 x 32)
   bool dynamic = true;       // tiles from the device-side queue (else the static stride)
-  KindDev oz, bf, i8;
+  // Ozaki instances by tile shape: oz on 128 x 32 tiles with two accumulators, oz_wide on
+  // 128 x 64 tiles with one (chosen per instance size bucket)
+  KindDev oz, oz_wide, bf, i8;
   std::unique_ptr<GroupedSimt> simt;
   void* const* C = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -441,6 +442,20 @@ struct Plan {
 };
 
 std::map<int, std::unique_ptr<Plan>> g_plans;   // one cached plan per device
+
+// Tile shape of one Ozaki instance: 128 x 64 tiles with one accumulator read the slice planes from
+// shared memory a third more efficiently per product than 128 x 32 tiles with two, whose gain is
+// an epilogue that overlaps the next tile's MMAs; so the wide tiles pay where K is long enough to
+// amortise the exposed epilogue and the narrow side fills them. Per size bucket (batch 1) the
+// tuning table may choose (SSBLAS_PATH_GROUPED_OZAKI_TILE: 0 = 128 x 64, 1 = 128 x 32); the
+// grouped configuration 0 or 2 forces one shape for all.
+bool ozaki_wide_tiles(const GroupedInst& in, int gcfg) {
+  if (gcfg == 0) return true;
+  if (gcfg == 2) return false;
+  const long narrow = in.m < in.n ? in.m : in.n;   // the tiles' narrow side after orientation
+  const int fallback = (in.k >= 384 && narrow >= 48) ? 0 : 1;
+  return choose_config(SSBLAS_PATH_GROUPED_OZAKI_TILE, in.m, in.n, in.k, 1, fallback) == 0;
+}
 
 std::vector<uint64_t> signature(const GroupedDesc& g, int mode, int oz_cfg) {
   std::vector<uint64_t> k;
@@ -467,11 +482,10 @@ std::vector<uint64_t> signature(const GroupedDesc& g, int mode, int oz_cfg) {
 
 cudaError_t run_plan(Plan& pl, cudaStream_t st) {
   cudaError_t e;
-  if (pl.oz_cfg == 1) {
-    if ((e = launch_kind<GCfgOz32, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic))) return e;
-  } else {
-    if ((e = launch_kind<GCfgOz, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic))) return e;
-  }
+  if ((e = launch_kind<GCfgOz, 2, 7>(pl.oz_wide, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic)))
+    return e;
+  if ((e = launch_kind<GCfgOz32, 2, 7>(pl.oz, pl.C, st, "grouped_ozaki_slice", "grouped_ozaki_gemm", pl.dynamic)))
+    return e;
   if ((e = launch_kind<GCfgBf, 1, 1>(pl.bf, pl.C, st, "grouped_split_bf16", "grouped_bf16x3_gemm", pl.dynamic))) return e;
   if ((e = launch_kind<GCfgI8, 0, 1>(pl.i8, pl.C, st, "grouped_pack_i8", "grouped_i8_gemm", pl.dynamic))) return e;
   if (pl.simt && (e = launch_simt_grouped(*pl.simt, st))) return e;
@@ -485,10 +499,10 @@ cudaError_t grouped_run(const GroupedDesc& g, cudaStream_t st) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  // configurations: 0 = 128 x 64 Ozaki tiles, dynamic tile queue; 1 (default) = 128 x 32 Ozaki
-  // tiles with two accumulators, dynamic tile queue; 2 = 128 x 32 tiles, static tile order
+  // configurations: 0 = every Ozaki instance on 128 x 64 tiles, dynamic tile queue; 1 (default) =
+  // the tile shape of each Ozaki instance from its size bucket (SSBLAS_PATH_GROUPED_OZAKI_TILE),
+  // dynamic tile queue; 2 = every Ozaki instance on 128 x 32 tiles, static tile order
   const int gcfg = choose_config(SSBLAS_PATH_GROUPED, 0, 0, 0, 0, 1);
-  const int oz_cfg = gcfg == 0 ? 0 : 1;
   const bool dynamic_order = gcfg != 2;
   std::vector<uint64_t> key = signature(g, mode, gcfg);
   auto it = g_plans.find(dev);
@@ -524,28 +538,25 @@ cudaError_t grouped_run(const GroupedDesc& g, cudaStream_t st) {
   // new signature: build the plan
   auto pl = std::make_unique<Plan>();
   pl->key = std::move(key);
-  pl->oz_cfg = oz_cfg;
   pl->dynamic = dynamic_order;
   pl->C = g.C;
-  std::vector<int> oz, bf, i8, plain;
+  std::vector<int> oz, oz_wide, bf, i8, plain;
   for (int i = 0; i < (int)g.inst.size(); ++i) {
     const GroupedInst& in = g.inst[i];
     if (in.k <= 0) continue;   // C untouched, as in the reference
     if (in.row == ROW_I8) i8.push_back(i);
-    else if (in.row == ROW_F64 && (mode & SSBLAS_MATH_FP64_OZAKI) && in.k <= 16384) oz.push_back(i);
+    else if (in.row == ROW_F64 && (mode & SSBLAS_MATH_FP64_OZAKI) && in.k <= 16384)
+      (ozaki_wide_tiles(in, gcfg) ? oz_wide : oz).push_back(i);
     else if (in.row == ROW_F32 && (mode & SSBLAS_MATH_FP32_BF16X3)) bf.push_back(i);
     else plain.push_back(i);
   }
   {
-    if (pl->oz_cfg == 1) {
-      KindPlan<GCfgOz32> k1;
-      plan_kind(g, oz, k1);
-      if ((e = upload_kind(k1, pl->oz, st))) return e;
-    } else {
-      KindPlan<GCfgOz> k1;
-      plan_kind(g, oz, k1);
-      if ((e = upload_kind(k1, pl->oz, st))) return e;
-    }
+    KindPlan<GCfgOz32> k1;
+    plan_kind(g, oz, k1);
+    if ((e = upload_kind(k1, pl->oz, st))) return e;
+    KindPlan<GCfgOz> k0;
+    plan_kind(g, oz_wide, k0);
+    if ((e = upload_kind(k0, pl->oz_wide, st))) return e;
     KindPlan<GCfgBf> k2;
     plan_kind(g, bf, k2);
     if ((e = upload_kind(k2, pl->bf, st))) return e;
@@ -557,11 +568,11 @@ cudaError_t grouped_run(const GroupedDesc& g, cudaStream_t st) {
     pl->simt = std::make_unique<GroupedSimt>();
     if ((e = plan_simt_grouped(g, plain, *pl->simt, st))) return e;
   }
-  pl->launches = (pl->oz.ninst ? 2 : 0) + (pl->bf.ninst ? 2 : 0) + (pl->i8.ninst ? 2 : 0) +
-                 (pl->simt ? pl->simt->launches : 0);
+  pl->launches = (pl->oz.ninst ? 2 : 0) + (pl->oz_wide.ninst ? 2 : 0) + (pl->bf.ninst ? 2 : 0) +
+                 (pl->i8.ninst ? 2 : 0) + (pl->simt ? pl->simt->launches : 0);
   g_plans[dev] = std::move(pl);
   Plan& p = *g_plans[dev];
-  note_path(SSBLAS_PATH_GROUPED, p.oz.ninst ? 7 : 0);
+  note_path(SSBLAS_PATH_GROUPED, (p.oz.ninst || p.oz_wide.ninst) ? 7 : 0);
   return run_plan(p, st);
 }
 

@@ -110,6 +110,9 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int slices, const int8_t* p
                                  const int32_t* exps, long Kp, cudaStream_t stream);
 // fp32 via three BF16 products
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t stream);
+// fp32 via three BF16 products in one kernel for instances of at most 128 x 128 (bf16x3_small.cu)
+bool bf16x3_small_fits(const BatchDesc& d);
+cudaError_t launch_bf16x3_small(const BatchDesc& d, cudaStream_t stream);
 // fp16 inputs (type extension row) on tcgen05 kind::f16, fp32 accumulation
 cudaError_t launch_f16_tcgen05(const BatchDesc& d, cudaStream_t stream);
 

@@ -39,6 +39,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking probe of a barrier phase (no suspension of the thread).
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, P;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Every wait in the library's kernels is bounded. When a wait gives up, the kernel records
 // `code` in the device error flag and the caller abandons its loop; the host turns a set flag
 // into SSBLAS_STATUS_INTERNAL_ERROR. `limit` is the number of try_wait rounds (kWaitLimit unless
@@ -48,6 +61,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* er
                                           uint32_t limit = kWaitLimit) {
   for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicExch(err, code);
+  return false;
+}
+
+// Bounded wait by polling (test_wait): for waits on short tensor-core work that many threads share,
+// where a suspended try_wait may resume later than the phase completes. The limit counts polls.
+constexpr uint32_t kPollLimit = 1u << 26;
+__device__ __forceinline__ bool mbar_poll(uint32_t bar, uint32_t parity, int* err, int code) {
+  for (uint32_t i = 0; i < kPollLimit; ++i)
+    if (mbar_test_wait(bar, parity)) return true;
   if (err) atomicExch(err, code);
   return false;
 }
@@ -65,6 +88,29 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Bulk tensor store shared -> global (3-D map), in this thread's bulk async group; writes outside
+// the tensor are dropped. commit closes the group; wait_read waits until the stores' shared-memory
+// reads are done (the buffer may be written again), wait_all until they are complete.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(src), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// L2 prefetch of one tile of a 4-D tensor map (no shared memory written, nothing to wait for).
+__device__ __forceinline__ void tma_prefetch_l2_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3)
                : "memory");
 }
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {

@@ -103,6 +103,9 @@ struct Params {
   long skip_copy;
   // int8 kinds: bit 0 = op(A) unsigned, bit 1 = op(B) unsigned (0: both signed)
   int ab_unsigned;
+  // the C tensor map (kernel argument tmC, {m, n, batch} of the instances' C) is valid: C_TMA
+  // configurations store the Ozaki results with bulk tensor stores when beta == 0
+  int c_tma;
 };
 
 // Grouped launches take tiles from a device-side queue: a scheduler warp (warp 10) of each CTA
@@ -167,6 +170,19 @@ struct Config {
   // each issued before the previous batch is combined, so only the first load latency is exposed
   static constexpr bool AREUSE = (OPT_ & 1) != 0;
   static constexpr bool DRAIN_PIPE = (OPT_ & 2) != 0;
+  // (bit 2) the producer prefetches into L2 the tiles of the K block 2 * STAGES ahead of the one it
+  // loads; (bit 3) each stage arrives in two parts with their own barriers -- A planes 0-3 with all
+  // B planes, then A planes 4-7 (the A stage holds 8 plane slots, the 8th zero-filled) -- so the
+  // MMAs of A planes 0-3 (79% of a stage's products for 7 slices) start before the rest lands
+  static constexpr bool L2_PREFETCH = (OPT_ & 4) != 0;
+  static constexpr bool SPLIT_STAGE = (OPT_ & 8) != 0;
+  // (bit 4) Ozaki epilogue with beta == 0 and a C tensor map: each epilogue warp writes its
+  // 32 x 16 outputs to a 4 KB shared-memory buffer and one lane hands them to a bulk tensor store,
+  // so the warp is free for the next tile's accumulator instead of waiting on its global stores
+  static constexpr bool C_TMA = (OPT_ & 16) != 0;
+  static constexpr int C_STAGING = C_TMA ? 8 * 32 * 16 * 8 : 0;
+  static constexpr int A_SLOTS = SPLIT_STAGE ? 8 : PA_;
+  static_assert(!SPLIT_STAGE || (PAIRS_ == 2 && PA_ > 4 && PA_ <= 8 && !AREUSE), "split stages: Ozaki, 5-8 slices");
   static constexpr int ELEM = (KIND == KIND_I8) ? 1 : 2;
   static constexpr int KROWS = KB_ / ELEM;             // K elements (MN-major: K rows) per stage
   static constexpr int MN_BLOCK = KROWS * 128;         // bytes of one 128-byte-wide MN block
@@ -174,13 +190,13 @@ struct Config {
                 "MN-major staging is for single-plane operands with 128-byte K stages");
   // split-K adds the pieces' sums afterwards: only exact integer sums give the unsplit result
   static constexpr bool SPLITTABLE = EPI_ == EPI_I32 || EPI_ == EPI_OZAKI;
-  static constexpr int A_STAGE = PA * BM * KB;
+  static constexpr int A_STAGE = A_SLOTS * BM * KB;
   static constexpr int B_STAGE = PB * BN * KB;
   static constexpr int STAGE = A_STAGE + B_STAGE;
   static constexpr int TMEM_COLS_USED = ACCB * NLEV * BN;
   static constexpr int TMEM_COLS = TMEM_COLS_USED <= 32 ? 32 : TMEM_COLS_USED <= 64 ? 64 : TMEM_COLS_USED <= 128 ? 128
                                    : TMEM_COLS_USED <= 256 ? 256 : 512;
-  static constexpr int SMEM = 1024 + STAGES * STAGE + 256 + kTileQueueBytes;
+  static constexpr int SMEM = 1024 + STAGES * STAGE + 256 + kTileQueueBytes + C_STAGING;
   static_assert(TMEM_COLS_USED <= 512, "tensor memory overflow");
   static_assert(A_STAGE % 1024 == 0 && B_STAGE % 1024 == 0, "stage alignment");
   static_assert(SMEM <= 232448, "shared memory overflow");
@@ -416,7 +432,8 @@ __device__ __noinline__ void split_k_region(uint32_t t_row, int32_t* split_ws, i
 // unsplit kernels carry no trace of the split epilogue.
 template <class Cfg, bool GROUPED, bool SPLIT = false>
 __global__ void __launch_bounds__(threads_of<GROUPED>(), 1)
-tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Params prm) {
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+               const __grid_constant__ CUtensorMap tmC, const Params prm) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* stages = smem;
@@ -427,6 +444,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   uint64_t* tempty = tfull + 2;
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+  uint64_t* full_hi = drain + 2;   // split stages: second part of each stage
   uint64_t* tq_full = (uint64_t*)(smem + Cfg::STAGES * Cfg::STAGE + 256);
   uint64_t* tq_empty = tq_full + kTQ;
   TileDesc* tq = (TileDesc*)(tq_empty + kTQ);
@@ -441,6 +459,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     for (int s = 0; s < Cfg::STAGES; ++s) {
       ptx::mbar_init(ptx::smem_u32(&full[s]), 1);
       ptx::mbar_init(ptx::smem_u32(&empty[s]), 1);
+      if (Cfg::SPLIT_STAGE) ptx::mbar_init(ptx::smem_u32(&full_hi[s]), 1);
     }
     for (int a = 0; a < 2; ++a) {
       ptx::mbar_init(ptx::smem_u32(&tfull[a]), 1);
@@ -501,8 +520,18 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           if (!ptx::mbar_wait(ptx::smem_u32(&empty[s]), ph ^ 1, err, 11, wl)) { ok = false; break; }
           if (!GROUPED && it == prm.skip_copy && blockIdx.x == 0) continue;   // injected fault
           const uint32_t fb = ptx::smem_u32(&full[s]);
-          ptx::mbar_arrive_expect_tx(fb, Cfg::STAGE);
           uint8_t* sa = stages + (size_t)s * Cfg::STAGE;
+          if constexpr (Cfg::SPLIT_STAGE && !GROUPED) {
+            // A planes 0-3 and all B planes, then A planes 4-7 (the A map's box holds 4 planes)
+            constexpr int HALF_A = 4 * Cfg::BM * Cfg::KB;
+            ptx::mbar_arrive_expect_tx(fb, HALF_A + Cfg::B_STAGE);
+            ptx::tma_load_4d(ptx::smem_u32(sa), &tmA, fb, kb * KE, ti.mt * Cfg::BM, 0, ti.b);
+            ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, ti.nt * Cfg::BN, 0, ti.b);
+            const uint32_t fh = ptx::smem_u32(&full_hi[s]);
+            ptx::mbar_arrive_expect_tx(fh, HALF_A);
+            ptx::tma_load_4d(ptx::smem_u32(sa + HALF_A), &tmA, fh, kb * KE, ti.mt * Cfg::BM, 4, ti.b);
+          } else {
+          ptx::mbar_arrive_expect_tx(fb, Cfg::STAGE);
           if constexpr (GROUPED) {
             ptx::bulk_load(ptx::smem_u32(sa), srcA + (size_t)kb * Cfg::A_STAGE, Cfg::A_STAGE, fb);
             ptx::bulk_load(ptx::smem_u32(sa + Cfg::A_STAGE), srcB + (size_t)kb * Cfg::B_STAGE, Cfg::B_STAGE, fb);
@@ -525,11 +554,24 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               ptx::tma_load_4d(ptx::smem_u32(sa + Cfg::A_STAGE), &tmB, fb, kb * KE, ti.nt * Cfg::BN, 0, ti.b);
             }
           }
+          }
+          if constexpr (Cfg::L2_PREFETCH && !GROUPED) {
+            // the tiles of K block kb + 2 STAGES of this output tile into L2, ahead of their loads
+            const int kp = kb + 2 * Cfg::STAGES;
+            if (kp < ti.kb1) {
+              ptx::tma_prefetch_l2_4d(&tmA, kp * KE, ti.mt * Cfg::BM, 0, ti.b);
+              ptx::tma_prefetch_l2_4d(&tmB, kp * KE, ti.nt * Cfg::BN, 0, ti.b);
+              if constexpr (Cfg::SPLIT_STAGE) ptx::tma_prefetch_l2_4d(&tmA, kp * KE, ti.mt * Cfg::BM, 4, ti.b);
+            }
+          }
         }
       }
       // no copy may still be in flight when the CTA exits
-      for (long j = (it > Cfg::STAGES ? it - Cfg::STAGES : 0); j < it; ++j)
+      for (long j = (it > Cfg::STAGES ? it - Cfg::STAGES : 0); j < it; ++j) {
         ptx::mbar_wait(ptx::smem_u32(&full[j % Cfg::STAGES]), (uint32_t)((j / Cfg::STAGES) & 1), err, 12, wl);
+        if (Cfg::SPLIT_STAGE)
+          ptx::mbar_wait(ptx::smem_u32(&full_hi[j % Cfg::STAGES]), (uint32_t)((j / Cfg::STAGES) & 1), err, 12, wl);
+      }
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------------ MMA issuer --------
@@ -602,6 +644,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             } else {
 #pragma unroll
             for (int p = 0; p < Cfg::PA; ++p) {
+              if (Cfg::SPLIT_STAGE && p == 4) {
+                // the stage's second part: A planes 4-7
+                if (!ptx::mbar_wait(ptx::smem_u32(&full_hi[s]), ph, err, 25, wl)) { ok = false; break; }
+                ptx::tc_fence_after();
+              }
 #pragma unroll
               for (int q0 = 0; q0 < Cfg::NLEV - p; q0 += MAXQ) {
                 const int nq = (Cfg::NLEV - p - q0) < MAXQ ? (Cfg::NLEV - p - q0) : MAXQ;
@@ -637,6 +684,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             }
           }
           }
+          if (!ok) break;   // a split stage's second part never arrived
           ptx::mma_commit(ptx::smem_u32(&empty[s]));   // frees the stage when these MMAs finish
         }
         if (!ok) break;
@@ -823,7 +871,48 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         if constexpr (PRE) {
           if (row_ok) ozaki_store<1, true>((double*)Cb, gi, n0, n, rs, ldc, pre_ea, exb, prm.exp_shift, alpha_d, beta_d, v, pre_eb);
         } else {
-          if (row_ok) ozaki_store<CH>((double*)Cb, gi, n0, n, rs, ldc, exa[gi], exb, prm.exp_shift, alpha_d, beta_d, v);
+          bool stored = false;
+          if constexpr (Cfg::C_TMA && !GROUPED && CH == 2) {
+            if (prm.c_tma && beta_d == 0.0) {
+              // every output's scale factor must be a normal double (the branch-free formula) for the
+              // bulk store; otherwise the whole region takes ozaki_store's rare-value handling
+              const int32_t ea = row_ok ? exa[gi] : 0;
+              double w[CH][16];
+              bool rare = false;
+#pragma unroll
+              for (int c = 0; c < CH; ++c)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  const long gj = n0 + c * 16 + j;
+                  const int E = ea + (gj < n ? exb[gj] : 0) + prm.exp_shift;
+                  rare |= row_ok && gj < n && (unsigned)(E + 1022) > 2045u;
+                  w[c][j] = fma(v[c][j] * __longlong_as_double((long long)(E + 1023) << 52), alpha_d, 0.0);
+                }
+              if (!__any_sync(0xffffffffu, rare)) {
+                // 32 rows x 16 columns per bulk store: buffer [column][row], rows and columns outside
+                // C are dropped by the store
+                double* stg = (double*)(stages + Cfg::STAGES * Cfg::STAGE + 256 + kTileQueueBytes) + (warp - 2) * 512;
+                const int row0 = ti.mt * Cfg::BM + quarter * 32;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                  if (n0 + c * 16 >= n) break;
+                  if (lane == 0) ptx::bulk_wait_read();   // the previous store has read the buffer
+                  __syncwarp();
+#pragma unroll
+                  for (int j = 0; j < 16; ++j) stg[j * 32 + lane] = w[c][j];
+                  ptx::fence_proxy_async_smem();
+                  __syncwarp();
+                  if (lane == 0) {
+                    ptx::tma_store_3d(&tmC, ptx::smem_u32(stg), row0, (int)(n0 + c * 16), ti.b + prm.c_batch_offset);
+                    ptx::bulk_commit();
+                  }
+                }
+                stored = true;
+              }
+            }
+          }
+          if (!stored && row_ok)
+            ozaki_store<CH>((double*)Cb, gi, n0, n, rs, ldc, exa[gi], exb, prm.exp_shift, alpha_d, beta_d, v);
         }
         continue;
       }
@@ -894,6 +983,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
   }
 
+  if constexpr (Cfg::C_TMA) {
+    // the epilogue's bulk stores complete before the CTA (and its shared memory) goes away
+    if (warp >= 2 && lane == 0) ptx::bulk_wait_all();
+  }
   ptx::tc_fence_before();
   __syncthreads();
   if (warp == 1) {

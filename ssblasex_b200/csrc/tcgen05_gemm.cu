@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <cstring>
 
 #include "internal.h"
 #include "prepass.h"
@@ -96,7 +97,10 @@ int choose_splits(const SplitPlan& sp, long m, long n, long k, long batch, long 
 
 template <class Cfg>
 cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params prm, cudaStream_t st,
-                     const char* name, const SplitPlan& plan = SplitPlan()) {
+                     const char* name, const SplitPlan& plan = SplitPlan(), const CUtensorMap* tcmap = nullptr) {
+  CUtensorMap tmc;
+  if (tcmap) tmc = *tcmap;
+  else memset(&tmc, 0, sizeof(tmc));
   static bool attr_set[kMaxDevices] = {};
   static bool attr_set_split[kMaxDevices] = {};
   if (cudaError_t e = smem_attr_once(attr_set, tc::tc_gemm_kernel<Cfg, false, false>, Cfg::SMEM)) return e;
@@ -141,9 +145,9 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   ProfScope prof(name, st);
   if (prm.splits > 1) {
     if constexpr (Cfg::SPLITTABLE)
-      tc::tc_gemm_kernel<Cfg, false, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
+      tc::tc_gemm_kernel<Cfg, false, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, tmc, prm);
   } else {
-    tc::tc_gemm_kernel<Cfg, false, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, prm);
+    tc::tc_gemm_kernel<Cfg, false, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, tmc, prm);
   }
   note_launch();
   return cudaGetLastError();
@@ -202,6 +206,14 @@ using OzCfg7N32 = tc::Config<tc::KIND_I8, 7, 7, 32, 32, 6, 7, 2, tc::EPI_OZAKI, 
 using OzCfg7KB64R = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 1>;
 using OzCfg7KB64D = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 2>;
 using OzCfg7KB64RD = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 3>;
+//   6: configuration 1 with an L2 prefetch of the K block two stages ahead of each load
+//   7: configuration 1 with each stage in two parts (A planes 0-3 and B, then A planes 4-6)
+//   8: both
+using OzCfg7KB64P = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 4>;
+using OzCfg7KB64S = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 8>;
+using OzCfg7KB64SP = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 12>;
+//   9: configuration 1 with the results written by bulk tensor stores (beta == 0)
+using OzCfg7KB64T = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 16>;
 
 // Ozaki split-K: a piece holds at most 16384 k (its int32 level sums stay exact); automatic
 // pieces keep at least 512 k.
@@ -222,8 +234,10 @@ cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const in
                            const int32_t* exb, long Kp, bool allow_split, cudaStream_t st) {
   const long sa = d.m * Kp, sb = d.n * Kp;
   CUtensorMap ta, tb;
-  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, Cfg::KB, 128, S,
-                Cfg::KB) ||
+  // split stages load A in two boxes of 4 planes (the second reads planes 4-7; planes past S are
+  // outside the tensor and arrive as zeros)
+  if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.m, S, d.batch, Kp, sa, sa * S, Cfg::KB, 128,
+                Cfg::SPLIT_STAGE ? 4 : S, Cfg::KB) ||
       !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_UINT8, d.k, d.n, S, d.batch, Kp, sb, sb * S, Cfg::KB, Cfg::BN, S,
                 Cfg::KB))
     return cudaErrorNotSupported;
@@ -232,7 +246,23 @@ cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const in
   prm.exp_b = exb;
   prm.exp_shift = -12;
   note_path(SSBLAS_PATH_OZAKI_TCGEN05, S);
-  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split));
+  // bulk tensor stores of C: beta == 0 and C instances addressable by one 3-D map
+  CUtensorMap tcm;
+  const CUtensorMap* tcp = nullptr;
+  if constexpr (Cfg::C_TMA) {
+    const bool uniform = d.batch == 1 || d.strideC > 0;
+    if (d.beta_d == 0.0 && d.C0 && uniform && ((uintptr_t)d.C0 % 16) == 0 && (d.ldc * 8) % 16 == 0 &&
+        d.strideC % 16 == 0 && d.m < (1L << 31) && d.n < (1L << 31)) {
+      const long dims[3] = {d.m, d.n, d.batch};
+      const long strides[2] = {d.ldc * 8, d.batch > 1 ? d.strideC : round_up(d.ldc * d.n * 8, 16)};
+      const int box[3] = {32, 16, 1};
+      if (make_tiled_map(&tcm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, d.C0, dims, strides, box, 0)) {
+        prm.c_tma = 1;
+        tcp = &tcm;
+      }
+    }
+  }
+  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split), tcp);
 }
 
 // exa: exponents of the rows of op(A), [batch][m]; exb: of the columns of op(B), [batch][n]
@@ -251,6 +281,10 @@ cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t
       if (c == 3) return ozaki_gemm_cfg<OzCfg7KB64R>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       if (c == 4) return ozaki_gemm_cfg<OzCfg7KB64D>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       if (c == 5) return ozaki_gemm_cfg<OzCfg7KB64RD>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 6) return ozaki_gemm_cfg<OzCfg7KB64P>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 7) return ozaki_gemm_cfg<OzCfg7KB64S>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 8) return ozaki_gemm_cfg<OzCfg7KB64SP>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 9) return ozaki_gemm_cfg<OzCfg7KB64T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
     }
     default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
@@ -475,6 +509,7 @@ cudaError_t ozaki_pipelined(const BatchDesc& d, int S, const PlaneArgs& a, const
     BatchDesc dc = d;
     dc.batch = nb;
     dc.C = d.C + b0;
+    dc.C0 = nullptr;   // a chunk's C is not addressed through the batch's C tensor map
     if ((e = ozaki_gemm(dc, S, pa + b0 * a.batch_stride, pb + b0 * b.batch_stride, exa + b0 * d.m,
                         exb + b0 * d.n, Kp, false, st)) != cudaSuccess)
       return e;
@@ -523,6 +558,13 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, co
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (d.m > (1L << 31) || d.n > (1L << 31) || d.k > (1L << 31)) return cudaErrorNotSupported;
+  // configurations: 0 / 1 = split pass then tiled GEMM with 64- / 128-column tiles (the defaults);
+  // 2 = one kernel that splits in shared memory, for instances of at most 128 x 128 -- measured
+  // slower on 4096 x 64^3 (0.38 ms against 0.156 ms: one instance in flight per CTA leaves it
+  // bound by memory latency), so only a configuration
+  const int fallback = d.n <= 64 ? 0 : 1;
+  const int cfg = choose_config(SSBLAS_PATH_BF16X3_TCGEN05, d.m, d.n, d.k, d.batch, fallback);
+  if (cfg == 2 && bf16x3_small_fits(d)) return launch_bf16x3_small(d, st);
   cudaError_t e;
   const long Kp = round_up(d.k, 8);
   const long sa = d.m * Kp * 2, sb = d.n * Kp * 2;   // bytes per plane
@@ -533,7 +575,7 @@ cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   PlaneArgs a{d.A, d.m, d.k, d.lda, d.transa == SSBLAS_OP_T, d.batch, pa, Kp, sa, sa * 2};
   PlaneArgs b{d.B, d.n, d.k, d.ldb, d.transb == SSBLAS_OP_N, d.batch, pb, Kp, sb, sb * 2};
   if ((e = launch_split_bf16_pair(a, b, st)) != cudaSuccess) return e;
-  const int BN = choose_config(SSBLAS_PATH_BF16X3_TCGEN05, d.m, d.n, d.k, d.batch, d.n <= 64 ? 0 : 1) == 0 ? 64 : 128;
+  const int BN = (cfg == 0 || (cfg == 2 && d.n <= 64)) ? 64 : 128;
   CUtensorMap ta, tb;
   if (!make_map(&ta, pa, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.m, 2, d.batch, Kp * 2, sa, sa * 2, 64, 128, 2, 128) ||
       !make_map(&tb, pb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, d.k, d.n, 2, d.batch, Kp * 2, sb, sb * 2, 64, BN, 2, 128))

@@ -209,3 +209,31 @@ def test_grouped_transposed_orientation(mode):
                 np.testing.assert_array_equal(C.reshape(p.n, p.ldc)[:, p.m:], p.C.reshape(p.n, p.ldc)[:, p.m:])
     finally:
         S.set_math_mode(0)
+
+
+@pytest.mark.parametrize("gcfg", [0, 1, 2])
+def test_grouped_ozaki_tile_shapes(gcfg):
+    """Ozaki instances on 128 x 64 tiles (0), on the shape their size bucket selects -- here long-K
+    instances on 128 x 64 and short ones on 128 x 32 tiles, in one call (1), and all on 128 x 32
+    tiles in the static order (2): bit-exact against the restatement in every case."""
+    import ssblasex_b200 as S
+    from ssblasex_b200 import runner, workloads as W
+    rng = np.random.default_rng(gcfg)
+    probs = []
+    for i in range(24):
+        m, n = (int(x) for x in rng.integers(20, 300, 2))
+        k = int(rng.choice([40, 200, 700, 1500]))
+        probs.append(W.make_problem("f64", i % 2, (i // 2) % 2, m, n, k, 1, 1.0, 0.5 if i % 3 == 0 else 0.0,
+                                    seed=900 + i, dist="expspread", name=f"o{i}"))
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("grouped", gcfg)
+    try:
+        gd = runner.GroupedDevice(probs)
+        for _ in range(2):
+            gd.reset_c()
+            assert gd.call(device_arrays=True) == 0
+            for p, C in zip(probs, gd.results()):
+                np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64), err_msg=p.name)
+    finally:
+        S.set_kernel_config("grouped", -1)
+        S.set_math_mode(0)

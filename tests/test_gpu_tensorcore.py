@@ -294,10 +294,63 @@ def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
         assert np.max(np.abs(got - ex) / nrm) <= 2.0 ** -14
 
 
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (128, 128, 200), (37, 29, 45), (100, 20, 300), (64, 100, 65),
+                                   (1, 1, 1)])
+@pytest.mark.parametrize("beta", [0.0, 0.25])
+def test_bf16x3_small_fused(S, ta, tb, shape, beta):
+    """Configuration 2: instances of at most 128 x 128 run as one kernel that splits hi/lo in
+    shared memory (no split pass): one launch, within FP32 accumulation error of the exact value of the three BF16
+    products and within the mode's stated 2^-14 of the exact product."""
+    from ssblasex_b200 import workloads as W
+    S.set_math_mode(S.SSBLAS_MATH_FP32_BF16X3)
+    m, n, k = shape
+    p = W.make_problem("f32", ta, tb, m, n, k, 5, 0.75, beta, ldc=m + 3, seed=m + n + k + ta, dist="outliers")
+    S.set_kernel_config("bf16x3_tcgen05", 2)
+    try:
+        C = run(p)
+        info = S.last_run_info()
+    finally:
+        S.set_kernel_config("bf16x3_tcgen05", -1)
+    assert info["path"] == "bf16x3_tcgen05" and info["kernel_launches"] == 1
+    for b in range(p.batch):
+        emu = O.bf16x3_f32(p, b)
+        ex, nrm = O.exact_f64(p, b)
+        got = p.c_view(C, b).astype(np.float64)
+        assert np.max(np.abs(got - emu) / nrm) <= 4 * k * 2.0 ** -24
+        assert np.max(np.abs(got - ex) / nrm) <= 2.0 ** -14
+    np.testing.assert_array_equal(C.reshape(p.batch, n, m + 3)[:, :, m:], p.C.reshape(p.batch, n, m + 3)[:, :, m:])
+
+
+@pytest.mark.parametrize("mode", ["device_array", "host_array"])
+@pytest.mark.parametrize("shape", [(300, 170, 333, 3), (1, 17, 40, 2), (130, 200, 1030, 2), (256, 64, 64, 5)])
+@pytest.mark.parametrize("extreme", [False, True])
+def test_ozaki_bulk_store_epilogue(S, mode, shape, extreme):
+    """Configuration 9 writes C with bulk tensor stores (beta = 0, equally spaced instances):
+    bit-exact against the restatement, C's ld padding untouched; regions holding a scale factor
+    outside the normal range (rows scaled by 2^-1060 and 2^1010) take the per-element path instead."""
+    from ssblasex_b200 import workloads as W
+    m, n, k, batch = shape
+    p = W.make_problem("f64", 0, 1, m, n, k, batch, 0.75, 0.0, ldc=m + 5, seed=m + n + k, dist="expspread")
+    if extreme:
+        for b in range(batch):
+            p.op_a(b)[0, :] *= 2.0 ** -1060
+            p.op_a(b)[m - 1, :] *= 2.0 ** 1010 if m > 1 else 1.0
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_tcgen05", 9)
+    try:
+        C = run(p, mode=mode)
+    finally:
+        S.set_kernel_config("ozaki_tcgen05", -1)
+    np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
+    pad = C.reshape(batch, n, m + 5)[:, :, m:]
+    np.testing.assert_array_equal(pad, p.C.reshape(batch, n, m + 5)[:, :, m:])
+
+
 # ------------------------------------------------------------------------- configurations ---
-@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2), ("ozaki_tcgen05", 3), ("ozaki_tcgen05", 4), ("ozaki_tcgen05", 5),
+@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2), ("ozaki_tcgen05", 3), ("ozaki_tcgen05", 4), ("ozaki_tcgen05", 5), ("ozaki_tcgen05", 6), ("ozaki_tcgen05", 7), ("ozaki_tcgen05", 8), ("ozaki_tcgen05", 9),
                                         ("i8_tcgen05", 0), ("i8_tcgen05", 1),
-                                        ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1),
+                                        ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1), ("bf16x3_tcgen05", 2),
                                         ("dmma", 0), ("dmma", 1), ("dmma", 2), ("dmma", 3), ("dmma", 4)])
 def test_every_kernel_configuration(S, family, cfg):
     """Each configuration the autotuner may pick gives the right answer on a ragged problem."""

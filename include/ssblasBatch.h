@@ -203,8 +203,8 @@ typedef enum {
   SSBLAS_PATH_F16_TCGEN05 = 11,     /* fp16 inputs (SSBLAS_EXT_R16F row) on tcgen05.mma kind::f16 */
   SSBLAS_PATH_GROUPED_OZAKI_TILE = 12 /* not a path: ssblasSetKernelConfig / tuning key of the tile
                                       shape of a grouped call's Ozaki instances per size bucket
-                                      (batch 1): 0 = 128 x 64 tiles, one accumulator; 1 = 128 x 32
-                                      tiles, two accumulators */
+                                      (batch 1): 0 = 128 x 64 tiles, one accumulator; 1 (default)
+                                      = 128 x 32 tiles, two accumulators */
 } ssblasPath_t;
 
 ssblasStatus_t ssblasGetLastRunInfo(ssblasRunInfo_t* info);

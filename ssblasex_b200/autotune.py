@@ -24,7 +24,7 @@ OUT = pathlib.Path(__file__).resolve().parent / "tune" / "ssblas_tune.json"
 
 # path -> (math mode, configurations, kernel name, problems)
 FAMILIES = {
-    "ozaki_tcgen05": (SSBLAS_MATH_FP64_OZAKI, [0, 1, 2, 3, 4, 5, 6, 7, 8, 9], "ozaki_gemm", [
+    "ozaki_tcgen05": (SSBLAS_MATH_FP64_OZAKI, [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11], "ozaki_gemm", [
         dict(row="f64", transa=0, transb=1, m=1024, n=1024, k=1024, batch=32, alpha=1.0, beta=0.0,
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=0, transb=0, m=512, n=512, k=512, batch=64, alpha=1.0, beta=0.0,
@@ -66,7 +66,7 @@ FAMILIES = {
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=1, transb=0, m=128, n=128, k=128, batch=256, alpha=1.0, beta=0.5),
     ]),
-    "simt": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4, 5], "(all)", [
+    "simt": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4, 5, 6, 7, 8, 9, 10, 11], "(all)", [
         dict(row="f32", transa=0, transb=0, m=128, n=128, k=128, batch=64, alpha=1.0, beta=0.5),
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),

@@ -214,8 +214,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_async_kerne
 // load latency per CTA. C of the item (when beta != 0) is read into registers before the
 // products, so that read overlaps them too.
 template <int BM, int BN, int BK, int TM, int TN, int KS, int MINB, bool A_MN, bool B_MN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kernel(SgemmArgs args, long tiles_m,
-                                                                                   long tiles, long total) {
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kernel(SgemmArgs args, uint32_t tiles_m,
+                                                                                   uint32_t tiles, uint32_t total) {
   constexpr int TX = BM / TM, TY = BN / TN, NT = TX * TY;
   constexpr int PA = BM + 4, PB = BN + 4;
   constexpr int STAGE = BK * (PA + PB);
@@ -228,9 +228,18 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kerne
   const long ktiles = (args.k + BK - 1) / BK;   // <= KS (checked by the launcher)
   const bool read_c = args.beta != 0.0f;
 
-  auto issue = [&](long w, int buf) {
-    const long b = w / tiles, t = w - b * tiles;
-    const long m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+  // work item w -> (instance b, tile t) -> (m0, n0), in 32-bit arithmetic (the launcher keeps the
+  // item count below 2^31): a 64-bit division costs dozens of instructions per item
+  auto item = [&](uint32_t w, long& b, long& m0, long& n0) {
+    const uint32_t bb = w / tiles, t = w - bb * tiles;
+    const uint32_t tn = t / tiles_m;
+    b = bb;
+    m0 = (long)(t - tn * tiles_m) * BM;
+    n0 = (long)tn * BN;
+  };
+  auto issue = [&](uint32_t w, int buf) {
+    long b, m0, n0;
+    item(w, b, m0, n0);
     const float* __restrict__ A = args.A[b];
     const float* __restrict__ B = args.B[b];
     const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kerne
     }
   };
 
-  long w = blockIdx.x;
+  uint32_t w = blockIdx.x;
   if (w < total) issue(w, 0);
   commit_s();
   for (int buf = 0; w < total; w += gridDim.x, buf ^= 1) {
@@ -252,8 +261,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kerne
     // closing barrier)
     if (w + gridDim.x < total) issue(w + gridDim.x, buf ^ 1);
     commit_s();
-    const long b = w / tiles, t = w - b * tiles;
-    const long m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+    long b, m0, n0;
+    item(w, b, m0, n0);
     float* __restrict__ C = args.C[b];
     const long gi0 = m0 + tx * TM;
     const bool cvec = (((uintptr_t)C) % 16 == 0) && (args.ldc % 4 == 0) && gi0 + TM <= args.m;
@@ -328,6 +337,244 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_small_kerne
   wait_s<0>();
 }
 
+// Register-heavy form for K <= KMAX: one 64 x 64 tile of one instance per CTA of 64 threads, each
+// thread an 8 x 8 block of C (rows 8 tx.., columns 8 ty.., tx = t % 8, ty = t / 8). The whole K of
+// the tile is requested at once (16-deep slices of the cp.async copies above, both operands
+// staged [k][rows]), C (beta != 0) is read into registers while the copies land, and the inner
+// loop issues 4 shared-memory vector loads per 64 FFMAs -- a quarter of the per-product overhead
+// of the 4 x 4 threads. Several CTAs per SM overlap one tile's loads with another's products.
+// (Staging a K-contiguous operand as it lies, [rows][k] with 16-byte copies, measured slower on
+// 4096 x 64^3 TT: 0.105 ms against 0.084 ms -- its rows 8 apart per thread turn the C stores
+// into 4-byte ones.)
+template <int KMAX, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__(64, MINB) sgemm_reg8_kernel(SgemmArgs args, uint32_t tiles_m, uint32_t tiles) {
+  constexpr int P = 64 + 4;
+  extern __shared__ __align__(16) float sm[];
+  float* sa = sm;                 // [KMAX][P] op(A): k, then m
+  float* sb = sm + KMAX * P;      // [KMAX][P] op(B): k, then n
+  const uint32_t w = blockIdx.x;
+  const uint32_t bb = w / tiles, t = w - bb * tiles;
+  const uint32_t tn = t / tiles_m;
+  const long b = bb;
+  const long m0 = (long)(t - tn * tiles_m) * 64, n0 = (long)tn * 64;
+  const float* __restrict__ A = args.A[b];
+  const float* __restrict__ B = args.B[b];
+  float* __restrict__ C = args.C[b];
+  const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
+  const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 4 == 0);
+  const int K = (int)args.k;   // <= KMAX (checked by the launcher)
+  const int slices = (K + 15) / 16;
+  for (int sl = 0; sl < slices; ++sl) {
+    sload<64, 16, 64, A_MN>(sa + sl * 16 * P, A, args.m, args.k, args.lda, m0, sl * 16, vecA);
+    sload<64, 16, 64, B_MN>(sb + sl * 16 * P, B, args.n, args.k, args.ldb, n0, sl * 16, vecB);
+  }
+  commit_s();
+
+  const int tx = threadIdx.x % 8, ty = threadIdx.x / 8;
+  const long gi0 = m0 + tx * 8;
+  const bool read_c = args.beta != 0.0f;
+  const bool cvec = (((uintptr_t)C) % 16 == 0) && (args.ldc % 4 == 0) && gi0 + 8 <= args.m;
+  // C of this thread's block, in flight while the operand copies land
+  float cv[8][8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const long gj = n0 + ty * 8 + j;
+    const float* cp = C + gi0 + gj * args.ldc;
+    if (read_c && gj < args.n && cvec) {
+      const float4 x0 = *(const float4*)cp, x1 = *(const float4*)(cp + 4);
+      cv[j][0] = x0.x; cv[j][1] = x0.y; cv[j][2] = x0.z; cv[j][3] = x0.w;
+      cv[j][4] = x1.x; cv[j][5] = x1.y; cv[j][6] = x1.z; cv[j][7] = x1.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) cv[j][i] = (read_c && gj < args.n && gi0 + i < args.m) ? cp[i] : 0.0f;
+    }
+  }
+  wait_s<0>();
+  __syncthreads();
+
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+#pragma unroll 4
+  for (int kk = 0; kk < K; ++kk) {
+    const float4 a0 = *(const float4*)(sa + kk * P + tx * 8), a1 = *(const float4*)(sa + kk * P + tx * 8 + 4);
+    const float4 b0 = *(const float4*)(sb + kk * P + ty * 8), b1 = *(const float4*)(sb + kk * P + ty * 8 + 4);
+    const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+  }
+
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const long gj = n0 + ty * 8 + j;
+    if (gj >= args.n) continue;
+    float* cp = C + gi0 + gj * args.ldc;
+    float o[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) o[i] = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[j][i] : 0.0f);
+    if (cvec) {
+      *(float4*)cp = make_float4(o[0], o[1], o[2], o[3]);
+      *(float4*)(cp + 4) = make_float4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (gi0 + i < args.m) cp[i] = o[i];
+    }
+  }
+}
+
+template <int KMAX, int MINB, bool A_MN, bool B_MN>
+cudaError_t launch_reg8(const SgemmArgs& a, cudaStream_t st) {
+  constexpr int SMEM = 2 * KMAX * (64 + 4) * 4;
+  auto kern = sgemm_reg8_kernel<KMAX, MINB, A_MN, B_MN>;
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
+  const long tiles_m = (a.m + 63) / 64;
+  const long tiles = tiles_m * ((a.n + 63) / 64);
+  const long total = tiles * a.batch;
+  if (total >= (1L << 31)) return cudaErrorNotSupported;
+  kern<<<(unsigned)total, 64, SMEM, st>>>(a, (uint32_t)tiles_m, (uint32_t)tiles);
+  return cudaGetLastError();
+}
+
+template <int KMAX, int MINB>
+cudaError_t launch_reg8_l(const SgemmArgs& a, bool a_mn, bool b_mn, cudaStream_t st) {
+  if (a_mn && b_mn) return launch_reg8<KMAX, MINB, true, true>(a, st);
+  if (a_mn) return launch_reg8<KMAX, MINB, true, false>(a, st);
+  if (b_mn) return launch_reg8<KMAX, MINB, false, true>(a, st);
+  return launch_reg8<KMAX, MINB, false, false>(a, st);
+}
+
+// K split inside the CTA, for k <= KMAX: one 64 x 64 tile per CTA of 256 threads, four groups of
+// 64 threads, each group an 8 x 8 block per thread over a quarter of K (as the 64-thread form
+// above), then the four partial tiles meet in shared memory (over the operand buffers) and every
+// thread adds its 16 outputs' parts in a fixed order (group 0 + 1 + 2 + 3) and applies alpha and
+// beta. Four times the warps of the 64-thread form per tile, so batches of few large-K tiles
+// (64 x 128^3: 256 tiles for 148 SMs) keep every scheduler fed.
+template <int KMAX, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__(256, MINB) sgemm_ksplit_kernel(SgemmArgs args, uint32_t tiles_m, uint32_t tiles) {
+  constexpr int P = 64 + 4;
+  extern __shared__ __align__(16) float sm[];
+  float* sa = sm;                 // [KMAX][P] op(A): k, then m
+  float* sb = sm + KMAX * P;      // [KMAX][P] op(B): k, then n
+  float* red = sm;                // after the products: [4 groups][64 columns][P] partial tiles
+  float* sc = sm + 2 * KMAX * P;  // [64 columns][P] C (beta != 0)
+  static_assert(2 * KMAX >= 4 * 64, "the partial tiles reuse the operand buffers");
+  const uint32_t w = blockIdx.x;
+  const uint32_t bb = w / tiles, t = w - bb * tiles;
+  const uint32_t tn = t / tiles_m;
+  const long b = bb;
+  const long m0 = (long)(t - tn * tiles_m) * 64, n0 = (long)tn * 64;
+  const float* __restrict__ A = args.A[b];
+  const float* __restrict__ B = args.B[b];
+  float* __restrict__ C = args.C[b];
+  const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
+  const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 4 == 0);
+  const int K = (int)args.k;   // <= KMAX (checked by the launcher)
+  const bool read_c = args.beta != 0.0f;
+  const bool vecC = ((uintptr_t)C % 16 == 0) && (args.ldc % 4 == 0);
+  for (int sl = 0; sl < (K + 15) / 16; ++sl) {
+    sload<64, 16, 256, A_MN>(sa + sl * 16 * P, A, args.m, args.k, args.lda, m0, sl * 16, vecA);
+    sload<64, 16, 256, B_MN>(sb + sl * 16 * P, B, args.n, args.k, args.ldb, n0, sl * 16, vecB);
+  }
+  // C tile (columns n0.., rows m0..) staged [column][row], in flight with the operands
+  if (read_c)
+    for (int sl = 0; sl < 4; ++sl)
+      sload<64, 16, 256, true>(sc + sl * 16 * P, C, args.m, args.n, args.ldc, m0, n0 + sl * 16, vecC);
+  commit_s();
+
+  // output mapping of the final sum: thread t takes rows 4 (t % 16).., columns 4 (t / 16)..
+  const int orow = 4 * (threadIdx.x % 16), ocol = 4 * (threadIdx.x / 16);
+  const long gi0 = m0 + orow;
+  const bool cvec = vecC && gi0 + 4 <= args.m;
+  wait_s<0>();
+  __syncthreads();
+
+  const int g = threadIdx.x / 64, t64 = threadIdx.x % 64;
+  const int tx = t64 % 8, ty = t64 / 8;
+  const int kq = (K + 3) / 4;
+  const int k0 = g * kq, k1 = (k0 + kq < K) ? k0 + kq : K;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+#pragma unroll 2
+  for (int kk = k0; kk < k1; ++kk) {
+    const float4 a0 = *(const float4*)(sa + kk * P + tx * 8), a1 = *(const float4*)(sa + kk * P + tx * 8 + 4);
+    const float4 b0 = *(const float4*)(sb + kk * P + ty * 8), b1 = *(const float4*)(sb + kk * P + ty * 8 + 4);
+    const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+  }
+  __syncthreads();   // every group is done with the operand buffers
+  float* part = red + g * 64 * P;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    float* q = part + (ty * 8 + j) * P + tx * 8;
+    *(float4*)q = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+    *(float4*)(q + 4) = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
+  }
+  __syncthreads();
+
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const long gj = n0 + ocol + j;
+    if (gj >= args.n) continue;
+    float4 s = *(const float4*)(red + (ocol + j) * P + orow);
+#pragma unroll
+    for (int gg = 1; gg < 4; ++gg) {
+      const float4 x = *(const float4*)(red + gg * 64 * P + (ocol + j) * P + orow);
+      s.x += x.x; s.y += x.y; s.z += x.z; s.w += x.w;
+    }
+    const float sv[4] = {s.x, s.y, s.z, s.w};
+    float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (read_c) c4 = *(const float4*)(sc + (ocol + j) * P + orow);
+    const float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+    float o[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) o[i] = fmaf(sv[i], args.alpha, read_c ? args.beta * cv[i] : 0.0f);
+    float* cp = C + gi0 + gj * args.ldc;
+    if (cvec) {
+      *(float4*)cp = make_float4(o[0], o[1], o[2], o[3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (gi0 + i < args.m) cp[i] = o[i];
+    }
+  }
+}
+
+template <int KMAX, int MINB, bool A_MN, bool B_MN>
+cudaError_t launch_ksplit(const SgemmArgs& a, cudaStream_t st) {
+  constexpr int SMEM = (2 * KMAX + 64) * (64 + 4) * 4;
+  auto kern = sgemm_ksplit_kernel<KMAX, MINB, A_MN, B_MN>;
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
+  const long tiles_m = (a.m + 63) / 64;
+  const long tiles = tiles_m * ((a.n + 63) / 64);
+  const long total = tiles * a.batch;
+  if (total >= (1L << 31)) return cudaErrorNotSupported;
+  kern<<<(unsigned)total, 256, SMEM, st>>>(a, (uint32_t)tiles_m, (uint32_t)tiles);
+  return cudaGetLastError();
+}
+
+template <int KMAX, int MINB>
+cudaError_t launch_ksplit_l(const SgemmArgs& a, bool a_mn, bool b_mn, cudaStream_t st) {
+  if (a_mn && b_mn) return launch_ksplit<KMAX, MINB, true, true>(a, st);
+  if (a_mn) return launch_ksplit<KMAX, MINB, true, false>(a, st);
+  if (b_mn) return launch_ksplit<KMAX, MINB, false, true>(a, st);
+  return launch_ksplit<KMAX, MINB, false, false>(a, st);
+}
+
 template <int BM, int BN, int BK, int TM, int TN, int KS, int MINB, bool A_MN, bool B_MN>
 cudaError_t launch_small(const SgemmArgs& a, cudaStream_t st) {
   constexpr int NT = (BM / TM) * (BN / TN);
@@ -346,8 +593,10 @@ cudaError_t launch_small(const SgemmArgs& a, cudaStream_t st) {
   const long tiles_m = (a.m + BM - 1) / BM;
   const long tiles = tiles_m * ((a.n + BN - 1) / BN);
   const long total = tiles * a.batch;
+  if (total >= (1L << 31)) return cudaErrorNotSupported;   // the caller takes the tiled kernel
   const long cap = (long)per_sm * num_sms();
-  kern<<<(unsigned)(total < cap ? total : cap), NT, SMEM, st>>>(a, tiles_m, tiles, total);
+  kern<<<(unsigned)(total < cap ? total : cap), NT, SMEM, st>>>(a, (uint32_t)tiles_m, (uint32_t)tiles,
+                                                                 (uint32_t)total);
   return cudaGetLastError();
 }
 
@@ -389,17 +638,42 @@ cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t st) 
   cudaError_t e;
   // 3: 64 x 64 tiles, 256 threads of 4 x 4, 32-deep K stages x 2 (k <= 64 entirely in flight)
   // 4: 128 x 128 tiles, 256 threads of 8 x 8, 16-deep K stages x 3
-  // 5 (k <= 64): 64 x 64 tiles, persistent CTAs that double-buffer their work items
-  if (config == 5 && d.k <= 64) {
+  // 5 (k <= 64): 64 x 64 tiles, persistent CTAs that double-buffer their work items, 256 threads
+  //   of 4 x 4
+  // 6 (k <= 64): as 5 with 128 threads of 8 x 4 (twice the products per thread for the same
+  //   per-item index, copy and epilogue work)
+  // 7: 32 x 64 tiles, 128 threads of 4 x 4, 32-deep K stages x 4 (k <= 128 entirely in flight):
+  //   four times the CTAs of configuration 3, for batches whose 64 x 64 tiles fill under a wave
+  // 8: 32 x 32 tiles, 64 threads of 4 x 4, 16-deep K stages x 8
+  // 9 (k <= 64) / 10 (k <= 128): 64 x 64 tiles, 64 threads of 8 x 8, the whole K at once
+  // 11 (k <= 128): 64 x 64 tiles, 256 threads: four 8 x 8 groups over quarters of K, summed in
+  //   shared memory
+  e = cudaErrorNotSupported;
+  if (config == 9 && d.k <= 64) {
+    e = launch_reg8_l<64, 4>(a, a_mn, b_mn, st);
+  } else if (config == 10 && d.k <= 128) {
+    e = launch_reg8_l<128, 3>(a, a_mn, b_mn, st);
+  } else if (config == 11 && d.k <= 128) {
+    e = launch_ksplit_l<128, 2>(a, a_mn, b_mn, st);
+  } else if (config == 5 && d.k <= 64) {
     if (a_mn && b_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, true, true>(a, st);
     else if (a_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, true, false>(a, st);
     else if (b_mn) e = launch_small<64, 64, 32, 4, 4, 2, 3, false, true>(a, st);
     else e = launch_small<64, 64, 32, 4, 4, 2, 3, false, false>(a, st);
+  } else if (config == 6 && d.k <= 64) {
+    if (a_mn && b_mn) e = launch_small<64, 64, 32, 8, 4, 2, 3, true, true>(a, st);
+    else if (a_mn) e = launch_small<64, 64, 32, 8, 4, 2, 3, true, false>(a, st);
+    else if (b_mn) e = launch_small<64, 64, 32, 8, 4, 2, 3, false, true>(a, st);
+    else e = launch_small<64, 64, 32, 8, 4, 2, 3, false, false>(a, st);
   } else if (config == 4) {
     e = launch_sl<128, 128, 16, 8, 8, 3, 1>(a, a_mn, b_mn, st);
-  } else {
-    e = launch_sl<64, 64, 32, 4, 4, 2, 3>(a, a_mn, b_mn, st);
+  } else if (config == 7) {
+    e = launch_sl<32, 64, 32, 4, 4, 4, 4>(a, a_mn, b_mn, st);
+  } else if (config == 8) {
+    e = launch_sl<32, 32, 16, 4, 4, 8, 8>(a, a_mn, b_mn, st);
   }
+  // configuration 3 serves the rest (and item counts of 2^31 or more for 5 and 6)
+  if (e == cudaErrorNotSupported) e = launch_sl<64, 64, 32, 4, 4, 2, 3>(a, a_mn, b_mn, st);
   note_launch();
   return e;
 }

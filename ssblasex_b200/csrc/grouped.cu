@@ -445,16 +445,15 @@ std::map<int, std::unique_ptr<Plan>> g_plans;   // one cached plan per device
 
 // Tile shape of one Ozaki instance: 128 x 64 tiles with one accumulator read the slice planes from
 // shared memory a third more efficiently per product than 128 x 32 tiles with two, whose gain is
-// an epilogue that overlaps the next tile's MMAs; so the wide tiles pay where K is long enough to
-// amortise the exposed epilogue and the narrow side fills them. Per size bucket (batch 1) the
-// tuning table may choose (SSBLAS_PATH_GROUPED_OZAKI_TILE: 0 = 128 x 64, 1 = 128 x 32); the
-// grouped configuration 0 or 2 forces one shape for all.
+// an epilogue that overlaps the next tile's MMAs. Per size bucket (batch 1) the tuning table may
+// choose (SSBLAS_PATH_GROUPED_OZAKI_TILE: 0 = 128 x 64, 1 = 128 x 32); without an entry the tiles
+// are 128 x 32: on the 10,000-instance mix (m, n, k log-uniform in [8, 512]) 128 x 64 tiles for
+// the instances with k >= 384 and both sides >= 48 took 1.95 ms against 1.80 ms for 128 x 32
+// everywhere. The grouped configuration 0 or 2 forces one shape for all.
 bool ozaki_wide_tiles(const GroupedInst& in, int gcfg) {
   if (gcfg == 0) return true;
   if (gcfg == 2) return false;
-  const long narrow = in.m < in.n ? in.m : in.n;   // the tiles' narrow side after orientation
-  const int fallback = (in.k >= 384 && narrow >= 48) ? 0 : 1;
-  return choose_config(SSBLAS_PATH_GROUPED_OZAKI_TILE, in.m, in.n, in.k, 1, fallback) == 0;
+  return choose_config(SSBLAS_PATH_GROUPED_OZAKI_TILE, in.m, in.n, in.k, 1, 1) == 0;
 }
 
 std::vector<uint64_t> signature(const GroupedDesc& g, int mode, int oz_cfg) {

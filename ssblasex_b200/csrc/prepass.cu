@@ -718,6 +718,10 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     ptx::fence_mbar_init();
   }
   __syncthreads();
+  // under a programmatic launch the set-up above overlaps the end of the kernel before; the
+  // operands, planes and exponents are touched only after it has completed
+  ptx::grid_dep_wait();
+  ptx::grid_dep_launch();
 
   // prologue: the first two items of this cluster
   for (int s = 0; s < 2; ++s) {
@@ -950,7 +954,7 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   cfg.blockDim = dim3(NTH, 1, 1);
   cfg.dynamicSmemBytes = SMEM;
   cfg.stream = st;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = (unsigned)CS;
   at[0].val.clusterDim.y = 1;
@@ -975,6 +979,11 @@ cudaError_t launch_cluster_st(const CUtensorMap& tm0, const CUtensorMap& tm1, co
   const long n_items = (n0 + n1) * KB;
   const long nclusters = n_items < max_clusters[CS] ? n_items : max_clusters[CS];
   cfg.gridDim = dim3((unsigned)(nclusters * CS), 1, 1);
+  // programmatic launch: the CTAs' set-up overlaps the end of the kernel before (the kernel waits
+  // for it before touching global memory)
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.numAttrs = 2;
   return cudaLaunchKernelEx(&cfg, kern, tm0, tm1, a0, e0, n0, a1, e1, n_items, CS, device_error_flag(), bits0,
                             bits1, KB);
 }

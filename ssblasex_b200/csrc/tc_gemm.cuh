@@ -20,6 +20,8 @@
 // warps 2-9 = epilogue (warp w reads TMEM lanes 32*(w%4) .. +31, half (w-2)/4 of the columns).
 #pragma once
 
+#include <type_traits>
+
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -180,9 +182,26 @@ struct Config {
   // 32 x 16 outputs to a 4 KB shared-memory buffer and one lane hands them to a bulk tensor store,
   // so the warp is free for the next tile's accumulator instead of waiting on its global stores
   static constexpr bool C_TMA = (OPT_ & 16) != 0;
+  // (bit 5) two-part accumulator release (Ozaki, one accumulator): the levels are split into a
+  // top group (the last TOPN, which the Horner pass reads first) and a bottom group, and every
+  // MMA stays inside one group. The epilogue hands the top group back as soon as it has read it;
+  // the MMA warp then issues the next tile's top-group products of its first STAGES K blocks and
+  // only waits for the bottom group after them, so the drain of the bottom levels (and their
+  // conversions) overlaps tensor-core work instead of stalling it. Same products, same Horner
+  // order: the results are bit for bit those of the other configurations. Measured slower than
+  // the ungrouped order on 32 x 1024^3 (GEMM 0.70 against 0.62 ms): MMAs confined to a group are
+  // more and narrower (11 per K step instead of 10, one N = 256 instead of four), and that costs
+  // more tensor time than the hidden drain saves.
+  static constexpr bool EARLY = (OPT_ & 32) != 0;
+  // (bit 7, with bit 5) a top group of two levels instead of three (13 MMAs per K step; measured
+  // 0.71 ms)
+  static constexpr int TOPN = (OPT_ & 128) ? 2 : 3;
+  static constexpr int TOP0 = NLEV_ - TOPN;           // first level of the top group
   static constexpr int C_STAGING = C_TMA ? 8 * 32 * 16 * 8 : 0;
   static constexpr int A_SLOTS = SPLIT_STAGE ? 8 : PA_;
   static_assert(!SPLIT_STAGE || (PAIRS_ == 2 && PA_ > 4 && PA_ <= 8 && !AREUSE), "split stages: Ozaki, 5-8 slices");
+  static_assert(!EARLY || (PAIRS_ == 2 && ACCB_ == 1 && NLEV_ >= 4 && !AREUSE && !SPLIT_STAGE && !DRAIN_PIPE),
+                "two-part release: Ozaki, one accumulator, plain MMA order");
   static constexpr int ELEM = (KIND == KIND_I8) ? 1 : 2;
   static constexpr int KROWS = KB_ / ELEM;             // K elements (MN-major: K rows) per stage
   static constexpr int MN_BLOCK = KROWS * 128;         // bytes of one 128-byte-wide MN block
@@ -486,6 +505,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   __syncthreads();
   ptx::tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  // the set-up above (barriers, tensor memory, tensor-map prefetch) touches no global data, so
+  // under a programmatic launch it overlaps the end of the kernel before; every global access
+  // comes after the wait
+  ptx::grid_dep_wait();
+  ptx::grid_dep_launch();
 
   const long tiles_mn = (long)prm.tiles_m * prm.tiles_n;
   const int KE = Cfg::KB / Cfg::ELEM;                       // K elements per stage
@@ -600,6 +624,75 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         const int acc = tcount % Cfg::ACCB;
         const uint32_t acc_ph = (uint32_t)((tcount / Cfg::ACCB) & 1);
+        if constexpr (Cfg::EARLY && !GROUPED) {
+          // two-part release: tempty[0] = top group drained, tempty[1] = bottom group drained
+          constexpr int MAXQ = 256 / Cfg::BN;
+          const uint32_t d_base = tmem_base;
+          // the MMAs of one group for one K block in stage s; first = the tile's first K block
+          // (the group is a compile-time constant, so every loop below unrolls completely and
+          // the descriptors fold into constants plus the stage address)
+          auto issue_group = [&](auto top_c, int s, bool first) {
+            constexpr bool top = decltype(top_c)::value;
+            const uint32_t sa = ptx::smem_u32(stages + (size_t)s * Cfg::STAGE);
+            const uint32_t sb = sa + Cfg::A_STAGE;
+#pragma unroll
+            for (int p = 0; p < Cfg::PA; ++p) {
+              const int qlo = top ? (Cfg::TOP0 - p > 0 ? Cfg::TOP0 - p : 0) : 0;
+              const int qhi = top ? Cfg::NLEV - 1 - p : Cfg::TOP0 - 1 - p;   // inclusive
+#pragma unroll
+              for (int q0 = qlo; q0 <= qhi; q0 += MAXQ) {
+                const int nq = (qhi - q0 + 1) < MAXQ ? (qhi - q0 + 1) : MAXQ;
+                const uint32_t idesc = ptx::idesc_i8(128, nq * Cfg::BN, true, true);
+                const uint32_t d = d_base + (uint32_t)((p + q0) * Cfg::BN);
+#pragma unroll
+                for (int kk = 0; kk < Cfg::KB / 32; ++kk) {
+                  const uint64_t ad = ptx::smem_desc_kmajor(sa + p * Cfg::BM * Cfg::KB + kk * 32, Cfg::KB);
+                  const uint64_t bd = ptx::smem_desc_kmajor(sb + q0 * Cfg::BN * Cfg::KB + kk * 32, Cfg::KB);
+                  // every level of a group is first written by its p = 0 MMA
+                  ptx::mma_i8(d, ad, bd, idesc, (!first || kk > 0 || p > 0) ? 1u : 0u);
+                }
+              }
+            }
+          };
+          if (!ptx::mbar_wait(ptx::smem_u32(&tempty[0]), acc_ph ^ 1, err, 21, wl)) { ok = false; break; }
+          ptx::tc_fence_after();
+          const long nkb = ti.kb1 - ti.kb0;
+          const int D = nkb < Cfg::STAGES ? (int)nkb : Cfg::STAGES;
+          // the top-group products of the first D K blocks, while the bottom group drains
+          for (int j = 0; j < D; ++j) {
+            const long itj = it + j;
+            if (!ptx::mbar_wait(ptx::smem_u32(&full[itj % Cfg::STAGES]), (uint32_t)((itj / Cfg::STAGES) & 1), err, 22,
+                                wl)) {
+              ok = false;
+              break;
+            }
+            ptx::tc_fence_after();
+            issue_group(std::true_type{}, (int)(itj % Cfg::STAGES), j == 0);
+          }
+          if (!ok) break;
+          if (!ptx::mbar_wait(ptx::smem_u32(&tempty[1]), acc_ph ^ 1, err, 26, wl)) { ok = false; break; }
+          ptx::tc_fence_after();
+          for (int j = 0; j < D; ++j) {
+            const int s = (int)((it + j) % Cfg::STAGES);
+            issue_group(std::false_type{}, s, j == 0);
+            ptx::mma_commit(ptx::smem_u32(&empty[s]));
+          }
+          it += D;
+          for (long kb = ti.kb0 + D; kb < ti.kb1; ++kb, ++it) {
+            const int s = (int)(it % Cfg::STAGES);
+            if (!ptx::mbar_wait(ptx::smem_u32(&full[s]), (uint32_t)((it / Cfg::STAGES) & 1), err, 22, wl)) {
+              ok = false;
+              break;
+            }
+            ptx::tc_fence_after();
+            issue_group(std::true_type{}, s, false);
+            issue_group(std::false_type{}, s, false);
+            ptx::mma_commit(ptx::smem_u32(&empty[s]));
+          }
+          if (!ok) break;
+          ptx::mma_commit(ptx::smem_u32(&tfull[0]));
+          continue;
+        }
         if (!ptx::mbar_wait(ptx::smem_u32(&tempty[acc]), acc_ph ^ 1, err, 21, wl)) { ok = false; break; }
         ptx::tc_fence_after();
         const uint32_t d_base = tmem_base + (uint32_t)(acc * Cfg::NLEV * Cfg::BN);
@@ -796,6 +889,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                                     warp - 2, row_in_tile, lane, ptx::smem_u32(&tempty[acc]), row_ok, Cb, gi, n0, n,
                                     ldc, (Cfg::EPI == EPI_OZAKI && row_ok) ? exa[gi] : 0, exb, prm.exp_shift, alpha_d, beta_d,
                                     alpha_i, beta_i);
+          if constexpr (Cfg::EARLY) {
+            // the split epilogue drains the whole accumulator before its arrival on tempty[0]
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[1]));
+          }
           continue;
         }
       }
@@ -805,7 +903,45 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // warp before the (slower) scaling and global stores.
         constexpr int CH = HALF / 16;
         double v[CH][16];
-        if constexpr (Cfg::DRAIN_PIPE && CH == 2 && Cfg::NLEV == 7) {
+        if constexpr (Cfg::EARLY) {
+          // the top group (levels NLEV-1 .. TOP0: the first TOPN Horner steps), handed back at
+          // once; then the bottom group continues the same Horner sequence
+#pragma unroll
+          for (int c = 0; c < CH; ++c) {
+            uint32_t raw[Cfg::TOPN][16];
+#pragma unroll
+            for (int q = 0; q < Cfg::TOPN; ++q)
+              ptx::tmem_ld16(t_row + (uint32_t)((Cfg::NLEV - 1 - q) * Cfg::BN + c * 16), raw[q]);
+            ptx::tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              double x = 0.0;
+#pragma unroll
+              for (int q = 0; q < Cfg::TOPN; ++q) x = fma(x, 0x1p-8, i32_to_f64(raw[q][j]));
+              v[c][j] = x;
+            }
+          }
+          ptx::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[0]));
+#pragma unroll
+          for (int c = 0; c < CH; ++c) {
+#pragma unroll
+            for (int l0 = Cfg::TOP0 - 1; l0 >= 0; l0 -= 4) {
+              uint32_t raw[4][16];
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (l0 - q >= 0) ptx::tmem_ld16(t_row + (uint32_t)((l0 - q) * Cfg::BN + c * 16), raw[q]);
+              ptx::tmem_wait_ld();
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (l0 - q >= 0) {
+#pragma unroll
+                  for (int j = 0; j < 16; ++j) v[c][j] = fma(v[c][j], 0x1p-8, i32_to_f64(raw[q][j]));
+                }
+            }
+          }
+        } else if constexpr (Cfg::DRAIN_PIPE && CH == 2 && Cfg::NLEV == 7) {
           // batches: chunk 0 levels 6..3, chunk 1 levels 6..3, chunk 0 levels 2..0, chunk 1
           // levels 2..0; each batch's loads go out before the previous batch is combined (the
           // same Horner order and operations as below, so the same results bit for bit)
@@ -867,7 +1003,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
         ptx::tc_fence_before();
         __syncwarp();
-        if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[acc]));
+        if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&tempty[Cfg::EARLY ? 1 : acc]));
         if constexpr (PRE) {
           if (row_ok) ozaki_store<1, true>((double*)Cb, gi, n0, n, rs, ldc, pre_ea, exb, prm.exp_shift, alpha_d, beta_d, v, pre_eb);
         } else {

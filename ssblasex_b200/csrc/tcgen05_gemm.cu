@@ -95,9 +95,12 @@ int choose_splits(const SplitPlan& sp, long m, long n, long k, long batch, long 
   return s < 1 ? 1 : (int)s;
 }
 
+// pdl: launch with programmatic stream serialization (the kernel's set-up overlaps the end of the
+// kernel before it in the stream; tc_gemm_kernel waits for that kernel before any global access)
 template <class Cfg>
 cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params prm, cudaStream_t st,
-                     const char* name, const SplitPlan& plan = SplitPlan(), const CUtensorMap* tcmap = nullptr) {
+                     const char* name, const SplitPlan& plan = SplitPlan(), const CUtensorMap* tcmap = nullptr,
+                     bool pdl = false) {
   CUtensorMap tmc;
   if (tcmap) tmc = *tcmap;
   else memset(&tmc, 0, sizeof(tmc));
@@ -146,6 +149,19 @@ cudaError_t run_gemm(const CUtensorMap& ta, const CUtensorMap& tb, tc::Params pr
   if (prm.splits > 1) {
     if constexpr (Cfg::SPLITTABLE)
       tc::tc_gemm_kernel<Cfg, false, true><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, tmc, prm);
+  } else if (pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(tc::kThreads, 1, 1);
+    cfg.dynamicSmemBytes = Cfg::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    note_launch();
+    return cudaLaunchKernelEx(&cfg, tc::tc_gemm_kernel<Cfg, false, false>, ta, tb, tmc, prm);
   } else {
     tc::tc_gemm_kernel<Cfg, false, false><<<(unsigned)grid, tc::kThreads, Cfg::SMEM, st>>>(ta, tb, tmc, prm);
   }
@@ -214,6 +230,12 @@ using OzCfg7KB64S = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI
 using OzCfg7KB64SP = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 12>;
 //   9: configuration 1 with the results written by bulk tensor stores (beta == 0)
 using OzCfg7KB64T = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 16>;
+//  10: configuration 9 with the accumulator handed back in two parts (the top three levels
+//      first), so the next tile's top-level products overlap the drain of the bottom levels;
+//  11: the same with a top group of two levels. Both are bit-exact and slower on 32 x 1024^3
+//      (GEMM 0.70 / 0.71 ms against 0.62): the grouped MMA order costs more than the drain it hides
+using OzCfg7KB64TE = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 48>;
+using OzCfg7KB64TE2 = tc::Config<tc::KIND_I8, 7, 7, 64, 64, 2, 7, 1, tc::EPI_OZAKI, 2, 0, 0, 176>;
 
 // Ozaki split-K: a piece holds at most 16384 k (its int32 level sums stay exact); automatic
 // pieces keep at least 512 k.
@@ -262,7 +284,8 @@ cudaError_t ozaki_gemm_cfg(const BatchDesc& d, int S, const int8_t* pa, const in
       }
     }
   }
-  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split), tcp);
+  // programmatic launch: the set-up overlaps the slicing kernel's last items
+  return run_gemm<Cfg>(ta, tb, prm, st, "ozaki_gemm", ozaki_split_plan<Cfg>(allow_split), tcp, true);
 }
 
 // exa: exponents of the rows of op(A), [batch][m]; exb: of the columns of op(B), [batch][n]
@@ -285,6 +308,8 @@ cudaError_t ozaki_gemm(const BatchDesc& d, int S, const int8_t* pa, const int8_t
       if (c == 7) return ozaki_gemm_cfg<OzCfg7KB64S>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       if (c == 8) return ozaki_gemm_cfg<OzCfg7KB64SP>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       if (c == 9) return ozaki_gemm_cfg<OzCfg7KB64T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 10) return ozaki_gemm_cfg<OzCfg7KB64TE>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
+      if (c == 11) return ozaki_gemm_cfg<OzCfg7KB64TE2>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
       return ozaki_gemm_cfg<OzCfg<7>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
     }
     default: return ozaki_gemm_cfg<OzCfg<8>::T>(d, S, pa, pb, exa, exb, Kp, allow_split, st);
@@ -558,14 +583,16 @@ cudaError_t launch_ozaki_gemm_on(const BatchDesc& d, int S, const int8_t* pa, co
 cudaError_t launch_bf16x3_f32(const BatchDesc& d, cudaStream_t st) {
   if (!is_sm100() || !encoder()) return cudaErrorNotSupported;
   if (d.m > (1L << 31) || d.n > (1L << 31) || d.k > (1L << 31)) return cudaErrorNotSupported;
-  // configurations: 0 / 1 = split pass then tiled GEMM with 64- / 128-column tiles (the defaults);
-  // 2 = one kernel that splits in shared memory, for instances of at most 128 x 128 -- measured
-  // slower on 4096 x 64^3 (0.38 ms against 0.156 ms: one instance in flight per CTA leaves it
-  // bound by memory latency), so only a configuration
+  // configurations: 0 / 1 = split pass then tiled GEMM with 64- / 128-column tiles; 2 = one
+  // kernel that splits in shared memory, for equally spaced instances of at most 128 x 128 (the
+  // others take configuration 0 / 1)
   const int fallback = d.n <= 64 ? 0 : 1;
   const int cfg = choose_config(SSBLAS_PATH_BF16X3_TCGEN05, d.m, d.n, d.k, d.batch, fallback);
-  if (cfg == 2 && bf16x3_small_fits(d)) return launch_bf16x3_small(d, st);
   cudaError_t e;
+  if (cfg == 2 && bf16x3_small_fits(d)) {
+    e = launch_bf16x3_small(d, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
   const long Kp = round_up(d.k, 8);
   const long sa = d.m * Kp * 2, sb = d.n * Kp * 2;   // bytes per plane
   void* pa = workspace(WS_PACK_A, (size_t)sa * 2 * d.batch, &e);

@@ -296,23 +296,30 @@ def test_bf16x3_against_emulation_oracle(S, ta, tb, shape):
 
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (128, 128, 200), (37, 29, 45), (100, 20, 300), (64, 100, 65),
-                                   (1, 1, 1)])
+                                   (1, 1, 1), (50, 128, 130)])
 @pytest.mark.parametrize("beta", [0.0, 0.25])
-def test_bf16x3_small_fused(S, ta, tb, shape, beta):
-    """Configuration 2: instances of at most 128 x 128 run as one kernel that splits hi/lo in
-    shared memory (no split pass): one launch, within FP32 accumulation error of the exact value of the three BF16
-    products and within the mode's stated 2^-14 of the exact product."""
+@pytest.mark.parametrize("aligned", [True, False])
+def test_bf16x3_small_fused(S, ta, tb, shape, beta, aligned):
+    """Configuration 2: instances of at most 128 x 128 that are equally spaced with leading
+    dimensions a multiple of 4 run as one kernel that splits hi/lo in shared memory (no split
+    pass): one launch (odd leading dimensions take the split pass and the tiled GEMM), within FP32
+    accumulation error of the exact value of the three BF16 products and within the mode's stated
+    2^-14 of the exact product; more instances than SMs, so every CTA streams several."""
     from ssblasex_b200 import workloads as W
     S.set_math_mode(S.SSBLAS_MATH_FP32_BF16X3)
     m, n, k = shape
-    p = W.make_problem("f32", ta, tb, m, n, k, 5, 0.75, beta, ldc=m + 3, seed=m + n + k + ta, dist="outliers")
+    arows, brows = (m if ta == 0 else k), (k if tb == 0 else n)
+    lda, ldb = ((arows + 3) // 4 * 4 + 4, (brows + 3) // 4 * 4 + 4) if aligned else (arows | 1, brows | 1)
+    batch = 300 if shape == (64, 64, 64) else 5
+    p = W.make_problem("f32", ta, tb, m, n, k, batch, 0.75, beta, lda=lda, ldb=ldb, ldc=m + 3,
+                       seed=m + n + k + ta, dist="outliers")
     S.set_kernel_config("bf16x3_tcgen05", 2)
     try:
         C = run(p)
         info = S.last_run_info()
     finally:
         S.set_kernel_config("bf16x3_tcgen05", -1)
-    assert info["path"] == "bf16x3_tcgen05" and info["kernel_launches"] == 1
+    assert info["path"] == "bf16x3_tcgen05" and info["kernel_launches"] == (1 if aligned else 2)
     for b in range(p.batch):
         emu = O.bf16x3_f32(p, b)
         ex, nrm = O.exact_f64(p, b)
@@ -320,6 +327,34 @@ def test_bf16x3_small_fused(S, ta, tb, shape, beta):
         assert np.max(np.abs(got - emu) / nrm) <= 4 * k * 2.0 ** -24
         assert np.max(np.abs(got - ex) / nrm) <= 2.0 ** -14
     np.testing.assert_array_equal(C.reshape(p.batch, n, m + 3)[:, :, m:], p.C.reshape(p.batch, n, m + 3)[:, :, m:])
+
+
+@pytest.mark.parametrize("cfg", [10, 11])
+@pytest.mark.parametrize("shape,beta,splits", [((300, 170, 333, 3), 0.0, 0), ((129, 65, 64, 2), 0.5, 0),
+                                               ((256, 128, 2000, 2), 0.0, 3), ((200, 300, 4100, 1), -1.5, 2),
+                                               ((1024, 512, 1024, 2), 0.0, 0)])
+def test_ozaki_two_part_release(S, cfg, shape, beta, splits):
+    """Configurations 10 and 11 hand the accumulator back in two parts (the top three / two levels
+    first) and issue the next tile's top-level products before the bottom levels are drained: bit-exact
+    against the restatement with one K block per tile (k = 64, fewer blocks than stages), many
+    blocks, forced split-K pieces (whose epilogue releases both parts at once), and enough tiles
+    that every CTA runs several in a row."""
+    from ssblasex_b200 import workloads as W
+    m, n, k, batch = shape
+    p = W.make_problem("f64", 0, 1, m, n, k, batch, 0.75, beta, seed=m + k + cfg, dist="expspread")
+    S.set_math_mode(S.SSBLAS_MATH_FP64_OZAKI)
+    S.set_kernel_config("ozaki_tcgen05", cfg)
+    S.set_kernel_config("splitk_ozaki", splits)
+    try:
+        C = run(p)
+        info = S.last_run_info()
+    finally:
+        S.set_kernel_config("ozaki_tcgen05", -1)
+        S.set_kernel_config("splitk_ozaki", -1)
+    assert info["path"] == "ozaki_tcgen05" and info["slices"] == 7
+    if splits:
+        assert info["split_k"] == splits
+    np.testing.assert_array_equal(C.view(np.uint64), O.ozaki_f64(p, 7)[1].view(np.uint64))
 
 
 @pytest.mark.parametrize("mode", ["device_array", "host_array"])
@@ -348,7 +383,7 @@ def test_ozaki_bulk_store_epilogue(S, mode, shape, extreme):
 
 
 # ------------------------------------------------------------------------- configurations ---
-@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2), ("ozaki_tcgen05", 3), ("ozaki_tcgen05", 4), ("ozaki_tcgen05", 5), ("ozaki_tcgen05", 6), ("ozaki_tcgen05", 7), ("ozaki_tcgen05", 8), ("ozaki_tcgen05", 9),
+@pytest.mark.parametrize("family,cfg", [("ozaki_tcgen05", 0), ("ozaki_tcgen05", 1), ("ozaki_tcgen05", 2), ("ozaki_tcgen05", 3), ("ozaki_tcgen05", 4), ("ozaki_tcgen05", 5), ("ozaki_tcgen05", 6), ("ozaki_tcgen05", 7), ("ozaki_tcgen05", 8), ("ozaki_tcgen05", 9), ("ozaki_tcgen05", 10), ("ozaki_tcgen05", 11),
                                         ("i8_tcgen05", 0), ("i8_tcgen05", 1),
                                         ("bf16x3_tcgen05", 0), ("bf16x3_tcgen05", 1), ("bf16x3_tcgen05", 2),
                                         ("dmma", 0), ("dmma", 1), ("dmma", 2), ("dmma", 3), ("dmma", 4)])
@@ -424,19 +459,22 @@ def test_dmma_layouts_and_alignment(S, transa, transb, aligned):
 
 
 # ------------------------------------------------------------------------- plain fp32 (cp.async)
-@pytest.mark.parametrize("cfg", [3, 4, 5])
+@pytest.mark.parametrize("cfg", [3, 4, 5, 6, 7, 8, 9, 10, 11])
 @pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("aligned", [True, False])
 def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
     """Plain fp32 on the cp.async-pipelined kernels (configuration 3: 64 x 64 tiles, 4: 128 x 128,
-    5: persistent 64 x 64 CTAs that double-buffer their (tile, instance) items, for k <= 64 -- run
-    with 300 instances, so every CTA walks several items) for every op(A)/op(B) pair, with 16-byte
-    aligned instances and leading dimensions that are multiples of 4 (16-byte copies) or instances
-    at odd 4-byte offsets with odd leading dimensions (4-byte copies), ragged edges in m, n and k,
-    beta != 0."""
+    7: 32 x 64, 8: 32 x 32; 5 and 6: persistent 64 x 64 CTAs that double-buffer their (tile,
+    instance) items, for k <= 64 -- run with 300 instances, so every CTA walks several items; 9
+    and 10: 64-thread CTAs of 8 x 8 blocks holding all of k <= 64 / k <= 128; 11: four such
+    groups over quarters of k <= 128, summed in shared memory) for every
+    op(A)/op(B) pair, with 16-byte aligned instances and leading dimensions that are multiples of
+    4 (16-byte copies) or instances at odd 4-byte offsets with odd leading dimensions (4-byte
+    copies), ragged edges in m, n and k, beta != 0."""
     import torch
     from ssblasex_b200 import workloads as W
-    m, n, k, batch = (141, 77, 203, 3) if cfg != 5 else (141, 77, 61, 300)
+    m, n, k, batch = {5: (141, 77, 61, 300), 6: (141, 77, 61, 300), 9: (141, 77, 61, 300),
+                      10: (141, 77, 127, 40), 11: (141, 77, 126, 40)}.get(cfg, (141, 77, 203, 3))
     arows, brows = (m if transa == 0 else k), (k if transb == 0 else n)
     pad = 0 if aligned else 1
     lda, ldb, ldc = arows + (3 if aligned else 2), brows + (1 if aligned else 2), m + (3 if aligned else 2)

@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 6 : MODE == 0 ? 6 : 8) gprep_
         double xd[4] = {x[0], x[1], x[2], x[3]};
         if (rscale[r][0] == 0.0) xd[0] = xd[1] = xd[2] = xd[3] = 0.0;
         uint32_t wd[S];
-        digit_words<S>(xd, rscale[r][0], rscale[r][1], wd);
+        digit_words_rs<S>(xd, rscale[r][0], rscale[r][1], wd);
 #pragma unroll
         for (int p = 0; p < P; ++p) *(uint32_t*)(row + p * GRT * PB) = wd[p];
       }

@@ -64,14 +64,23 @@ static __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
 static __device__ __forceinline__ double pow2(int h) {
   return __longlong_as_double((long long)(h + 1023) << 52);
 }
-// the two power-of-two factors of 2^(8S-2-e) (0 for a non-finite row: its digits are zero);
-// with e in [-1073, 1024] both halves of the shift stay inside the normal range
+// the two power-of-two factors of 2^(8S-2-e) (0 for a non-finite row: its digits are zero):
+// s0 = 2^(8S-2-e) and s1 = 1 when that is a normal double (every row whose largest magnitude is
+// above 2^-960), else the shift split in halves, which with e in [-1073, 1024] both stay inside
+// the normal range. x * s0 * s1 is the exact product x * 2^(8S-2-e) (or that product rounded
+// once, when it is below the normal range and so rounds to zero digits) either way, so the
+// digits do not depend on the split; with s1 = 1 the second multiplication can be skipped.
 static __device__ __forceinline__ void row_scale(int S, int e, double& s0, double& s1) {
   if (e == kNonFiniteExp) {
     s0 = s1 = 0.0;
     return;
   }
   const int sh = 8 * S - 2 - e;
+  if (sh >= -1022 && sh <= 1023) {
+    s0 = pow2(sh);
+    s1 = 1.0;
+    return;
+  }
   const int h1 = sh / 2;
   s0 = pow2(h1);
   s1 = pow2(sh - h1);
@@ -98,9 +107,10 @@ static __device__ __forceinline__ void byte_transpose4(const uint32_t (&w)[4], u
 //   t2 = v2 + 1.5*2^52               the low word of t2 is rint(v2) (|v2| < 2^51)
 // rint(v) = v1 + rint(v2) (v1 is an even integer), so
 //   Y = (bits(a) << 11) + rint(v2) + bias - (bits(1.5*2^63) << 11)   (mod 2^64).
+template <bool ONE = false>
 static __device__ __forceinline__ unsigned long long slice_y(double x, double s0, double s1, unsigned long long bias) {
   const double C1 = 0x1.8p63, M = 0x1.8p52;
-  const double v = __dmul_rn(__dmul_rn(x, s0), s1);
+  const double v = ONE ? __dmul_rn(x, s0) : __dmul_rn(__dmul_rn(x, s0), s1);   // ONE: s1 == 1
   const double a = __dadd_rn(v, C1);
   const double v2 = __dsub_rn(v, __dsub_rn(a, C1));
   const int32_t r2 = (int32_t)__double2loint(__dadd_rn(v2, M));
@@ -109,8 +119,9 @@ static __device__ __forceinline__ unsigned long long slice_y(double x, double s0
 }
 
 // Digit words of 4 consecutive-k values of one row: word p holds digit p of the 4 values (the
-// value with the lowest k in the lowest byte). s0 * s1 = 2^(8S-2-e).
-template <int S>
+// value with the lowest k in the lowest byte). s0 * s1 = 2^(8S-2-e); ONE: s1 == 1 (one
+// multiplication per value instead of two; digit_words_rs picks the form for a row).
+template <int S, bool ONE = false>
 static __device__ __forceinline__ void digit_words(const double (&x)[4], double s0, double s1, uint32_t (&wd)[S]) {
   unsigned long long bias = 0;
 #pragma unroll
@@ -118,7 +129,7 @@ static __device__ __forceinline__ void digit_words(const double (&x)[4], double 
   uint32_t lo[4], hi[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const unsigned long long Y = slice_y(x[i], s0, s1, bias);
+    const unsigned long long Y = slice_y<ONE>(x[i], s0, s1, bias);
     lo[i] = (uint32_t)Y;
     hi[i] = (uint32_t)(Y >> 32);
   }
@@ -131,6 +142,12 @@ static __device__ __forceinline__ void digit_words(const double (&x)[4], double 
     const uint32_t w = byte < 4 ? L[byte] : H[byte - 4];
     wd[p] = p > 0 ? (w ^ 0x80808080u) : w;
   }
+}
+
+template <int S>
+static __device__ __forceinline__ void digit_words_rs(const double (&x)[4], double s0, double s1, uint32_t (&wd)[S]) {
+  if (s1 == 1.0) digit_words<S, true>(x, s0, s1, wd);
+  else digit_words<S, false>(x, s0, s1, wd);
 }
 
 }  // namespace ssb

@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
   for (int g = 0; g < PER / 4; ++g) {
     uint32_t wd[S];
     const double x[4] = {v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]};
-    digit_words<S>(x, s0, s1, wd);
+    digit_words_rs<S>(x, s0, s1, wd);
     const int kk = kk_of(4 * g);
 #pragma unroll
     for (int p = 0; p < S; ++p) *(uint32_t*)(st + (p * RT + r) * OPITCH + kk) = wd[p];
@@ -903,7 +903,7 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     for (int j = 0; j < RUNS; ++j) {
       uint32_t wd[S];
       const double x[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
-      digit_words<S>(x, s0, s1, wd);
+      digit_words_rs<S>(x, s0, s1, wd);
 #pragma unroll
       for (int p = 0; p < S; ++p) st[(p * R + r) * PW + c + NC * j] = wd[p];
     }

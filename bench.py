@@ -145,7 +145,7 @@ def peaks():
 #   (153 MB) and scaled by the instances it processes.
 #   imma_pipe: sm__pipe_tensor_cycles_active share of the int8 (imma) tensor pipe in that capture;
 #   it reads below `frac` because the int8 peak used for `frac` is derived (2 x measured bf16).
-NCU = {("f64_batch32_1024", "ozaki"): {"traffic": 153.1e6 * 4, "imma_pipe_frac": 0.676,
+NCU = {("f64_batch32_1024", "ozaki"): {"traffic": 153.1e6 * 4, "imma_pipe_frac": 0.685,
                                        "profile": "profiles/ozaki_gemm_f64_batch8_1024_full.md"}}
 
 

@@ -551,6 +551,10 @@ __global__ void __launch_bounds__(NTH) ozaki_digits_kernel(PlaneArgs a0, int32_t
 //   k contiguous (element (r, k) at X[r*ld + k]): r = t / NC, c = t % NC; the tile is staged
 //     [k / 256][R rows][256 k] (one TMA box per 256 k).
 constexpr int CL_NTH = 512;
+// Row-exponent reduction of the clusters-of-one path: a thread whose values are all zero takes
+// kRowZeroKey (below every exponent); with rows spread over several warps, the row maxima meet in
+// 64 words past the reduction buffer's [W][32] doubles (32 per parity of the item counter)
+constexpr int kRowZeroKey = -0x40000000;
 
 template <int R, int KC, int NTH, int RUNS = 4>
 struct ClShape {
@@ -564,7 +568,9 @@ struct ClShape {
   static_assert(TILE / NTH == 4 * RUNS && TILE % NTH == 0, "tile shape");
   static_assert(W % RG == 0 && (32 / LR) * NW == NC && NTH % NC == 0, "thread mapping");
   template <int S>
-  static constexpr int smem_bytes() { return 2 * TILE * 8 + S * R * PW * 4 + W * 32 * 8 + 2 * R * 8 + R * 16 + 16; }
+  static constexpr int smem_bytes() {
+    return 2 * TILE * 8 + S * R * PW * 4 + (W * 32 + 32) * 8 + 2 * R * 8 + R * 16 + 16;
+  }
   // position of element (r, k) of a tile staged with K contiguous
   static __device__ __forceinline__ int kc_index(int r, int k) { return (k / 256) * R * 256 + r * 256 + (k % 256); }
 };
@@ -689,8 +695,9 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
   extern __shared__ __align__(16) uint8_t dyn[];
   double* stages = (double*)dyn;                                                   // [2][TILE]
   uint32_t* st = (uint32_t*)(dyn + 2 * TILE * 8);                                  // [S][R][PW]
-  double* red = (double*)(dyn + 2 * TILE * 8 + S * R * PW * 4);                    // [W][32]
-  double* pmax = red + Sh::W * 32;                                                    // [2][R]
+  double* red = (double*)(dyn + 2 * TILE * 8 + S * R * PW * 4);                    // [W][32] + 32
+  double* pmax = red + Sh::W * 32 + 32;                                               // [2][R]
+  constexpr int kRowMaxWords = Sh::W * 64;   // int words of red past the [W][32] doubles
   double* rscale = pmax + 2 * R;                                                   // [R][2]
   uint64_t* full = (uint64_t*)(rscale + 2 * R);                                    // [2] (TMA)
 
@@ -717,6 +724,8 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
     ptx::mbar_init(ptx::smem_u32(&full[1]), 1);
     ptx::fence_mbar_init();
   }
+  // per-row maximum words of the clusters-of-one path (rows not contiguous in K), two parities
+  if (t < 64) ((int*)red)[kRowMaxWords + t] = kRowZeroKey;
   __syncthreads();
   // under a programmatic launch the set-up above overlaps the end of the kernel before; the
   // operands, planes and exponents are touched only after it has completed
@@ -795,7 +804,7 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
       // threads' exponents: 32-bit reductions instead of 64-bit keys. A thread whose values are
       // all zero (the fill past k, or zeros) takes a sentinel below every exponent (-1073 is the
       // smallest), and a row that is zero throughout gets 0 back.
-      constexpr int kZeroKey = -0x40000000;
+      constexpr int kZeroKey = kRowZeroKey;
       const unsigned long long key = row_key(v);
       int e = key ? row_exponent(key) : kZeroKey;
       int* const redi = (int*)red;
@@ -809,18 +818,21 @@ __global__ void __launch_bounds__(NTH, RUNS == 4 ? CL_NTH / NTH : 6) ozaki_clust
         for (int off = 1; off < 32; off <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, off));
         if (lane == 0) redi[warp] = e;
       } else {
+        // rows spread over NW warps: each warp's maxima meet in one word per row by a shared-
+        // memory atomicMax (the words of this item's parity; the other parity's are reset below
+        // for the next item), so every thread then reads one word instead of NW
 #pragma unroll
         for (int off = LR; off < 32; off <<= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, off));
-        if (lane < LR) redi[(warp / RG) * 32 + r] = e;
+        if (lane < LR) atomicMax(&redi[kRowMaxWords + (int)(iter & 1) * 32 + r], e);
       }
       __syncthreads();   // red visible; stage s fully read; the previous item's st reads done
       if (a.kcontig && NC > 32) {
         e = redi[r * (NC / 32)];
         for (int w = 1; w < NC / 32; ++w) e = max(e, redi[r * (NC / 32) + w]);
       } else if (!a.kcontig) {
-        e = redi[r];
-#pragma unroll
-        for (int w = 1; w < NW; ++w) e = max(e, redi[w * 32 + r]);
+        e = redi[kRowMaxWords + (int)(iter & 1) * 32 + r];
+        // the other parity was last read in the previous item, before its second barrier
+        if (t < R) redi[kRowMaxWords + (int)((iter + 1) & 1) * 32 + t] = kZeroKey;
       }
       if (e == kZeroKey) e = 0;
       if (c == 0 && ci.row0 + r < a.rows) exps[ci.b * a.rows + ci.row0 + r] = e;

@@ -76,16 +76,16 @@ __device__ __forceinline__ uint32_t swz(uint32_t line, uint32_t g) {
 
 // hi = bf16(x), lo = bf16(x - hi) of 4 fp32 values, packed 2 per word
 __device__ __forceinline__ void split4(const float4 x, uint2& hi, uint2& lo) {
-  const __nv_bfloat16 h0 = __float2bfloat16_rn(x.x), h1 = __float2bfloat16_rn(x.y);
-  const __nv_bfloat16 h2 = __float2bfloat16_rn(x.z), h3 = __float2bfloat16_rn(x.w);
-  const __nv_bfloat16 l0 = __float2bfloat16_rn(x.x - __bfloat162float(h0));
-  const __nv_bfloat16 l1 = __float2bfloat16_rn(x.y - __bfloat162float(h1));
-  const __nv_bfloat16 l2 = __float2bfloat16_rn(x.z - __bfloat162float(h2));
-  const __nv_bfloat16 l3 = __float2bfloat16_rn(x.w - __bfloat162float(h3));
-  hi.x = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-  hi.y = (uint32_t)__bfloat16_as_ushort(h2) | ((uint32_t)__bfloat16_as_ushort(h3) << 16);
-  lo.x = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-  lo.y = (uint32_t)__bfloat16_as_ushort(l2) | ((uint32_t)__bfloat16_as_ushort(l3) << 16);
+  // paired conversions (one instruction per two values, each rounded to nearest even as a
+  // single conversion would be); bf16 -> fp32 is exact, so x - float(hi) is the split's residue
+  const __nv_bfloat162 h01 = __floats2bfloat162_rn(x.x, x.y), h23 = __floats2bfloat162_rn(x.z, x.w);
+  const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+  const __nv_bfloat162 l01 = __floats2bfloat162_rn(x.x - f01.x, x.y - f01.y);
+  const __nv_bfloat162 l23 = __floats2bfloat162_rn(x.z - f23.x, x.w - f23.y);
+  hi.x = *(const uint32_t*)&h01;
+  hi.y = *(const uint32_t*)&h23;
+  lo.x = *(const uint32_t*)&l01;
+  lo.y = *(const uint32_t*)&l23;
 }
 
 // One operand's fp32 chunk of ROWS x 64 k -> its hi / lo planes. K contiguous: the chunk is

@@ -13,12 +13,12 @@
 //   warp 0     TMA: each 64-wide K chunk of op(A) and op(B), as it lies in memory (K or M/N
 //              contiguous), into an fp32 stage (F32S stages); a second lane brings each item's C
 //              tile (beta != 0) into its own ring
-//   warps 2-5  converters: fp32 stage -> BF16 hi and lo planes in the 128-byte-swizzled layout the
+//   warps 2-9  converters: fp32 stage -> BF16 hi and lo planes in the 128-byte-swizzled layout the
 //              tensor core reads (K-major for an operand whose K is contiguous in memory, MN-major
 //              otherwise, so every thread reads 16 contiguous bytes and writes 8 + 8), BFS stages
 //   warp 1     MMA: 4 K steps x 3 products per chunk into a tensor-memory accumulator of
 //              128 lanes x NB columns, two accumulators alternating between items
-//   warps 6-9  epilogue: a lane per row combines alpha * acc + beta * C over the item's C tile
+//   warps 10-13 epilogue: a lane per row combines alpha * acc + beta * C over the item's C tile
 //              (brought in by TMA while the products run) and one bulk tensor store writes it;
 //              where C is not addressable by a tensor map the lanes read and write C themselves
 // Rows past m of the A planes and columns past n of the B planes hold zeros (TMA fill) or are
@@ -37,7 +37,9 @@ namespace ssb {
 namespace {
 
 constexpr int kKC = 64;          // K elements per chunk (one 128-byte swizzle span of bf16)
-constexpr int kFusedThreads = 320;
+constexpr int kConvWarps = 8;                  // converter warps (warps 2 .. 2 + kConvWarps - 1)
+constexpr int kEpiWarp0 = 2 + kConvWarps;      // first of the 4 epilogue warps
+constexpr int kFusedThreads = 32 * (kEpiWarp0 + 4);
 
 // MB, NB: the instance's row / column extent rounded up to 64 or 128; F32S, BFS: stage counts;
 // CST: stages of C tiles (beta != 0), 0 = the epilogue reads C itself
@@ -91,14 +93,15 @@ __device__ __forceinline__ void split4(const float4 x, uint2& hi, uint2& lo) {
 // One operand's fp32 chunk of ROWS x 64 k -> its hi / lo planes. K contiguous: the chunk is
 // [ROWS][64 k] and the planes K-major (a line = one row's 64 k); otherwise the chunk is
 // [64 k][ROWS] and the planes MN-major (a line = 64 rows at one k, blocks of 64 rows 8 KB apart).
-// Unit = 4 consecutive fp32 values; the 128 converter threads take consecutive units, so a warp
+// Unit = 4 consecutive fp32 values; the 256 converter threads take consecutive units, so a warp
 // reads 512 contiguous bytes and writes whole lines.
 template <int ROWS>
 __device__ __forceinline__ void convert(const float* __restrict__ src, uint8_t* hi, uint8_t* lo, bool kcontig, int ct) {
+  constexpr int CT = 32 * kConvWarps;
   constexpr int UNITS = ROWS * kKC / 4;
-  static_assert(UNITS % 128 == 0, "converter shape");
+  static_assert(UNITS % CT == 0, "converter shape");
 #pragma unroll 4
-  for (int u = ct; u < UNITS; u += 128) {
+  for (int u = ct; u < UNITS; u += CT) {
     const float4 x = *(const float4*)(src + 4 * u);
     uint2 h, l;
     split4(x, h, l);
@@ -149,8 +152,8 @@ bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   uint8_t* cst = bf + F::BFS * F::BF_STAGE;                   // [CST][C_STAGE]
   uint64_t* bars = (uint64_t*)(cst + F::CST * F::C_STAGE);
   uint64_t* f_full = bars;                                    // fp32 chunk landed (TMA bytes)
-  uint64_t* f_empty = f_full + F::F32S;                       // fp32 chunk converted (4 warps)
-  uint64_t* b_full = f_empty + F::F32S;                       // planes written (4 warps)
+  uint64_t* f_empty = f_full + F::F32S;                       // fp32 chunk converted (converter warps)
+  uint64_t* b_full = f_empty + F::F32S;                       // planes written (converter warps)
   uint64_t* b_empty = b_full + F::BFS;                        // planes read by the MMAs (commit)
   uint64_t* acc_full = b_empty + F::BFS;                      // [2] accumulator complete (commit)
   uint64_t* acc_empty = acc_full + 2;                         // [2] accumulator drained (4 warps)
@@ -167,10 +170,10 @@ bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
   if (threadIdx.x == 0) {
     for (int s = 0; s < F::F32S; ++s) {
       ptx::mbar_init(ptx::smem_u32(&f_full[s]), 1);
-      ptx::mbar_init(ptx::smem_u32(&f_empty[s]), 4);
+      ptx::mbar_init(ptx::smem_u32(&f_empty[s]), kConvWarps);
     }
     for (int t = 0; t < F::BFS; ++t) {
-      ptx::mbar_init(ptx::smem_u32(&b_full[t]), 4);
+      ptx::mbar_init(ptx::smem_u32(&b_full[t]), kConvWarps);
       ptx::mbar_init(ptx::smem_u32(&b_empty[t]), 1);
     }
     for (int q = 0; q < 2; ++q) {
@@ -286,7 +289,7 @@ bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
       ptx::mma_commit(ptx::smem_u32(drain));
       ptx::mbar_wait(ptx::smem_u32(drain), 0, err, 65, wl);
     }
-  } else if (warp < 6) {
+  } else if (warp < kEpiWarp0) {
     // ------------------------------------------------------------------ converters --------
     const int ct = threadIdx.x - 64;
     long c = 0;
@@ -358,7 +361,7 @@ bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
           if (lane == 0) ptx::mbar_arrive(ptx::smem_u32(&acc_empty[acc]));
           ptx::fence_proxy_async_smem();   // the tile's generic writes -> the bulk store
           asm volatile("bar.sync 1, 128;" ::: "memory");
-          if (warp == 6 && lane == 0) {
+          if (warp == kEpiWarp0 && lane == 0) {
             ptx::tma_store_3d(&tmC, ptx::smem_u32(tile), 0, 0, (int)b);
             ptx::bulk_commit();
             ptx::bulk_wait_read();         // the store has read the tile: it may be refilled
@@ -366,7 +369,7 @@ bf16x3_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
           }
           asm volatile("bar.sync 1, 128;" ::: "memory");
         }
-        if (warp == 6 && lane == 0) ptx::bulk_wait_all();
+        if (warp == kEpiWarp0 && lane == 0) ptx::bulk_wait_all();
       }
     } else {
       // C read and written by the epilogue threads (C not addressable by a tensor map, or tiles

@@ -232,15 +232,11 @@ __global__ void __launch_bounds__(GNT, MODE == 2 ? 6 : MODE == 0 ? 6 : 8) gprep_
         for (int i = 0; i < 4; ++i) w |= ((uint32_t)(uint8_t)x[i]) << (8 * i);
         *(uint32_t*)row = w;
       } else if constexpr (MODE == 1) {
-        __nv_bfloat16 h[4], l[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          h[i] = __float2bfloat16_rn(x[i]);
-          l[i] = __float2bfloat16_rn(x[i] - __bfloat162float(h[i]));
-        }
-        __nv_bfloat162 h01, h23, l01, l23;
-        h01.x = h[0]; h01.y = h[1]; h23.x = h[2]; h23.y = h[3];
-        l01.x = l[0]; l01.y = l[1]; l23.x = l[2]; l23.y = l[3];
+        // paired conversions, each value rounded to nearest even as a single conversion would be
+        const __nv_bfloat162 h01 = __floats2bfloat162_rn(x[0], x[1]), h23 = __floats2bfloat162_rn(x[2], x[3]);
+        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+        const __nv_bfloat162 l01 = __floats2bfloat162_rn(x[0] - f01.x, x[1] - f01.y);
+        const __nv_bfloat162 l23 = __floats2bfloat162_rn(x[2] - f23.x, x[3] - f23.y);
         *(__nv_bfloat162*)row = h01;
         *(__nv_bfloat162*)(row + 4) = h23;
         *(__nv_bfloat162*)(row + GRT * PB) = l01;

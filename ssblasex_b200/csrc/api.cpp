@@ -32,10 +32,24 @@ Settings& settings() {
       if (v.find("BF16X3") != std::string::npos) mode |= SSBLAS_MATH_FP32_BF16X3;
       t.math_mode = mode;
     }
+    // SSBLAS_OZAKI_SLICES: forced slice count (3..8); SSBLAS_OZAKI_TOLERANCE: the bound's target
+    // (a positive number, e.g. 1e-15); both as ssblasSetOzakiSlices / ssblasSetOzakiTolerance
+    if (const char* e = getenv("SSBLAS_OZAKI_SLICES")) {
+      const int v = atoi(e);
+      if (v >= 3 && v <= 8) t.ozaki_slices = v;
+    }
+    if (const char* e = getenv("SSBLAS_OZAKI_TOLERANCE")) {
+      const double v = strtod(e, nullptr);
+      if (v > 0.0) t.ozaki_tolerance = v;
+    }
+    t.log = getenv("SSBLAS_LOG") != nullptr;
     return t;
   }();
   return s;
 }
+
+// SSBLAS_LOG: the kernel choice of each call, after it returns
+static void log_call(const char* entry, ssblasStatus_t st, long m, long n, long k, long batch);
 
 static std::mutex g_mutex;
 static ssblasRunInfo_t g_info;
@@ -790,6 +804,15 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
   return SSBLAS_STATUS_SUCCESS;
 }
 
+static void log_call(const char* entry, ssblasStatus_t st, long m, long n, long k, long batch) {
+  static const char* const names[] = {"none", "simt", "i8_tcgen05", "ozaki_tcgen05", "bf16x3_tcgen05", "grouped",
+                                      "dmma", "", "", "", "", "f16_tcgen05"};
+  const int p = g_info.path;
+  fprintf(stderr, "ssblas: %s m=%ld n=%ld k=%ld batch=%ld status=%d path=%s slices=%d launches=%d split_k=%d%s\n",
+          entry, m, n, k, batch, (int)st, (p >= 0 && p < 12 && names[p][0]) ? names[p] : "?", g_info.slices,
+          g_info.kernel_launches, g_info.split_k, g_info.device_error ? " device_error" : "");
+}
+
 }  // namespace ssb
 
 using namespace ssb;
@@ -803,8 +826,10 @@ ssblasStatus_t ssblasGemmBatchedEx(ssblasOperation_t transa, ssblasOperation_t t
                                    void* const C[], ssblasDataType_t Ctype, const SSINT ldc,
                                    const SSINT batchCount, ssblasComputeType_t computeType,
                                    ssblasGemmAlgo_t algo) {
-  return gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta, C, Ctype,
-                      ldc, batchCount, computeType, algo);
+  const ssblasStatus_t st = gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta,
+                                          C, Ctype, ldc, batchCount, computeType, algo);
+  if (ssb::settings().log) ssb::log_call("ssblasGemmBatchedEx", st, m, n, k, batchCount);
+  return st;
 }
 
 ssblasStatus_t ssblasGemmBatchedEx_64(ssblasOperation_t transa, ssblasOperation_t transb,
@@ -815,8 +840,10 @@ ssblasStatus_t ssblasGemmBatchedEx_64(ssblasOperation_t transa, ssblasOperation_
                                       void* const C[], ssblasDataType_t Ctype, const SSLONG ldc,
                                       const SSLONG batchCount, ssblasComputeType_t computeType,
                                       ssblasGemmAlgo_t algo) {
-  return gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta, C, Ctype,
-                      ldc, batchCount, computeType, algo);
+  const ssblasStatus_t st = gemm_batched(transa, transb, m, n, k, alpha, A, Atype, lda, B, Btype, ldb, beta,
+                                          C, Ctype, ldc, batchCount, computeType, algo);
+  if (ssb::settings().log) ssb::log_call("ssblasGemmBatchedEx_64", st, m, n, k, batchCount);
+  return st;
 }
 
 // Grouped batched GEMM. Validation follows the batched call for each group; groups run in order

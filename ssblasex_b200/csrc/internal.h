@@ -54,6 +54,7 @@ struct Settings {
   double ozaki_tolerance = 0;  // 0 = kOzakiDefaultTolerance
   int fault = 0;               // one-shot ssblasFault_t armed by ssblasSetFaultInjection
   int extensions = 0;          // ssblasExtension_t flags (ssblasSetExtensions)
+  bool log = false;            // SSBLAS_LOG: one line per call on stderr (path, slices, launches)
 };
 Settings& settings();
 

@@ -193,3 +193,38 @@ def test_extension_flags_and_their_status_rules():
         assert runner.call(p, mode="host_matrices", transb=2)[0] == S.SSBLAS_STATUS_INVALID_VALUE
     finally:
         S.set_extensions(0)
+
+
+def _run_with_env(code, **env):
+    import os
+    import subprocess
+    import sys
+    e = dict(os.environ)
+    e.update(env)
+    e["PYTHONPATH"] = str(ROOT) + os.pathsep + e.get("PYTHONPATH", "")
+    r = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+def test_environment_knobs():
+    """SSBLAS_OZAKI_SLICES / SSBLAS_OZAKI_TOLERANCE set the slice choice of a process (as the
+    setters do; out-of-range values are ignored), and SSBLAS_LOG prints one line per call on
+    stderr with the status -- here of calls refused before any device work."""
+    code = "import ssblasex_b200 as S; print(S.get_ozaki_slices())"
+    assert _run_with_env(code).stdout.strip() == "7"
+    assert _run_with_env(code, SSBLAS_OZAKI_SLICES="5").stdout.strip() == "5"
+    assert _run_with_env(code, SSBLAS_OZAKI_SLICES="12").stdout.strip() == "7"
+    assert _run_with_env(code, SSBLAS_OZAKI_TOLERANCE="1e-6").stdout.strip() == "3"
+    assert _run_with_env(code, SSBLAS_OZAKI_TOLERANCE="0x1p-56").stdout.strip() == "8"
+    call = ("import ssblasex_b200 as S\n"
+            "st = S.lib().ssblasGemmBatchedEx(0, 0, 0, 4, 4, None, None, S.SSBLAS_R_32F, 4, None, S.SSBLAS_R_32F, 4,"
+            " None, None, S.SSBLAS_R_32F, 4, 1, 0, 0)\n"
+            "print(st)\n")
+    r = _run_with_env(call, SSBLAS_LOG="1")
+    assert r.stdout.strip() == str(S_INTERNAL_ERROR)
+    assert "ssblas: ssblasGemmBatchedEx m=0 n=4 k=4 batch=1 status=3" in r.stderr
+    assert "ssblas:" not in _run_with_env(call).stderr
+
+
+S_INTERNAL_ERROR = 3

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "grouped.h"
+#include "hostcopy.h"
 #include "internal.h"
 
 namespace ssb {
@@ -356,18 +357,33 @@ static ssblasStatus_t map_err(cudaError_t e) {
 
 // Stages the instances of one host-resident operand into device memory. Returns the device
 // pointers in dptr (host vector). copy_in=false allocates without copying.
+// Pageable (not page-locked) host memory: copied through the pinned staging of hostcopy.cpp
+// rather than by the driver's bounce-buffered copies.
+static bool is_pageable(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered;
+}
+constexpr size_t kStagedCopyMin = (size_t)4 << 20;   // below this, plain per-instance copies
+
 static cudaError_t stage_operand(WsSlot slot, const void* const* hptr, long batch, size_t inst_bytes,
                                  bool copy_in, cudaStream_t st, std::vector<void*>& dptr,
                                  long* dev_stride) {
   long s = uniform_stride(hptr, batch);
   dptr.resize(batch);
   cudaError_t e;
+  const bool staged = copy_in && inst_bytes * (size_t)batch >= kStagedCopyMin && is_pageable(hptr[0]);
   // one copy of the whole span when the instances are equally spaced and densely packed
   if (batch == 1 || (s > 0 && (size_t)s >= inst_bytes && (size_t)s <= 2 * inst_bytes + 4096)) {
     size_t span = (batch == 1) ? inst_bytes : (size_t)s * (batch - 1) + inst_bytes;
     char* d = (char*)workspace(slot, span, &e);
     if (!d) return e;
-    if (copy_in) {
+    if (staged && batch > 1) {
+      if ((e = gather_to_device(d, (size_t)s, hptr, batch, inst_bytes, st)) != cudaSuccess) return e;
+    } else if (copy_in) {
       e = cudaMemcpyAsync(d, hptr[0], span, cudaMemcpyHostToDevice, st);
       if (e != cudaSuccess) return e;
     }
@@ -378,6 +394,12 @@ static cudaError_t stage_operand(WsSlot slot, const void* const* hptr, long batc
   size_t pitch = (inst_bytes + 255) & ~(size_t)255;
   char* d = (char*)workspace(slot, pitch * batch, &e);
   if (!d) return e;
+  if (staged) {
+    // scattered pageable instances: packed by host threads into pinned slots, one DMA per slot
+    for (long b = 0; b < batch; ++b) dptr[b] = d + pitch * b;
+    *dev_stride = (long)pitch;
+    return gather_to_device(d, pitch, hptr, batch, inst_bytes, st);
+  }
   for (long b = 0; b < batch; ++b) {
     dptr[b] = d + pitch * b;
     if (copy_in) {
@@ -787,7 +809,13 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
   if (host_matrices) {
     // copy back only the m x n part of each C (the ld padding of the caller stays untouched)
     long hs = uniform_stride((const void* const*)C, batchCount);
-    if (batchCount > 1 && hs == (long)(ldc * n * ec) && (char*)staged_c[1] - (char*)staged_c[0] == hs) {
+    const long dstride = batchCount > 1 ? (long)((char*)staged_c[1] - (char*)staged_c[0]) : 0;
+    if (batchCount > 1 && (size_t)(ldc * n * ec) * batchCount >= kStagedCopyMin && is_pageable(hc[0]) &&
+        uniform_stride((const void* const*)staged_c.data(), batchCount) == dstride) {
+      // pageable destinations: through the pinned staging, unpacked by host threads
+      e = scatter_to_host(hc.data(), (size_t)(ldc * ec), (const char*)staged_c[0], (size_t)dstride, batchCount,
+                          (size_t)(m * ec), n, st);
+    } else if (batchCount > 1 && hs == (long)(ldc * n * ec) && (char*)staged_c[1] - (char*)staged_c[0] == hs) {
       e = cudaMemcpy2DAsync(hc[0], ldc * ec, staged_c[0], ldc * ec, m * ec, (size_t)n * batchCount,
                             cudaMemcpyDeviceToHost, st);
     } else {

@@ -224,7 +224,11 @@ class Leg:
                                                 p.lda, self.Bh, tb, p.ldb, self.be.ctypes.data, self.Ch, tc,
                                                 p.ldc, p.batch, 0, 0)
 
-    def timed(self, math_mode, steps, warmup, profile=False, clk=None, barrier=None):
+    def timed(self, math_mode, steps, warmup, profile=False, clk=None, barrier=None, queued=False):
+        """CUDA-event time per step on the library stream. queued: a spin kernel (about 80 us per
+        step) goes on the stream first, so every call is enqueued before the GPU reaches it and the
+        events time the kernels back to back; otherwise a call whose host work outlasts its kernels
+        leaves the stream idle and the time per step is the host's."""
         import torch
         S = self.S
         S.set_math_mode(math_mode)
@@ -239,6 +243,8 @@ class Leg:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.time()
         with torch.cuda.stream(self.stream):
+            if queued:
+                torch.cuda._sleep(int(steps * 80e-6 * 2.0e9))
             e0.record(self.stream)
             for _ in range(steps):
                 st = self.call()
@@ -417,9 +423,15 @@ def secondary_legs(S, device: str, stream, pk: dict) -> dict:
     err = leg.error(S.SSBLAS_MATH_PLAIN, instances=range(p.batch), rows=range(p.m))
     ms, prof, info = leg.timed(S.SSBLAS_MATH_PLAIN, 50, 5, profile=True)
     name, kms, per = dominant(prof, 50)
+    # the same 50 calls enqueued behind a spin kernel: the device time of the kernels alone
+    qms, qprof, _ = leg.timed(S.SSBLAS_MATH_PLAIN, 50, 5, profile=True, queued=True)
+    _, qkms, _ = dominant(qprof, 50)
     out["fp32_batch64_128"] = {"ms_per_step": ms, "tflops": p.flops() / (ms * 1e-3) / 1e12,
                                "max_normalized_error": err, "path": info["path"], "kernel": name,
-                               "kernel_ms": kms, "hbm_bound_ms": p.algorithmic_bytes() / (pk["hbm_gbs"] * 1e9) * 1e3}
+                               "kernel_ms": kms, "hbm_bound_ms": p.algorithmic_bytes() / (pk["hbm_gbs"] * 1e9) * 1e3,
+                               "queued": {"ms_per_step": qms, "kernel_ms": qkms,
+                                          "note": "calls enqueued behind a spin kernel; kernel_ms is the "
+                                                  "kernel's device time with no host gap before it"}}
     del leg
     # grouped 10,000
     out["grouped_10000"] = grouped_leg(S, 10000, 5, 2, stream)

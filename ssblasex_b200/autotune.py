@@ -97,6 +97,9 @@ def time_kernel(p, dp, kernel, reps):
         assert call() == 0
     torch.cuda.synchronize()
     set_profiling(True)
+    # a spin kernel ahead of the calls keeps them all enqueued before the GPU starts them, so the
+    # per-launch events time kernels, not the host's per-call work between them
+    torch.cuda._sleep(int(reps * 80e-6 * 2.0e9))
     for _ in range(reps):
         assert call() == 0
     prof = get_profile()
@@ -122,6 +125,7 @@ def time_grouped(gd, reps):
         assert gd.call(device_arrays=True) == 0
     torch.cuda.synchronize()
     set_profiling(True)
+    torch.cuda._sleep(int(reps * 80e-6 * 2.0e9))
     for _ in range(reps):
         assert gd.call(device_arrays=True) == 0
     prof = get_profile()

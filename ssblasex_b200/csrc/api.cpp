@@ -585,7 +585,9 @@ static ssblasStatus_t grouped_device(
 // is split into chunks whose host->device copies, kernels and device->host copies run on three
 // streams, so the copies of one chunk overlap the computation and the copies of the others and
 // both PCIe directions are busy at once. Returns SSBLAS_STATUS_NOT_COMPUTED_ERROR when the layout
-// does not qualify (the caller then stages the whole batch at once).
+// does not qualify, or when the operands are pageable and large (the caller then stages the whole
+// batch at once, through pinned slots: 32 x 1024^3 FP64 from one pageable array took 70 ms through
+// this pipeline's pageable copies and 22 ms staged).
 static ssblasStatus_t run_host_pipelined(BatchDesc d, const void* const A[], const void* const B[],
                                          void* const C[], size_t a_bytes, size_t b_bytes, size_t c_bytes,
                                          size_t ec, cudaStream_t st) {
@@ -594,6 +596,10 @@ static ssblasStatus_t run_host_pipelined(BatchDesc d, const void* const A[], con
   const long sc = uniform_stride((const void* const*)C, batch);
   auto dense = [](long s, size_t bytes) { return s > 0 && (size_t)s >= bytes && (size_t)s <= 2 * bytes + 4096; };
   if (!dense(sa, a_bytes) || !dense(sb, b_bytes) || !dense(sc, c_bytes)) return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
+  // pageable operands: the driver bounces every chunk through its own staging on this thread;
+  // the pinned staging of hostcopy.cpp packs them with several threads instead
+  if (a_bytes * (size_t)batch >= kStagedCopyMin && (is_pageable(A[0]) || is_pageable(B[0])))
+    return SSBLAS_STATUS_NOT_COMPUTED_ERROR;
 
   constexpr int NCH = 16;  // chunks: copies of chunk c+1 overlap the GEMM of chunk c and the copy-back of c-1
   struct PipeStreams {

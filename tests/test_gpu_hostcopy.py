@@ -19,9 +19,12 @@ def S():
     S.set_math_mode(S.SSBLAS_MATH_PLAIN)
 
 
+@pytest.mark.parametrize("layout", ["scattered", "dense"])
 @pytest.mark.parametrize("row,mode,ta,tb,beta", [("f64", "ozaki", 0, 1, 0.0), ("f64", "plain", 1, 0, 0.5),
                                                  ("i8", "plain", 1, 0, 1), ("f32", "bf16x3", 0, 0, 0.25)])
-def test_scattered_pageable_instances(S, row, mode, ta, tb, beta):
+def test_scattered_pageable_instances(S, row, mode, ta, tb, beta, layout):
+    """scattered: one allocation per instance; dense: the instances are equally spaced views of one
+    pageable array (the layout the chunked pipeline would take if the memory were page-locked)."""
     from ssblasex_b200 import runner, workloads as W
     m, n, k, batch = 300, 260, 200, 20
     arows, brows = (m if ta == 0 else k), (k if tb == 0 else n)
@@ -35,7 +38,9 @@ def test_scattered_pageable_instances(S, row, mode, ta, tb, beta):
     A = [None] * batch
     B = [None] * batch
     C = [None] * batch
-    for b in reversed(range(batch)):
+    if layout == "dense":
+        A, B, C = list(np.array(p.A, copy=True)), list(np.array(p.B, copy=True)), list(np.array(p.C, copy=True))
+    for b in reversed(range(batch) if layout == "scattered" else []):
         A[b] = np.array(p.A[b], copy=True)
         B[b] = np.array(p.B[b], copy=True)
         C[b] = np.array(p.C[b], copy=True)

@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <iostream>
 #include <mutex>
@@ -194,11 +195,13 @@ void* workspace(WsSlot slot, size_t bytes, cudaError_t* err) {
   return w.ptr[slot];
 }
 
+static void release_pointer_arrays(int dev);
 static void release_workspace() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return;
-  if ((int)g_ws.size() <= dev) return;
   cudaDeviceSynchronize();
+  release_pointer_arrays(dev);
+  if ((int)g_ws.size() <= dev) return;
   for (int s = 0; s < WS_NUM; ++s) {
     if (g_ws[dev].ptr[s]) cudaFree(g_ws[dev].ptr[s]);
     g_ws[dev].ptr[s] = nullptr;
@@ -347,6 +350,115 @@ static void pinned_done(cudaStream_t st) {
   if (dev < 0) return;
   PinnedSlot& s = g_pins[dev][g_pin_cur[dev]];
   if (cudaEventRecord(s.done, st) == cudaSuccess) s.pending = true;
+}
+
+// Device copies of the pointer arrays of recent calls, per device, keyed by the pointer values.
+// A caller that repeats a layout (a loop over steps; the staging slots of host matrices) gets
+// the arrays it had before: no host->device copy on the stream and no wait for a pinned slot, so
+// the calls of a loop queue up behind one another. Since the key is the values, memory freed and
+// allocated again at the same addresses is harmless. An entry is rewritten only after the last
+// call that read it has finished (its `used` event), and a call on another stream than the
+// entry's last user first waits for that use, so `used` always covers every earlier use.
+struct PtrArrays {
+  std::vector<const void*> key;   // A[0..batch), B[0..batch), C[0..batch)
+  void** dev = nullptr;
+  size_t cap = 0;                 // pointers the device buffer holds
+  cudaEvent_t used = nullptr;
+  cudaStream_t last_stream = nullptr;
+  bool in_use = false;
+  unsigned long tick = 0;
+};
+constexpr int kPtrEntries = 4;
+static PtrArrays g_ptr_arrays[kMaxDevices][kPtrEntries];
+static unsigned long g_ptr_tick = 0;
+static PtrArrays* g_ptr_current = nullptr;   // entry of the call in progress
+
+static bool same_key(const PtrArrays& e, const std::vector<void*>& a, const std::vector<void*>& b,
+                     const std::vector<void*>& c) {
+  const size_t n = a.size();
+  if (e.key.size() != 3 * n) return false;
+  const void* const* k = e.key.data();
+  return memcmp(k, a.data(), n * sizeof(void*)) == 0 && memcmp(k + n, b.data(), n * sizeof(void*)) == 0 &&
+         memcmp(k + 2 * n, c.data(), n * sizeof(void*)) == 0;
+}
+
+static cudaError_t device_pointer_arrays(const std::vector<void*>& a, const std::vector<void*>& b,
+                                         const std::vector<void*>& c, cudaStream_t st, void*** out) {
+  const int dev = current_device();
+  if (!valid_device(dev)) return cudaErrorInvalidDevice;
+  const size_t n = a.size();
+  PtrArrays* hit = nullptr;
+  PtrArrays* victim = nullptr;
+  for (PtrArrays& e : g_ptr_arrays[dev]) {
+    if (same_key(e, a, b, c)) {
+      hit = &e;
+      break;
+    }
+    if (!victim || e.tick < victim->tick) victim = &e;
+  }
+  cudaError_t err;
+  if (hit) {
+    if (hit->in_use && hit->last_stream != st && (err = cudaStreamWaitEvent(st, hit->used, 0)) != cudaSuccess)
+      return err;
+  } else {
+    hit = victim;
+    if (hit->in_use) {
+      if ((err = cudaEventSynchronize(hit->used)) != cudaSuccess) return err;
+      hit->in_use = false;
+    }
+    hit->key.clear();   // no valid contents until the upload below is queued
+    if (!hit->used && (err = cudaEventCreateWithFlags(&hit->used, cudaEventDisableTiming)) != cudaSuccess)
+      return err;
+    if (hit->cap < 3 * n) {
+      if (hit->dev) cudaFree(hit->dev);
+      hit->dev = nullptr;
+      hit->cap = 0;
+      const size_t cap = std::max<size_t>(3 * n, 64);
+      if ((err = cudaMalloc((void**)&hit->dev, cap * sizeof(void*))) != cudaSuccess) {
+        cudaGetLastError();
+        return err;
+      }
+      hit->cap = cap;
+    }
+    void* h = pinned(3 * n * sizeof(void*), &err);
+    if (!h) return err;
+    void** hp = (void**)h;
+    memcpy(hp, a.data(), n * sizeof(void*));
+    memcpy(hp + n, b.data(), n * sizeof(void*));
+    memcpy(hp + 2 * n, c.data(), n * sizeof(void*));
+    if ((err = cudaMemcpyAsync(hit->dev, hp, 3 * n * sizeof(void*), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return err;
+    pinned_done(st);
+    hit->key.assign((const void* const*)hp, (const void* const*)hp + 3 * n);
+  }
+  hit->tick = ++g_ptr_tick;
+  g_ptr_current = hit;
+  *out = hit->dev;
+  return cudaSuccess;
+}
+
+// after the launches of the call that took its arrays from device_pointer_arrays
+static void pointer_arrays_used(cudaStream_t st) {
+  PtrArrays* e = g_ptr_current;
+  g_ptr_current = nullptr;
+  if (!e) return;
+  if (cudaEventRecord(e->used, st) == cudaSuccess) {
+    e->in_use = true;
+    e->last_stream = st;
+  } else {
+    cudaGetLastError();
+    e->key.clear();   // cannot tell when its readers finish: never reused, rewritten after a sync
+    cudaStreamSynchronize(st);
+  }
+}
+
+static void release_pointer_arrays(int dev) {
+  if (!valid_device(dev)) return;
+  for (PtrArrays& e : g_ptr_arrays[dev]) {
+    if (e.dev) cudaFree(e.dev);
+    if (e.used) cudaEventDestroy(e.used);
+    e = PtrArrays{};
+  }
 }
 
 static ssblasStatus_t map_err(cudaError_t e) {
@@ -789,18 +901,9 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
       if (batchCount == 1) { d.strideA = d.strideB = d.strideC = 0; }
     }
     d.A0 = da[0]; d.B0 = db[0]; d.C0 = dc[0];
-    // upload the three pointer arrays
-    void* h = pinned(3 * sizeof(void*) * batchCount, &e);
-    if (!h) return map_err(e);
-    void** hp = (void**)h;
-    memcpy(hp, da.data(), sizeof(void*) * batchCount);
-    memcpy(hp + batchCount, db.data(), sizeof(void*) * batchCount);
-    memcpy(hp + 2 * batchCount, dc.data(), sizeof(void*) * batchCount);
-    void** dp = (void**)workspace(WS_PTRS, 3 * sizeof(void*) * batchCount, &e);
-    if (!dp) return map_err(e);
-    if ((e = cudaMemcpyAsync(dp, hp, 3 * sizeof(void*) * batchCount, cudaMemcpyHostToDevice, st)))
-      return map_err(e);
-    pinned_done(st);
+    // the three pointer arrays on the device (uploaded unless a recent call had the same)
+    void** dp = nullptr;
+    if ((e = device_pointer_arrays(da, db, dc, st, &dp)) != cudaSuccess) return map_err(e);
     d.A = (const void* const*)dp;
     d.B = (const void* const*)(dp + batchCount);
     d.C = (void* const*)(dp + 2 * batchCount);
@@ -810,7 +913,9 @@ static ssblasStatus_t gemm_batched(ssblasOperation_t transa, ssblasOperation_t t
     }
   }
 
-  if ((e = dispatch(d, st)) != cudaSuccess) return map_err(e);
+  e = dispatch(d, st);
+  pointer_arrays_used(st);
+  if (e != cudaSuccess) return map_err(e);
 
   if (host_matrices) {
     // copy back only the m x n part of each C (the ld padding of the caller stays untouched)

@@ -66,7 +66,7 @@ FAMILIES = {
              lda=1032, ldb=1032, ldc=1032, dist="expspread"),
         dict(row="f64", transa=1, transb=0, m=128, n=128, k=128, batch=256, alpha=1.0, beta=0.5),
     ]),
-    "simt": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4, 5, 6, 7, 8, 9, 10, 11], "(all)", [
+    "simt": (SSBLAS_MATH_PLAIN, [0, 1, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13], "(all)", [
         dict(row="f32", transa=0, transb=0, m=128, n=128, k=128, batch=64, alpha=1.0, beta=0.5),
         dict(row="f32", transa=1, transb=1, m=64, n=64, k=64, batch=4096, alpha=0.75, beta=0.25,
              dist="outliers"),

@@ -634,8 +634,14 @@ cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t st) 
   a.beta = d.beta_f;
   const bool a_mn = d.transa == SSBLAS_OP_N;   // op(A) rows (m) contiguous
   const bool b_mn = d.transb == SSBLAS_OP_T;   // op(B) columns (n) contiguous
-  ProfScope prof("sgemm_async", st);
   cudaError_t e;
+  // 12 / 13: 64 x 64 tiles, TMA staging and bulk stores (equally spaced, 16-byte aligned
+  //   instances): two stages and two C tiles, two CTAs per SM / three and three, one CTA per SM
+  if (config == 12 || config == 13) {
+    e = launch_sgemm_tma(d, config - 12, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  ProfScope prof("sgemm_async", st);
   // 3: 64 x 64 tiles, 256 threads of 4 x 4, 32-deep K stages x 2 (k <= 64 entirely in flight)
   // 4: 128 x 128 tiles, 256 threads of 8 x 8, 16-deep K stages x 3
   // 5 (k <= 64): 64 x 64 tiles, persistent CTAs that double-buffer their work items, 256 threads

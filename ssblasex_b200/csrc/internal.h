@@ -99,6 +99,10 @@ int* device_error_flag();
 cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream);
 // plain fp32 with a cp.async pipeline (config 3: 64 x 64 tiles, 4: 128 x 128)
 cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t stream);
+// plain fp32 with TMA staging (gemm_sgemm_tma.cu); cudaErrorNotSupported unless the instances are
+// equally spaced with 16-byte-aligned bases, strides and leading dimensions
+bool sgemm_tma_fits(const BatchDesc& d);
+cudaError_t launch_sgemm_tma(const BatchDesc& d, int variant, cudaStream_t stream);
 // plain fp64 on the FP64 tensor cores (DMMA)
 cudaError_t launch_dmma_f64(const BatchDesc& d, cudaStream_t stream);
 // int8 -> int32 on tcgen05; returns cudaErrorNotSupported when the layout is not eligible.

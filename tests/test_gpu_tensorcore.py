@@ -459,7 +459,7 @@ def test_dmma_layouts_and_alignment(S, transa, transb, aligned):
 
 
 # ------------------------------------------------------------------------- plain fp32 (cp.async)
-@pytest.mark.parametrize("cfg", [3, 4, 5, 6, 7, 8, 9, 10, 11])
+@pytest.mark.parametrize("cfg", [3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13])
 @pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("aligned", [True, False])
 def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
@@ -467,7 +467,8 @@ def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
     7: 32 x 64, 8: 32 x 32; 5 and 6: persistent 64 x 64 CTAs that double-buffer their (tile,
     instance) items, for k <= 64 -- run with 300 instances, so every CTA walks several items; 9
     and 10: 64-thread CTAs of 8 x 8 blocks holding all of k <= 64 / k <= 128; 11: four such
-    groups over quarters of k <= 128, summed in shared memory) for every
+    groups over quarters of k <= 128, summed in shared memory; 12 and 13: TMA-staged 64 x 64
+    tiles, which the unaligned layouts leave for configuration 3) for every
     op(A)/op(B) pair, with 16-byte aligned instances and leading dimensions that are multiples of
     4 (16-byte copies) or instances at odd 4-byte offsets with odd leading dimensions (4-byte
     copies), ragged edges in m, n and k, beta != 0."""
@@ -503,6 +504,45 @@ def test_sgemm_layouts_and_alignment(S, cfg, transa, transb, aligned):
     C = np.stack([flat[pad + b * per: pad + b * per + p.C[0].size] for b in range(batch)]).reshape(p.C.shape)
     assert O.normalized_error(p, C) <= 4 * k * 2.0 ** -24
     np.testing.assert_array_equal(C.reshape(batch, n, ldc)[:, :, m:], p.C.reshape(batch, n, ldc)[:, :, m:])
+
+
+@pytest.mark.parametrize("cfg", [12, 13])
+@pytest.mark.parametrize("transa,transb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("shape", [(64, 64, 64, 300, 0.0), (64, 64, 64, 300, 0.5), (50, 70, 20, 97, 0.0),
+                                   (128, 128, 128, 64, 0.5), (200, 65, 257, 5, -1.0), (1, 1, 1, 3, 0.5),
+                                   (64, 64, 64, 2000, 0.25), (64, 64, 64, 2000, 0.0), (70, 40, 130, 700, 0.5)])
+def test_sgemm_tma_items(S, cfg, transa, transb, shape):
+    """The TMA-staged FFMA kernel (configurations 12 and 13), from one work item per CTA to about
+    seven and five per CTA (2000 and 700 instances: the stage and C-tile rings wrap several
+    times), with beta = 0 (C holds NaN and must not be read),
+    ragged m, n and k (zero-filled tiles, clipped stores), k below one 64-deep chunk, and several
+    chunks; the launch must be the TMA kernel, the result within 4 k u of the FP64-exact oracle,
+    and the ld padding of C untouched."""
+    import torch
+    from ssblasex_b200 import runner, workloads as W
+    m, n, k, batch, beta = shape
+    arows, brows = (m if transa == 0 else k), (k if transb == 0 else n)
+    r4 = lambda x: (x + 3) // 4 * 4
+    p = W.make_problem("f32", transa, transb, m, n, k, batch, 0.75, beta, lda=r4(arows + 1), ldb=r4(brows),
+                       ldc=r4(m + 2), seed=700 + 4 * cfg + 2 * transa + transb + m, dist="outliers")
+    C0 = p.C.copy()
+    if beta == 0.0:
+        C0.reshape(batch, n, -1)[:, :, :m] = np.nan
+    dp = runner.DeviceProblem(p, C=C0)
+    S.set_kernel_config("simt", cfg)
+    S.set_profiling(True)
+    try:
+        st, C = runner.call(p, mode="host_array", dp=dp)
+        prof = S.get_profile()
+        assert st == 0 and S.last_run_info()["path"] == "simt"
+    finally:
+        S.set_profiling(False)
+        S.set_kernel_config("simt", -1)
+    assert list(prof) == ["sgemm_tma"], prof
+    C = C.reshape(p.C.shape)
+    assert np.isfinite(C.reshape(batch, n, -1)[:, :, :m]).all()
+    assert O.normalized_error(p, C) <= 4 * max(k, 1) * 2.0 ** -24
+    np.testing.assert_array_equal(C.reshape(batch, n, -1)[:, :, m:], C0.reshape(batch, n, -1)[:, :, m:])
 
 
 # ------------------------------------------------------------------------- Ozaki: Inf / NaN ---

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "grouped.h"
 #include "internal.h"
 
 namespace ssb {
@@ -97,101 +98,122 @@ __device__ __forceinline__ void load_slab(double* dst, const double* __restrict_
   }
 }
 
-template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB, bool A_MN, bool B_MN>
-__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, MINB) dmma_gemm_kernel(DmmaArgs args) {
+// One BM x BN tile of C = alpha op(A) op(B) + beta C for one instance, by the whole CTA: the K loop
+// over the stage ring, then the epilogue. Leaves the stage buffers free (every copy has landed and
+// every thread has passed a barrier after its last read).
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, bool A_MN, bool B_MN>
+__device__ __forceinline__ void dmma_tile(const double* __restrict__ A, const double* __restrict__ B,
+                                          double* __restrict__ C, long m, long n, long k, long lda, long ldb,
+                                          long ldc, double alpha, double beta, long m0, long n0, double* smem) {
   constexpr int NWM = BM / WM, NWN = BN / WN;
   constexpr int NT = NWM * NWN * 32;
   constexpr int MI = WM / 8, NI = WN / 8;
   using Sm = DmmaSmem<BM, BN, BK>;
-  extern __shared__ __align__(16) double smem[];
-
-  const long tiles_m = (args.m + BM - 1) / BM;
-  const long m0 = (blockIdx.x % tiles_m) * BM;
-  const long n0 = (blockIdx.x / tiles_m) * BN;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int wm = warp % NWM, wn = warp / NWM;
   const int fr = lane >> 2, fk = lane & 3;    // fragment row (m or n) and k within an 8x4 block
+  const bool vecA = ((uintptr_t)A % 16 == 0) && (lda % 2 == 0);
+  const bool vecB = ((uintptr_t)B % 16 == 0) && (ldb % 2 == 0);
 
-  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) {
-    const double* __restrict__ A = args.A[b];
-    const double* __restrict__ B = args.B[b];
-    const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 2 == 0);
-    const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 2 == 0);
+  double acc[MI][NI][2];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    double acc[MI][NI][2];
+  const long ktiles = (k + BK - 1) / BK;
+  auto issue = [&](long kt) {
+    double* sa = smem + (kt % STAGES) * Sm::STAGE;
+    double* sb = sa + Sm::A_MAX;
+    load_slab<BM, BK, NT, A_MN>(sa, A, m, k, lda, m0, kt * BK, vecA);
+    load_slab<BN, BK, NT, B_MN>(sb, B, n, k, ldb, n0, kt * BK, vecB);
+  };
 #pragma unroll
-    for (int i = 0; i < MI; ++i)
-#pragma unroll
-      for (int j = 0; j < NI; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-    const long ktiles = (args.k + BK - 1) / BK;
-    auto issue = [&](long kt) {
-      double* sa = smem + (kt % STAGES) * Sm::STAGE;
-      double* sb = sa + Sm::A_MAX;
-      load_slab<BM, BK, NT, A_MN>(sa, A, args.m, args.k, args.lda, m0, kt * BK, vecA);
-      load_slab<BN, BK, NT, B_MN>(sb, B, args.n, args.k, args.ldb, n0, kt * BK, vecB);
-    };
-#pragma unroll
-    for (int s = 0; s < STAGES - 1; ++s) {
-      if (s < ktiles) issue(s);
-      cp_commit();
-    }
-    for (long kt = 0; kt < ktiles; ++kt) {
-      cp_wait<STAGES - 2>();
-      __syncthreads();
-      if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
-      cp_commit();
-      const double* sa = smem + (kt % STAGES) * Sm::STAGE;
-      const double* sb = sa + Sm::A_MAX;
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) issue(s);
+    cp_commit();
+  }
+  for (long kt = 0; kt < ktiles; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
+    cp_commit();
+    const double* sa = smem + (kt % STAGES) * Sm::STAGE;
+    const double* sb = sa + Sm::A_MAX;
 #pragma unroll 2
-      for (int k4 = 0; k4 < BK / 4; ++k4) {
-        const int kk = 4 * k4 + fk;
-        double af[MI], bf[NI];
+    for (int k4 = 0; k4 < BK / 4; ++k4) {
+      const int kk = 4 * k4 + fk;
+      double af[MI], bf[NI];
 #pragma unroll
-        for (int i = 0; i < MI; ++i) {
-          const int r = wm * WM + 8 * i + fr;
-          af[i] = A_MN ? sa[kk * Sm::PMN_A + r] : sa[r * Sm::PK + kk];
-        }
-#pragma unroll
-        for (int j = 0; j < NI; ++j) {
-          const int c = wn * WN + 8 * j + fr;
-          bf[j] = B_MN ? sb[kk * Sm::PMN_B + c] : sb[c * Sm::PK + kk];
-        }
-#pragma unroll
-        for (int i = 0; i < MI; ++i)
-#pragma unroll
-          for (int j = 0; j < NI; ++j) dmma(acc[i][j], af[i], bf[j]);
+      for (int i = 0; i < MI; ++i) {
+        const int r = wm * WM + 8 * i + fr;
+        af[i] = A_MN ? sa[kk * Sm::PMN_A + r] : sa[r * Sm::PK + kk];
       }
+#pragma unroll
+      for (int j = 0; j < NI; ++j) {
+        const int c = wn * WN + 8 * j + fr;
+        bf[j] = B_MN ? sb[kk * Sm::PMN_B + c] : sb[c * Sm::PK + kk];
+      }
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j) dmma(acc[i][j], af[i], bf[j]);
     }
-    cp_wait<0>();
-    __syncthreads();   // the next instance's copies reuse the stage buffers
+  }
+  cp_wait<0>();
+  __syncthreads();   // the next tile's copies reuse the stage buffers
 
-    // epilogue: lane holds C rows m0 + wm*WM + 8i + fr, columns n0 + wn*WN + 8j + 2fk + {0,1}
-    double* __restrict__ C = args.C[b];
-    const bool read_c = args.beta != 0.0;
+  // epilogue: lane holds C rows m0 + wm*WM + 8i + fr, columns n0 + wn*WN + 8j + 2fk + {0,1}
+  const bool read_c = beta != 0.0;
 #pragma unroll
-    for (int j = 0; j < NI; ++j) {
+  for (int j = 0; j < NI; ++j) {
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const long gj = n0 + wn * WN + 8 * j + 2 * fk + h;
-        if (gj >= args.n) continue;
-        double cv[MI];
+    for (int h = 0; h < 2; ++h) {
+      const long gj = n0 + wn * WN + 8 * j + 2 * fk + h;
+      if (gj >= n) continue;
+      double cv[MI];
 #pragma unroll
-        for (int i = 0; i < MI; ++i) {
-          const long gi = m0 + wm * WM + 8 * i + fr;
-          cv[i] = (read_c && gi < args.m) ? C[gi + gj * args.ldc] : 0.0;
-        }
+      for (int i = 0; i < MI; ++i) {
+        const long gi = m0 + wm * WM + 8 * i + fr;
+        cv[i] = (read_c && gi < m) ? C[gi + gj * ldc] : 0.0;
+      }
 #pragma unroll
-        for (int i = 0; i < MI; ++i) {
-          const long gi = m0 + wm * WM + 8 * i + fr;
-          if (gi < args.m) {
-            const double tb = read_c ? args.beta * cv[i] : 0.0;
-            C[gi + gj * args.ldc] = fma(acc[i][j][h], args.alpha, tb);
-          }
+      for (int i = 0; i < MI; ++i) {
+        const long gi = m0 + wm * WM + 8 * i + fr;
+        if (gi < m) {
+          const double tb = read_c ? beta * cv[i] : 0.0;
+          C[gi + gj * ldc] = fma(acc[i][j][h], alpha, tb);
         }
       }
     }
   }
+}
+
+template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, MINB) dmma_gemm_kernel(DmmaArgs args) {
+  extern __shared__ __align__(16) double smem[];
+  const long tiles_m = (args.m + BM - 1) / BM;
+  const long m0 = (blockIdx.x % tiles_m) * BM;
+  const long n0 = (blockIdx.x / tiles_m) * BN;
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y)
+    dmma_tile<BM, BN, BK, WM, WN, STAGES, A_MN, B_MN>(args.A[b], args.B[b], args.C[b], args.m, args.n, args.k,
+                                                       args.lda, args.ldb, args.ldc, args.alpha, args.beta, m0, n0,
+                                                       smem);
+}
+
+// Grouped form (plain fp64 instances of ssblasGemmGroupedBatchedEx): one CTA per (instance,
+// 64 x 64 tile) entry of a tile table whose instances all have this op(A) / op(B) layout.
+constexpr int kGBM = 64, kGBK = 16, kGW = 32, kGST = 4;
+template <bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((kGBM / kGW) * (kGBM / kGW) * 32, 2)
+dmma_grouped_kernel(const SimtGInst* __restrict__ inst, const int* __restrict__ tiles, const double* const* A,
+                    const double* const* B, double* const* C) {
+  extern __shared__ __align__(16) double smem[];
+  const int* t = tiles + 3 * (long)blockIdx.x;
+  const SimtGInst g = inst[t[0]];
+  dmma_tile<kGBM, kGBM, kGBK, kGW, kGW, kGST, A_MN, B_MN>(A[g.idx], B[g.idx], C[g.idx], g.m, g.n, g.k, g.lda, g.ldb,
+                                                          g.ldc, g.alpha_d, g.beta_d, (long)t[1] * kGBM,
+                                                          (long)t[2] * kGBM, smem);
 }
 
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MINB, bool A_MN, bool B_MN>
@@ -216,7 +238,38 @@ cudaError_t launch_layout(const DmmaArgs& a, bool a_mn, bool b_mn, cudaStream_t 
   return launch_cfg<BM, BN, BK, WM, WN, STAGES, MINB, false, false>(a, st);
 }
 
+template <bool A_MN, bool B_MN>
+cudaError_t launch_grouped_layout(const GroupedSimt& s, int lay, cudaStream_t st) {
+  constexpr int SMEM = kGST * DmmaSmem<kGBM, kGBM, kGBK>::STAGE * 8;
+  auto kern = dmma_grouped_kernel<A_MN, B_MN>;
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
+  kern<<<(unsigned)s.ndmma[lay], (kGBM / kGW) * (kGBM / kGW) * 32, SMEM, st>>>(
+      (const SimtGInst*)s.inst64, (const int*)s.dmma_tiles[lay], (const double* const*)s.A,
+      (const double* const*)s.B, (double* const*)s.C);
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+// The plain fp64 tiles of a grouped call, one launch per op(A) / op(B) layout present
+// (layout index = 2 * (op(A) rows contiguous) + (op(B) columns contiguous)).
+cudaError_t launch_dmma_grouped(const GroupedSimt& s, cudaStream_t st) {
+  if (!s.ndmma[0] && !s.ndmma[1] && !s.ndmma[2] && !s.ndmma[3]) return cudaSuccess;
+  ProfScope prof("dmma_grouped", st);
+  cudaError_t e = cudaSuccess;
+  for (int lay = 0; lay < 4 && e == cudaSuccess; ++lay) {
+    if (!s.ndmma[lay]) continue;
+    switch (lay) {
+      case 3: e = launch_grouped_layout<true, true>(s, lay, st); break;
+      case 2: e = launch_grouped_layout<true, false>(s, lay, st); break;
+      case 1: e = launch_grouped_layout<false, true>(s, lay, st); break;
+      default: e = launch_grouped_layout<false, false>(s, lay, st); break;
+    }
+  }
+  return e;
+}
 
 cudaError_t launch_dmma_f64(const BatchDesc& d, cudaStream_t st) {
   DmmaArgs a;

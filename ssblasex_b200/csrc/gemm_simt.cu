@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "grouped.h"
 #include "internal.h"
 
@@ -304,7 +306,7 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
 }
 
 GroupedSimt::~GroupedSimt() {
-  for (void* p : {inst32, tiles32, inst64, tiles64})
+  for (void* p : {inst32, tiles32, inst64, tiles64, dmma_tiles[0], dmma_tiles[1], dmma_tiles[2], dmma_tiles[3]})
     if (p) cudaFree(p);
 }
 
@@ -312,6 +314,11 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
                               cudaStream_t st) {
   std::vector<SimtGInst> in32, in64;
   std::vector<int> t32, t64;
+  struct DTile {
+    long k;
+    int li, a, b;
+  };
+  std::vector<DTile> td[4];
   for (int id : members) {
     const GroupedInst& x = g.inst[id];
     SimtGInst s{x.transa, x.transb, x.m, x.n, x.k, x.lda, x.ldb, x.ldc, x.idx, x.alpha_d, x.beta_d, x.alpha_f, x.beta_f};
@@ -319,12 +326,29 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
     auto& tv = (x.row == ROW_F64) ? t64 : t32;
     const int li = (int)iv.size();
     iv.push_back(s);
+    // plain fp64 on the FP64 tensor cores, as the batched call does, unless its DMMA configuration
+    // for this shape is 2 (the DFMA kernel)
+    const bool dmma = x.row == ROW_F64 && choose_config(SSBLAS_PATH_DMMA, x.m, x.n, x.k, 1, 0) != 2;
+    const int lay = 2 * (x.transa == SSBLAS_OP_N ? 1 : 0) + (x.transb == SSBLAS_OP_T ? 1 : 0);
     for (long a = 0; a < (x.m + 63) / 64; ++a)
       for (long b = 0; b < (x.n + 63) / 64; ++b) {
+        if (dmma) {
+          td[lay].push_back({x.k, li, (int)a, (int)b});
+          continue;
+        }
         tv.push_back(li);
         tv.push_back((int)a);
         tv.push_back((int)b);
       }
+  }
+  std::vector<int> tdl[4];
+  for (int l = 0; l < 4; ++l) {
+    std::stable_sort(td[l].begin(), td[l].end(), [](const DTile& p, const DTile& q) { return p.k > q.k; });
+    for (const DTile& t : td[l]) {
+      tdl[l].push_back(t.li);
+      tdl[l].push_back(t.a);
+      tdl[l].push_back(t.b);
+    }
   }
   cudaError_t e;
   auto up = [&](void** dst, const void* src, size_t n) -> cudaError_t {
@@ -338,14 +362,21 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
       (e = up(&out.inst64, in64.data(), in64.size() * sizeof(SimtGInst))) ||
       (e = up(&out.tiles64, t64.data(), t64.size() * sizeof(int))))
     return e;
+  for (int l = 0; l < 4; ++l)
+    if ((e = up(&out.dmma_tiles[l], tdl[l].data(), tdl[l].size() * sizeof(int)))) return e;
   out.ntiles32 = (long)t32.size() / 3;
   out.ntiles64 = (long)t64.size() / 3;
   out.A = g.A; out.B = g.B; out.C = g.C;
   out.launches = (out.ntiles32 ? 1 : 0) + (out.ntiles64 ? 1 : 0);
+  for (int l = 0; l < 4; ++l) {
+    out.ndmma[l] = (long)tdl[l].size() / 3;
+    out.launches += out.ndmma[l] ? 1 : 0;
+  }
   return cudaStreamSynchronize(st);
 }
 
 cudaError_t launch_simt_grouped(const GroupedSimt& s, cudaStream_t st) {
+  if (!s.ntiles32 && !s.ntiles64) return cudaSuccess;
   ProfScope prof("simt_grouped", st);
   if (s.ntiles32) {
     simt_grouped_kernel<float, 64, 64, 16, 4, 4><<<(unsigned)s.ntiles32, 256, 0, st>>>(

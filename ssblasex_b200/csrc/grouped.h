@@ -37,6 +37,11 @@ struct SimtGInst {
 struct GroupedSimt {
   void *inst32 = nullptr, *tiles32 = nullptr, *inst64 = nullptr, *tiles64 = nullptr;
   long ntiles32 = 0, ntiles64 = 0;
+  // fp64 tiles for the FP64 tensor cores (gemm_dmma.cu), one table per op(A) / op(B) layout
+  // (2 * (op(A) rows contiguous) + (op(B) columns contiguous)), longest k first; their instances
+  // are in inst64
+  void* dmma_tiles[4] = {};
+  long ndmma[4] = {};
   const void* const* A = nullptr;
   const void* const* B = nullptr;
   void* const* C = nullptr;
@@ -46,6 +51,7 @@ struct GroupedSimt {
 cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& members, GroupedSimt& out,
                               cudaStream_t st);
 cudaError_t launch_simt_grouped(const GroupedSimt& s, cudaStream_t st);
+cudaError_t launch_dmma_grouped(const GroupedSimt& s, cudaStream_t st);
 
 // Runs all instances with device-resident operands: one pre-pass and one persistent GEMM launch per
 // kind, replayed from a captured CUDA graph when the same call signature repeats.

@@ -145,6 +145,8 @@ bool make_tiled_map(CUtensorMap* map, CUtensorMapDataType dt, int rank, const vo
 
 // Configuration index of a kernel family for a problem (tune.cpp): forced, tuned, or `fallback`.
 int choose_config(int path, long m, long n, long k, long batch, int fallback);
+// the configuration forced by ssblasSetKernelConfig for `path`, -1 if none
+int forced_config(int path);
 
 // Optional per-kernel CUDA-event timing (ssblasSetProfiling): records an event pair around each
 // launch on its stream; ssblasGetProfile resolves them. Each launch is also an NVTX range of the

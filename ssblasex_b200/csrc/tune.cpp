@@ -75,6 +75,11 @@ int choose_config(int path, long m, long n, long k, long batch, int fallback) {
   return it != g_table.end() ? it->second : fallback;
 }
 
+int forced_config(int path) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  return (path >= 0 && path < kKeys) ? g_forced[path] : -1;
+}
+
 }  // namespace ssb
 
 extern "C" ssblasStatus_t ssblasSetKernelConfig(int path, int config) {

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "grouped.h"
 #include "internal.h"
 
 namespace ssb {
@@ -103,108 +104,129 @@ __device__ __forceinline__ void sload(float* dst, const float* __restrict__ X, l
   }
 }
 
-template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB, bool A_MN, bool B_MN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_async_kernel(SgemmArgs args) {
+// One BM x BN tile of C = alpha op(A) op(B) + beta C for one instance, by the whole CTA: the K loop
+// over the stage ring, then the epilogue. Leaves the stage buffers free.
+template <int BM, int BN, int BK, int TM, int TN, int STAGES, bool A_MN, bool B_MN>
+__device__ __forceinline__ void sgemm_tile(const float* __restrict__ A, const float* __restrict__ B,
+                                           float* __restrict__ C, long m, long n, long k, long lda, long ldb,
+                                           long ldc, float alpha, float beta, long m0, long n0, float* sm) {
   constexpr int TX = BM / TM, TY = BN / TN, NT = TX * TY;
   constexpr int PA = BM + 4, PB = BN + 4;
   constexpr int STAGE = BK * (PA + PB);
-  extern __shared__ __align__(16) float sm[];
-
-  const long tiles_m = (args.m + BM - 1) / BM;
-  const long m0 = (blockIdx.x % tiles_m) * BM;
-  const long n0 = (blockIdx.x / tiles_m) * BN;
   // warp = 4 (m) x 8 (n) threads
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
   constexpr int WX = TX / 4;   // warps along m
   const int tx = (warp % WX) * 4 + lane % 4;
   const int ty = (warp / WX) * 8 + lane / 4;
+  const bool vecA = ((uintptr_t)A % 16 == 0) && (lda % 4 == 0);
+  const bool vecB = ((uintptr_t)B % 16 == 0) && (ldb % 4 == 0);
+  float acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
 
-  for (long b = blockIdx.y; b < args.batch; b += gridDim.y) {
-    const float* __restrict__ A = args.A[b];
-    const float* __restrict__ B = args.B[b];
-    const bool vecA = ((uintptr_t)A % 16 == 0) && (args.lda % 4 == 0);
-    const bool vecB = ((uintptr_t)B % 16 == 0) && (args.ldb % 4 == 0);
-    float acc[TM][TN];
+  const long ktiles = (k + BK - 1) / BK;
+  auto issue = [&](long kt) {
+    float* sa = sm + (kt % STAGES) * STAGE;
+    float* sb = sa + BK * PA;
+    sload<BM, BK, NT, A_MN>(sa, A, m, k, lda, m0, kt * BK, vecA);
+    sload<BN, BK, NT, B_MN>(sb, B, n, k, ldb, n0, kt * BK, vecB);
+  };
 #pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TN; ++j) acc[i][j] = 0.0f;
-
-    const long ktiles = (args.k + BK - 1) / BK;
-    auto issue = [&](long kt) {
-      float* sa = sm + (kt % STAGES) * STAGE;
-      float* sb = sa + BK * PA;
-      sload<BM, BK, NT, A_MN>(sa, A, args.m, args.k, args.lda, m0, kt * BK, vecA);
-      sload<BN, BK, NT, B_MN>(sb, B, args.n, args.k, args.ldb, n0, kt * BK, vecB);
-    };
-#pragma unroll
-    for (int s = 0; s < STAGES - 1; ++s) {
-      if (s < ktiles) issue(s);
-      commit_s();
-    }
-    for (long kt = 0; kt < ktiles; ++kt) {
-      wait_s<STAGES - 2>();
-      __syncthreads();
-      if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
-      commit_s();
-      const float* sa = sm + (kt % STAGES) * STAGE;
-      const float* sb = sa + BK * PA;
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) issue(s);
+    commit_s();
+  }
+  for (long kt = 0; kt < ktiles; ++kt) {
+    wait_s<STAGES - 2>();
+    __syncthreads();
+    if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
+    commit_s();
+    const float* sa = sm + (kt % STAGES) * STAGE;
+    const float* sb = sa + BK * PA;
 #pragma unroll 4
-      for (int kk = 0; kk < BK; ++kk) {
-        float av[TM], bv[TN];
+    for (int kk = 0; kk < BK; ++kk) {
+      float av[TM], bv[TN];
 #pragma unroll
-        for (int i = 0; i < TM; i += 4) {
-          const float4 x = *(const float4*)(sa + kk * PA + tx * TM + i);
-          av[i] = x.x; av[i + 1] = x.y; av[i + 2] = x.z; av[i + 3] = x.w;
-        }
-#pragma unroll
-        for (int j = 0; j < TN; j += 4) {
-          const float4 x = *(const float4*)(sb + kk * PB + ty * TN + j);
-          bv[j] = x.x; bv[j + 1] = x.y; bv[j + 2] = x.z; bv[j + 3] = x.w;
-        }
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-#pragma unroll
-          for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      for (int i = 0; i < TM; i += 4) {
+        const float4 x = *(const float4*)(sa + kk * PA + tx * TM + i);
+        av[i] = x.x; av[i + 1] = x.y; av[i + 2] = x.z; av[i + 3] = x.w;
       }
-    }
-    wait_s<0>();
-    __syncthreads();   // the next instance's copies reuse the stage buffers
-
-    // epilogue: C rows m0 + tx*TM + i (contiguous per thread), columns n0 + ty*TN + j; 16-byte
-    // reads and writes when the thread's rows are inside C and C is 16-byte aligned
-    float* __restrict__ C = args.C[b];
-    const bool read_c = args.beta != 0.0f;
-    const long gi0 = m0 + tx * TM;
-    const bool cvec = (((uintptr_t)C) % 16 == 0) && (args.ldc % 4 == 0) && gi0 + TM <= args.m;
 #pragma unroll
-    for (int j = 0; j < TN; ++j) {
-      const long gj = n0 + ty * TN + j;
-      if (gj >= args.n) continue;
-      float* cp = C + gi0 + gj * args.ldc;
-      if (cvec) {
-        float4 cv[TM / 4];
-#pragma unroll
-        for (int i = 0; i < TM; i += 4) cv[i / 4] = read_c ? *(const float4*)(cp + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int i = 0; i < TM; i += 4) {
-          float4 o;
-          o.x = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[i / 4].x : 0.0f);
-          o.y = fmaf(acc[i + 1][j], args.alpha, read_c ? args.beta * cv[i / 4].y : 0.0f);
-          o.z = fmaf(acc[i + 2][j], args.alpha, read_c ? args.beta * cv[i / 4].z : 0.0f);
-          o.w = fmaf(acc[i + 3][j], args.alpha, read_c ? args.beta * cv[i / 4].w : 0.0f);
-          *(float4*)(cp + i) = o;
-        }
-      } else {
-        float cv[TM];
-#pragma unroll
-        for (int i = 0; i < TM; ++i) cv[i] = (read_c && gi0 + i < args.m) ? cp[i] : 0.0f;
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-          if (gi0 + i < args.m) cp[i] = fmaf(acc[i][j], args.alpha, read_c ? args.beta * cv[i] : 0.0f);
+      for (int j = 0; j < TN; j += 4) {
+        const float4 x = *(const float4*)(sb + kk * PB + ty * TN + j);
+        bv[j] = x.x; bv[j + 1] = x.y; bv[j + 2] = x.z; bv[j + 3] = x.w;
       }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
   }
+  wait_s<0>();
+  __syncthreads();   // the next tile's copies reuse the stage buffers
+
+  // epilogue: C rows m0 + tx*TM + i (contiguous per thread), columns n0 + ty*TN + j; 16-byte
+  // reads and writes when the thread's rows are inside C and C is 16-byte aligned
+  const bool read_c = beta != 0.0f;
+  const long gi0 = m0 + tx * TM;
+  const bool cvec = (((uintptr_t)C) % 16 == 0) && (ldc % 4 == 0) && gi0 + TM <= m;
+#pragma unroll
+  for (int j = 0; j < TN; ++j) {
+    const long gj = n0 + ty * TN + j;
+    if (gj >= n) continue;
+    float* cp = C + gi0 + gj * ldc;
+    if (cvec) {
+      float4 cv[TM / 4];
+#pragma unroll
+      for (int i = 0; i < TM; i += 4) cv[i / 4] = read_c ? *(const float4*)(cp + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int i = 0; i < TM; i += 4) {
+        float4 o;
+        o.x = fmaf(acc[i][j], alpha, read_c ? beta * cv[i / 4].x : 0.0f);
+        o.y = fmaf(acc[i + 1][j], alpha, read_c ? beta * cv[i / 4].y : 0.0f);
+        o.z = fmaf(acc[i + 2][j], alpha, read_c ? beta * cv[i / 4].z : 0.0f);
+        o.w = fmaf(acc[i + 3][j], alpha, read_c ? beta * cv[i / 4].w : 0.0f);
+        *(float4*)(cp + i) = o;
+      }
+    } else {
+      float cv[TM];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) cv[i] = (read_c && gi0 + i < m) ? cp[i] : 0.0f;
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+        if (gi0 + i < m) cp[i] = fmaf(acc[i][j], alpha, read_c ? beta * cv[i] : 0.0f);
+    }
+  }
+}
+
+template <int BM, int BN, int BK, int TM, int TN, int STAGES, int MINB, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB) sgemm_async_kernel(SgemmArgs args) {
+  extern __shared__ __align__(16) float sm[];
+  const long tiles_m = (args.m + BM - 1) / BM;
+  const long m0 = (blockIdx.x % tiles_m) * BM;
+  const long n0 = (blockIdx.x / tiles_m) * BN;
+  for (long b = blockIdx.y; b < args.batch; b += gridDim.y)
+    sgemm_tile<BM, BN, BK, TM, TN, STAGES, A_MN, B_MN>(args.A[b], args.B[b], args.C[b], args.m, args.n, args.k,
+                                                       args.lda, args.ldb, args.ldc, args.alpha, args.beta, m0, n0,
+                                                       sm);
+}
+
+// Grouped form (plain fp32 instances of ssblasGemmGroupedBatchedEx): one CTA per (instance,
+// 64 x 64 tile) entry of a tile table whose instances all have this op(A) / op(B) layout; the tile
+// shape of configuration 3.
+constexpr int kGT = 64, kGBK = 32, kGTM = 4, kGST = 2;
+template <bool A_MN, bool B_MN>
+__global__ void __launch_bounds__((kGT / kGTM) * (kGT / kGTM), 3)
+sgemm_grouped_kernel(const SimtGInst* __restrict__ inst, const int* __restrict__ tiles, const float* const* A,
+                     const float* const* B, float* const* C) {
+  extern __shared__ __align__(16) float sm[];
+  const int* t = tiles + 3 * (long)blockIdx.x;
+  const SimtGInst g = inst[t[0]];
+  sgemm_tile<kGT, kGT, kGBK, kGTM, kGTM, kGST, A_MN, B_MN>(A[g.idx], B[g.idx], C[g.idx], g.m, g.n, g.k, g.lda, g.ldb,
+                                                         g.ldc, g.alpha_f, g.beta_f, (long)t[1] * kGT,
+                                                         (long)t[2] * kGT, sm);
 }
 
 // Persistent form for K <= KS * BK (the whole K of a work item fits the KS stages of one buffer):
@@ -623,6 +645,37 @@ cudaError_t launch_sl(const SgemmArgs& a, bool a_mn, bool b_mn, cudaStream_t st)
 }
 
 }  // namespace
+
+template <bool A_MN, bool B_MN>
+cudaError_t launch_sgemm_grouped_layout(const GroupedSimt& s, int lay, cudaStream_t st) {
+  constexpr int SMEM = kGST * kGBK * (2 * kGT + 8) * 4;
+  auto kern = sgemm_grouped_kernel<A_MN, B_MN>;
+  static bool attr[kMaxDevices] = {};
+  if (cudaError_t e = smem_attr_once(attr, kern, SMEM)) return e;
+  kern<<<(unsigned)s.nsg[lay], (kGT / kGTM) * (kGT / kGTM), SMEM, st>>>(
+      (const SimtGInst*)s.inst32, (const int*)s.sg_tiles[lay], (const float* const*)s.A, (const float* const*)s.B,
+      (float* const*)s.C);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// The plain fp32 tiles of a grouped call, one launch per op(A) / op(B) layout present (layout
+// index = 2 * (op(A) rows contiguous) + (op(B) columns contiguous)).
+cudaError_t launch_sgemm_grouped(const GroupedSimt& s, cudaStream_t st) {
+  if (!s.nsg[0] && !s.nsg[1] && !s.nsg[2] && !s.nsg[3]) return cudaSuccess;
+  ProfScope prof("sgemm_grouped", st);
+  cudaError_t e = cudaSuccess;
+  for (int lay = 0; lay < 4 && e == cudaSuccess; ++lay) {
+    if (!s.nsg[lay]) continue;
+    switch (lay) {
+      case 3: e = launch_sgemm_grouped_layout<true, true>(s, lay, st); break;
+      case 2: e = launch_sgemm_grouped_layout<true, false>(s, lay, st); break;
+      case 1: e = launch_sgemm_grouped_layout<false, true>(s, lay, st); break;
+      default: e = launch_sgemm_grouped_layout<false, false>(s, lay, st); break;
+    }
+  }
+  return e;
+}
 
 cudaError_t launch_sgemm_async(const BatchDesc& d, int config, cudaStream_t st) {
   SgemmArgs a;

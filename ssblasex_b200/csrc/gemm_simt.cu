@@ -306,7 +306,8 @@ cudaError_t launch_simt_gemm(const BatchDesc& d, cudaStream_t stream) {
 }
 
 GroupedSimt::~GroupedSimt() {
-  for (void* p : {inst32, tiles32, inst64, tiles64, dmma_tiles[0], dmma_tiles[1], dmma_tiles[2], dmma_tiles[3]})
+  for (void* p : {inst32, tiles32, inst64, tiles64, dmma_tiles[0], dmma_tiles[1], dmma_tiles[2], dmma_tiles[3],
+                  sg_tiles[0], sg_tiles[1], sg_tiles[2], sg_tiles[3]})
     if (p) cudaFree(p);
 }
 
@@ -318,7 +319,7 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
     long k;
     int li, a, b;
   };
-  std::vector<DTile> td[4];
+  std::vector<DTile> td[4], ts[4];   // DMMA (fp64) and cp.async FFMA (fp32) tiles per layout
   for (int id : members) {
     const GroupedInst& x = g.inst[id];
     SimtGInst s{x.transa, x.transb, x.m, x.n, x.k, x.lda, x.ldb, x.ldc, x.idx, x.alpha_d, x.beta_d, x.alpha_f, x.beta_f};
@@ -329,11 +330,14 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
     // plain fp64 on the FP64 tensor cores, as the batched call does, unless its DMMA configuration
     // for this shape is 2 (the DFMA kernel)
     const bool dmma = x.row == ROW_F64 && choose_config(SSBLAS_PATH_DMMA, x.m, x.n, x.k, 1, 0) != 2;
+    // plain fp32 on the cp.async FFMA tiles unless the SIMT configuration for this shape is 0 or 1
+    // (the register-tiled SIMT kernel)
+    const bool sg = x.row == ROW_F32 && choose_config(SSBLAS_PATH_SIMT, x.m, x.n, x.k, 1, 3) >= 3;
     const int lay = 2 * (x.transa == SSBLAS_OP_N ? 1 : 0) + (x.transb == SSBLAS_OP_T ? 1 : 0);
     for (long a = 0; a < (x.m + 63) / 64; ++a)
       for (long b = 0; b < (x.n + 63) / 64; ++b) {
-        if (dmma) {
-          td[lay].push_back({x.k, li, (int)a, (int)b});
+        if (dmma || sg) {
+          (dmma ? td : ts)[lay].push_back({x.k, li, (int)a, (int)b});
           continue;
         }
         tv.push_back(li);
@@ -341,14 +345,18 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
         tv.push_back((int)b);
       }
   }
-  std::vector<int> tdl[4];
-  for (int l = 0; l < 4; ++l) {
-    std::stable_sort(td[l].begin(), td[l].end(), [](const DTile& p, const DTile& q) { return p.k > q.k; });
-    for (const DTile& t : td[l]) {
-      tdl[l].push_back(t.li);
-      tdl[l].push_back(t.a);
-      tdl[l].push_back(t.b);
+  std::vector<int> tdl[4], tsl[4];
+  auto flatten = [](std::vector<DTile>& v, std::vector<int>& out) {
+    std::stable_sort(v.begin(), v.end(), [](const DTile& p, const DTile& q) { return p.k > q.k; });
+    for (const DTile& t : v) {
+      out.push_back(t.li);
+      out.push_back(t.a);
+      out.push_back(t.b);
     }
+  };
+  for (int l = 0; l < 4; ++l) {
+    flatten(td[l], tdl[l]);
+    flatten(ts[l], tsl[l]);
   }
   cudaError_t e;
   auto up = [&](void** dst, const void* src, size_t n) -> cudaError_t {
@@ -363,14 +371,17 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
       (e = up(&out.tiles64, t64.data(), t64.size() * sizeof(int))))
     return e;
   for (int l = 0; l < 4; ++l)
-    if ((e = up(&out.dmma_tiles[l], tdl[l].data(), tdl[l].size() * sizeof(int)))) return e;
+    if ((e = up(&out.dmma_tiles[l], tdl[l].data(), tdl[l].size() * sizeof(int))) ||
+        (e = up(&out.sg_tiles[l], tsl[l].data(), tsl[l].size() * sizeof(int))))
+      return e;
   out.ntiles32 = (long)t32.size() / 3;
   out.ntiles64 = (long)t64.size() / 3;
   out.A = g.A; out.B = g.B; out.C = g.C;
   out.launches = (out.ntiles32 ? 1 : 0) + (out.ntiles64 ? 1 : 0);
   for (int l = 0; l < 4; ++l) {
     out.ndmma[l] = (long)tdl[l].size() / 3;
-    out.launches += out.ndmma[l] ? 1 : 0;
+    out.nsg[l] = (long)tsl[l].size() / 3;
+    out.launches += (out.ndmma[l] ? 1 : 0) + (out.nsg[l] ? 1 : 0);
   }
   return cudaStreamSynchronize(st);
 }

@@ -10,8 +10,8 @@
 // Phase 2 (GEMM, one launch per kind): the persistent tcgen05 kernel walks a device-side tile
 //   table (instance, row tile, column tile), longest K first; its producer stages each chunk with a
 //   single plain bulk copy, so no per-instance tensor map is needed.
-// Plain fp32 instances run through the grouped SIMT kernel (gemm_simt.cu), plain fp64 ones on the
-// FP64 tensor cores (gemm_dmma.cu, one launch per op(A) / op(B) layout present).
+// Plain fp32 instances run on the cp.async FFMA tiles (gemm_sgemm.cu), plain fp64 ones on the FP64
+// tensor cores (gemm_dmma.cu), one launch per op(A) / op(B) layout present.
 //
 // The sequence is captured once per distinct call signature into a CUDA graph and replayed.
 #include <cuda_bf16.h>
@@ -459,6 +459,7 @@ std::vector<uint64_t> signature(const GroupedDesc& g, int mode, int oz_cfg) {
   k.push_back((uint64_t)mode | ((uint64_t)oz_cfg << 32));
   // a forced DMMA configuration decides whether plain fp64 instances take the tensor cores
   k.push_back((uint64_t)(int64_t)forced_config(SSBLAS_PATH_DMMA));
+  k.push_back((uint64_t)(int64_t)forced_config(SSBLAS_PATH_SIMT));
   k.push_back((uint64_t)(uintptr_t)g.A);
   k.push_back((uint64_t)(uintptr_t)g.B);
   k.push_back((uint64_t)(uintptr_t)g.C);
@@ -488,6 +489,7 @@ cudaError_t run_plan(Plan& pl, cudaStream_t st) {
   if ((e = launch_kind<GCfgI8, 0, 1>(pl.i8, pl.C, st, "grouped_pack_i8", "grouped_i8_gemm", pl.dynamic))) return e;
   if (pl.simt && (e = launch_simt_grouped(*pl.simt, st))) return e;
   if (pl.simt && (e = launch_dmma_grouped(*pl.simt, st))) return e;
+  if (pl.simt && (e = launch_sgemm_grouped(*pl.simt, st))) return e;
   return cudaSuccess;
 }
 

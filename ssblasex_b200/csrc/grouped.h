@@ -27,7 +27,8 @@ struct GroupedDesc {
   void* const* C;
 };
 
-// plain fp32/fp64 instances of a grouped call (SIMT kernels, 64 x 64 tiles)
+// plain fp32/fp64 instances of a grouped call (64 x 64 tiles: FFMA / DMMA kernels, or the SIMT
+// kernel where a forced configuration asks for it)
 struct SimtGInst {
   int transa, transb;
   long m, n, k, lda, ldb, ldc, idx;
@@ -42,6 +43,9 @@ struct GroupedSimt {
   // are in inst64
   void* dmma_tiles[4] = {};
   long ndmma[4] = {};
+  // fp32 tiles for the cp.async FFMA kernel (gemm_sgemm.cu), the same way; instances in inst32
+  void* sg_tiles[4] = {};
+  long nsg[4] = {};
   const void* const* A = nullptr;
   const void* const* B = nullptr;
   void* const* C = nullptr;
@@ -52,6 +56,7 @@ cudaError_t plan_simt_grouped(const GroupedDesc& g, const std::vector<int>& memb
                               cudaStream_t st);
 cudaError_t launch_simt_grouped(const GroupedSimt& s, cudaStream_t st);
 cudaError_t launch_dmma_grouped(const GroupedSimt& s, cudaStream_t st);
+cudaError_t launch_sgemm_grouped(const GroupedSimt& s, cudaStream_t st);
 
 // Runs all instances with device-resident operands: one pre-pass and one persistent GEMM launch per
 // kind, replayed from a captured CUDA graph when the same call signature repeats.

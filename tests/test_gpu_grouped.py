@@ -239,20 +239,23 @@ def test_grouped_ozaki_tile_shapes(gcfg):
         S.set_math_mode(0)
 
 
-@pytest.mark.parametrize("dmma_cfg", [-1, 2])
-def test_grouped_plain_fp64_tensor_cores(dmma_cfg):
-    """Plain fp64 instances of a grouped call run on the FP64 tensor cores (one DMMA launch per
-    op(A) / op(B) layout present, tiles longest k first), as the batched call does; forcing the
-    DMMA configuration 2 sends them to the DFMA kernel instead. Every layout, ragged and tiny
+@pytest.mark.parametrize("row,forced", [("f64", -1), ("f64", 2), ("f32", -1), ("f32", 1)])
+def test_grouped_plain_tensor_and_ffma_tiles(row, forced):
+    """Plain instances of a grouped call on the batched call's kernels: fp64 on the FP64 tensor
+    cores (DMMA), fp32 on the cp.async FFMA tiles -- one launch per op(A) / op(B) layout present,
+    tiles longest k first; forcing the DMMA configuration 2 (fp64) or the SIMT configuration 1
+    (fp32) sends them to the register-tiled SIMT kernel instead. Every layout, ragged and tiny
     shapes, beta = 0 and beta != 0, each within 4 k u of the FP64-exact oracle, fresh plan and
     graph replay."""
     import ssblasex_b200 as S
     from ssblasex_b200 import runner, workloads as W
     shapes = [(1, 1, 1), (70, 33, 5), (64, 64, 64), (130, 200, 97), (256, 96, 300), (17, 150, 16)]
-    probs = [W.make_problem("f64", ta, tb, m, n, k, 1, 0.75, 0.0 if i % 2 else -0.5, seed=400 + 10 * i + 2 * ta + tb)
+    probs = [W.make_problem(row, ta, tb, m, n, k, 1, 0.75, 0.0 if i % 2 else -0.5, seed=400 + 10 * i + 2 * ta + tb)
              for i, (m, n, k) in enumerate(shapes) for ta in (0, 1) for tb in (0, 1)]
+    key = "dmma" if row == "f64" else "simt"
+    u = 2.0 ** -53 if row == "f64" else 2.0 ** -24
     S.set_math_mode(S.SSBLAS_MATH_PLAIN)
-    S.set_kernel_config("dmma", dmma_cfg)
+    S.set_kernel_config(key, forced)
     try:
         gd = runner.GroupedDevice(probs)
         for rep in range(3):            # plan (profiled), capture, replay
@@ -262,13 +265,13 @@ def test_grouped_plain_fp64_tensor_cores(dmma_cfg):
             if rep == 0:
                 prof = S.get_profile()
                 S.set_profiling(False)
-                want = "simt_grouped" if dmma_cfg == 2 else "dmma_grouped"
+                want = "simt_grouped" if forced >= 0 else ("dmma_grouped" if row == "f64" else "sgemm_grouped")
                 assert want in prof and set(prof) <= {want}, prof
-                # one DMMA launch per layout, or one DFMA launch for all
-                assert S.last_run_info()["kernel_launches"] == (1 if dmma_cfg == 2 else 4)
+                # one launch per layout, or one SIMT launch for all
+                assert S.last_run_info()["kernel_launches"] == (1 if forced >= 0 else 4)
             for p, C in zip(probs, gd.results()):
-                assert O.normalized_error(p, C) <= 4 * max(p.k, 1) * 2.0 ** -53, p.name
+                assert O.normalized_error(p, C) <= 4 * max(p.k, 1) * u, p.name
     finally:
         S.set_profiling(False)
-        S.set_kernel_config("dmma", -1)
+        S.set_kernel_config(key, -1)
         S.set_math_mode(0)

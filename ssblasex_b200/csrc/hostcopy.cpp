@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "hostcopy.h"
+#include "hostcopy_plan.h"
 #include "internal.h"
 
 namespace ssb {
@@ -143,12 +144,11 @@ cudaError_t gather_to_device(char* dst, size_t pitch, const void* const* src, lo
     // the chunk's bytes of every instance overlapping [c0, c1), split over the pool
     const int parts = P.size() * 2;
     P.run(parts, [&](int part) {
-      const size_t p0 = c0 + (c1 - c0) * part / parts, p1 = c0 + (c1 - c0) * (part + 1) / parts;
-      for (long b = (long)(p0 / pitch); b < batch && (size_t)b * pitch < p1; ++b) {
-        const size_t i0 = (size_t)b * pitch, i1 = i0 + bytes;   // instance b in the device layout
-        const size_t lo = std::max(p0, i0), hi = std::min(p1, i1);
-        if (lo < hi) memcpy(buf + (lo - c0), (const char*)src[b] + (lo - i0), hi - lo);
-      }
+      size_t p0, p1;
+      window_part(c0, c1, part, parts, &p0, &p1);
+      gather_pieces(p0, p1, pitch, batch, bytes, [&](long b, size_t in_inst, size_t at, size_t len) {
+        memcpy(buf + (at - c0), (const char*)src[b] + in_inst, len);
+      });
     });
     if ((e = cudaMemcpyAsync(dst + c0, buf, c1 - c0, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(sg->ev[slot], st)) != cudaSuccess) return e;
@@ -186,16 +186,12 @@ cudaError_t scatter_to_host(void* const* dst, size_t ld_bytes, const char* src, 
     // the first row_bytes of every column that overlap [c0, c1), split over the pool
     const int parts = P.size() * 2;
     P.run(parts, [&](int part) {
-      const size_t p0 = c0 + (c1 - c0) * part / parts, p1 = c0 + (c1 - c0) * (part + 1) / parts;
-      for (long b = (long)(p0 / pitch); b < batch && (size_t)b * pitch < p1; ++b) {
-        const size_t ib = (size_t)b * pitch;
-        long j = p0 > ib ? (long)((p0 - ib) / ld_bytes) : 0;
-        for (; j < cols && ib + (size_t)j * ld_bytes < p1; ++j) {
-          const size_t s0 = ib + (size_t)j * ld_bytes, s1 = s0 + row_bytes;
-          const size_t lo = std::max(p0, s0), hi = std::min(p1, s1);
-          if (lo < hi) memcpy((char*)dst[b] + (size_t)j * ld_bytes + (lo - s0), buf + (lo - c0), hi - lo);
-        }
-      }
+      size_t p0, p1;
+      window_part(c0, c1, part, parts, &p0, &p1);
+      scatter_pieces(p0, p1, pitch, batch, ld_bytes, row_bytes, cols,
+                     [&](long b, size_t in_inst, size_t at, size_t len) {
+                       memcpy((char*)dst[b] + in_inst, buf + (at - c0), len);
+                     });
     });
   }
   return cudaSuccess;

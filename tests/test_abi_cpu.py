@@ -153,6 +153,108 @@ int main() {
     assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout)
 
 
+def test_staged_copy_pieces(tmp_path):
+    """The byte arithmetic of the staged host copies (csrc/hostcopy_plan.h): for random instance
+    sizes, pitches, column layouts, staging windows and part counts, every byte of every instance
+    lands exactly once at its place -- instance b at b * pitch on the device side; for the copy
+    back only the first row_bytes of each column -- and no byte between instances (or in the
+    caller's column padding) is written."""
+    src = tmp_path / "t.cpp"
+    src.write_text(r"""
+#include "hostcopy_plan.h"
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <vector>
+using namespace ssb;
+int main() {
+  std::mt19937_64 rng(7);
+  auto U = [&](long lo, long hi) { return lo + (long)(rng() % (unsigned long)(hi - lo + 1)); };
+  for (int trial = 0; trial < 400; ++trial) {
+    // gather: instance b (bytes) to b * pitch
+    {
+      const long batch = U(1, 40);
+      const size_t bytes = U(1, 5000), pitch = bytes + U(0, 300);
+      const size_t total = pitch * (batch - 1) + bytes;
+      std::vector<std::vector<unsigned char>> inst(batch, std::vector<unsigned char>(bytes));
+      for (auto& v : inst) for (auto& x : v) x = (unsigned char)rng();
+      std::vector<unsigned char> dev(total, 0xEE);
+      std::vector<int> hits(total, 0);
+      const size_t W = U(1, 20000);
+      const int parts = (int)U(1, 17);
+      for (size_t c0 = 0; c0 < total; c0 += W) {
+        const size_t c1 = c0 + W < total ? c0 + W : total;
+        for (int part = 0; part < parts; ++part) {
+          size_t p0, p1;
+          window_part(c0, c1, part, parts, &p0, &p1);
+          gather_pieces(p0, p1, pitch, batch, bytes, [&](long b, size_t in_inst, size_t at, size_t len) {
+            if (at < p0 || at + len > p1 || in_inst + len > bytes) { std::printf("range\n"); std::exit(1); }
+            std::memcpy(&dev[at], &inst[b][in_inst], len);
+            for (size_t i = 0; i < len; ++i) ++hits[at + i];
+          });
+        }
+      }
+      for (long b = 0; b < batch; ++b)
+        for (size_t x = 0; x < pitch && b * pitch + x < total; ++x) {
+          const size_t at = b * pitch + x;
+          if (x < bytes ? (hits[at] != 1 || dev[at] != inst[b][x]) : (hits[at] != 0 || dev[at] != 0xEE)) {
+            std::printf("gather trial %d b %ld x %zu\n", trial, b, x);
+            return 2;
+          }
+        }
+    }
+    // scatter: the first row_bytes of each of cols columns (ld_bytes apart) of instance b
+    {
+      const long batch = U(1, 30), cols = U(1, 40);
+      const size_t row_bytes = U(1, 400), ld_bytes = row_bytes + U(0, 64);
+      const size_t span = ld_bytes * (cols - 1) + row_bytes, pitch = span + U(0, 200);
+      const size_t total = pitch * (batch - 1) + span;
+      std::vector<unsigned char> dev(total);
+      for (auto& x : dev) x = (unsigned char)rng();
+      std::vector<std::vector<unsigned char>> host(batch, std::vector<unsigned char>(ld_bytes * cols, 0xEE));
+      std::vector<std::vector<int>> hits(batch, std::vector<int>(ld_bytes * cols, 0));
+      const size_t W = U(1, 9000);
+      const int parts = (int)U(1, 17);
+      for (size_t c0 = 0; c0 < total; c0 += W) {
+        const size_t c1 = c0 + W < total ? c0 + W : total;
+        for (int part = 0; part < parts; ++part) {
+          size_t p0, p1;
+          window_part(c0, c1, part, parts, &p0, &p1);
+          scatter_pieces(p0, p1, pitch, batch, ld_bytes, row_bytes, cols,
+                         [&](long b, size_t in_inst, size_t at, size_t len) {
+                           if (at < p0 || at + len > p1 || in_inst + len > ld_bytes * cols) {
+                             std::printf("range\n");
+                             std::exit(3);
+                           }
+                           std::memcpy(&host[b][in_inst], &dev[at], len);
+                           for (size_t i = 0; i < len; ++i) ++hits[b][in_inst + i];
+                         });
+        }
+      }
+      for (long b = 0; b < batch; ++b)
+        for (long j = 0; j < cols; ++j)
+          for (size_t r = 0; r < ld_bytes; ++r) {
+            const size_t x = j * ld_bytes + r;
+            const bool in = r < row_bytes;
+            if (in ? (hits[b][x] != 1 || host[b][x] != dev[b * pitch + x]) : (hits[b][x] != 0 || host[b][x] != 0xEE)) {
+              std::printf("scatter trial %d b %ld col %ld r %zu\n", trial, b, j, r);
+              return 4;
+            }
+          }
+    }
+  }
+  std::puts("ok");
+  return 0;
+}
+""")
+    exe = tmp_path / "t"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(ROOT / "ssblasex_b200" / "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout)
+
+
 def test_fault_injection_setter():
     import ssblasex_b200 as S
     for f in (S.SSBLAS_FAULT_SKIP_COPY, S.SSBLAS_FAULT_ALLOC, S.SSBLAS_FAULT_NONE):

@@ -364,12 +364,18 @@ def grouped_leg(S, count: int, steps: int, warmup: int, stream):
                                         p.lda, arrs[1], p.types[1], p.ldb, be.ctypes.data, arrs[2], p.types[2],
                                         p.ldc, 1, 0, 0)
     ms_l, wall_l = timed(loop, max(1, steps // 5), 1)
+    # the same grouped call in plain mode (fp64 tiles on DMMA, fp32 tiles on FFMA): the same
+    # arithmetic as the loop above, one call
+    ms_gp, wall_gp = timed(lambda: gd.call(device_arrays=True), steps, warmup)
+    launches_p = S.last_run_info()["kernel_launches"]
     S.set_sync_mode(True)
     return {"workload": f"grouped_{count}", "instances": count, "flops": flops,
             "tflops": flops / (ms_g * 1e-3) / 1e12,
             "grouped": {"ms_device": ms_g, "ms_wall": wall_g, "launches": launches},
             "plain_loop": {"ms_device": ms_l, "ms_wall": wall_l, "launches": count},
-            "speedup_vs_plain_loop": ms_l / ms_g, "speedup_vs_plain_loop_wall": wall_l / wall_g}
+            "speedup_vs_plain_loop": ms_l / ms_g, "speedup_vs_plain_loop_wall": wall_l / wall_g,
+            "grouped_plain": {"ms_device": ms_gp, "ms_wall": wall_gp, "launches": launches_p,
+                              "speedup_vs_plain_loop": ms_l / ms_gp}}
 
 
 def run_grouped(args):

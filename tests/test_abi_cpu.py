@@ -330,3 +330,21 @@ def test_environment_knobs():
 
 
 S_INTERNAL_ERROR = 3
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` (the reference's own CPU implementation, or the C restatement
+    where the reference was not built) prints one JSON line with the contract's keys: the
+    metric and unit of the GPU arm, an `e2e` with no host<->device bytes, and a `cpu_baseline`
+    naming the kind, the threads and the sample."""
+    import json
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "0",
+                        "--workload", "fp32_batch64_128"], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "TFLOP/s" and line["value"] > 0
+    assert line["higher_is_better"] is True and line["n_gpus"] == 1 and line["steps"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    cb = line["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and "instances" in cb["sample"]
+    assert line["config"]["workload"] == "fp32_batch64_128"
